@@ -1,0 +1,247 @@
+/*
+ * cansfz.h -- C ABI of the B200-native CaNS-Fizzy per-time-step hot path.
+ *
+ * One GPU, one 1x1 pencil.  All fields use the reference's storage convention:
+ * FP64, Fortran column-major (x fastest), one ghost layer, i.e. a field of the
+ * interior size n = (nx,ny,nz) is an array a(0:nx+1,0:ny+1,0:nz+1) of
+ * (nx+2)*(ny+2)*(nz+2) doubles.  Tendency arrays (the AB2 histories) are
+ * interior-only, a(1:nx,1:ny,1:nz).  1-D z metrics (dzci, dzfi, ...) are
+ * a(0:nz+1).
+ *
+ * Every entry point returns an int status (CANSFZ_OK == 0).  The reference
+ * returns nothing and aborts with `error stop`; a Fortran shim maps a non-zero
+ * status to the reference's abort message.
+ *
+ * Per-procedure entries take DEVICE pointers (what `!$acc host_data
+ * use_device(...)` hands a bind(C) interface) and run on the context's stream.
+ * Scalars are passed by value.  Hidden `save` state of the reference (AB2
+ * histories, dlmin, first-call flags) lives in the context.
+ */
+#ifndef CANSFZ_H
+#define CANSFZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CANSFZ_OK               0
+#define CANSFZ_ERR_ARG          1  /* bad size, pointer or parameter        */
+#define CANSFZ_ERR_CUDA         2  /* a CUDA runtime call failed            */
+#define CANSFZ_ERR_TIMEOUT      3  /* a bounded device wait ran out         */
+#define CANSFZ_ERR_NAN          4  /* NaN in the divergence check           */
+#define CANSFZ_ERR_DIVERGENCE   5  /* max divergence above `small`          */
+#define CANSFZ_ERR_DT           6  /* dt_cfl < small, or dt_f above limit   */
+#define CANSFZ_ERR_UNSUPPORTED  7  /* BC / option not built for the GPU     */
+#define CANSFZ_ERR_NOMEM        8  /* device allocation failed              */
+#define CANSFZ_ERR_NOT_FOUND    9  /* no CUDA device / extension missing    */
+
+/* ---- runtime switches for the reference's compile-time macros ------------ */
+enum { CANSFZ_ACDI = 0, CANSFZ_VOF_THINC = 1 };    /* _INTERFACE_CAPTURING_VOF */
+enum { CANSFZ_FORM_FP64 = 0, CANSFZ_FORM_MIXED = 1 };
+
+/*
+ * Run parameters: the namelists &dns and &two_fluid of input.nml
+ * (src/param.f90:91-120) plus the derived quantities and the macros that the
+ * reference fixes at compile time.  Character arrays keep Fortran order, e.g.
+ * cbcvel(0:1,3,3) -> cbcvel[ivel][idir][ibound], so a bind(C) derived type
+ * with the same members maps onto this struct member by member.
+ */
+typedef struct cansfz_params {
+  /* &dns */
+  int32_t ng[3];
+  double  l[3];
+  int32_t gtype;
+  double  gr;
+  double  cfl, dtmax, dt_f;
+  int32_t is_solve_ns, is_track_interface;
+  int32_t icheck;
+  char    cbcvel[3][3][2];
+  double  bcvel[3][3][2];
+  char    cbcpre[3][2];
+  double  bcpre[3][2];
+  double  bforce[3], gacc[3];
+  /* &two_fluid */
+  char    cbcpsi[3][2];
+  double  bcpsi[3][2];
+  char    cbcnor[3][3][2];
+  double  bcnor[3][3][2];
+  double  sigma, rho12[2], mu12[2], beta12[2];
+  double  psi_thickness_factor;
+  double  acdi_gam_factor, acdi_gam_min;   /* not namelist inputs in the reference */
+  /* compile-time macros of the reference (src/param.f90, configs/flags.mk) */
+  int32_t interface_capturing;  /* CANSFZ_ACDI (default) or CANSFZ_VOF_THINC   */
+  int32_t sdf_normals;          /* _SDF_NORMALS, default 1                     */
+  int32_t brackbill;            /* _CAPILLARY_BRACKBILL_NORMALIZATION, default 1 */
+  /* forms of this library (no reference counterpart) */
+  int32_t form;                 /* CANSFZ_FORM_FP64 (drop-in) or CANSFZ_FORM_MIXED */
+  int32_t refine_sweeps;        /* mixed form: FP64-residual refinement sweeps */
+  int32_t reserved[8];
+} cansfz_params;
+
+/* Per-step diagnostics, mirrored from the device (main.f90 prints). */
+typedef struct cansfz_diag {
+  double  time;
+  int64_t istep;
+  double  dt, dto, dt_cfl;
+  double  gam, seps;
+  double  divtot, divmax;     /* last chkdt/chkdiv evaluation (every icheck) */
+  double  mass12[2];          /* phase masses, cmpt_mean_mass (output.f90:759) */
+  int32_t status;             /* last abort reason, CANSFZ_OK when none      */
+  int32_t reserved[7];
+} cansfz_diag;
+
+typedef struct cansfz_ctx cansfz_ctx;
+
+/* ---- lifecycle ----------------------------------------------------------
+ * cansfz_create: replaces the set-up part of program cans
+ *   (src/main.f90:147-412): initmpi (1x1 pencil), initgrid, initsolver,
+ *   acdi_set_epsilon, device allocation of every field and workspace.
+ * `stream` is a cudaStream_t (NULL: the context creates its own).          */
+int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out);
+int cansfz_destroy(cansfz_ctx* ctx);
+const char* cansfz_status_string(int status);
+int cansfz_version(void);
+
+/* Field I/O in the reference halo layout.  `on_device` != 0: the pointers
+ * are device pointers; otherwise host pointers (pinned or pageable).
+ * Replaces `!$acc enter data copyin(u,v,w,p,psi)` + boundary fills and the
+ * restart read `load_one('r',...)` (src/main.f90:321-356).               */
+int cansfz_set_fields(cansfz_ctx* ctx, const double* u, const double* v,
+                      const double* w, const double* p, const double* psi,
+                      int on_device);
+int cansfz_get_fields(cansfz_ctx* ctx, double* u, double* v, double* w,
+                      double* p, double* psi, int on_device);
+/* Read one auxiliary field (phi, kappa, normx, normy, normz, psiflx_x..z,
+ * psio, pn, po) by name into a halo-layout buffer.                        */
+int cansfz_get_aux(cansfz_ctx* ctx, const char* name, double* out, int on_device);
+
+/* Finish the start-up sequence after set_fields: BCs, phi, normals,
+ * curvature, Gamma and the first chkdt (src/main.f90:337-412).            */
+int cansfz_prepare(cansfz_ctx* ctx);
+
+/* Advance n time steps: the loop body of src/main.f90:422-562 (AB2 phase
+ * update, momentum, projection, pressure update, Gamma every step,
+ * chkdt/chkdiv every icheck).  Captured as a CUDA graph after the first
+ * call.  Returns CANSFZ_ERR_DIVERGENCE / _NAN / _DT on the reference's abort
+ * conditions, after finishing the step that triggered them.              */
+int cansfz_step(cansfz_ctx* ctx, int nsteps);
+int cansfz_get_diag(cansfz_ctx* ctx, cansfz_diag* d);
+/* Device stream the context runs on (cudaStream_t). */
+void* cansfz_stream(cansfz_ctx* ctx);
+
+/* ---- per-procedure drop-in entries (device pointers) ---------------------
+ * Argument order follows the reference.  n = interior sizes of the 1x1
+ * pencil (must equal the context's).                                      */
+
+/* rk_2fl (src/rk.f90:193-254): AB2 phase update + clip; keeps the
+ * dpsidtrk/dpsidtrko histories in ctx.  ACDI or THINC per the context.   */
+int cansfz_rk_2fl(cansfz_ctx* ctx, const double rkpar[2], double dt,
+                  double gam, double seps, double beta,
+                  const double* u, const double* v, const double* w,
+                  const double* normx, const double* normy, const double* normz,
+                  const double* phi, double* psi,
+                  double* psiflx_x, double* psiflx_y, double* psiflx_z);
+
+/* acdi_transport_pf (src/acdi.f90:64-225): dpsidt (interior) + face fluxes */
+int cansfz_acdi_transport_pf(cansfz_ctx* ctx, double gam, double seps,
+                             const double* u, const double* v, const double* w,
+                             const double* normx, const double* normy,
+                             const double* normz, const double* phi,
+                             const double* psi, double* dpsidt,
+                             double* flux_x, double* flux_y, double* flux_z);
+
+/* vof_thinc_transport_psi (src/vof_thinc_qq.f90:39-133) */
+int cansfz_vof_thinc_transport_psi(cansfz_ctx* ctx, double beta,
+                                   const double* u, const double* v, const double* w,
+                                   const double* normx, const double* normy,
+                                   const double* normz, const double* phi,
+                                   const double* psi, double* dpsidt,
+                                   double* flux_x, double* flux_y, double* flux_z);
+
+/* acdi_cmpt_phi (src/acdi.f90:227-248), vof_thinc_cmpt_phi
+ * (src/vof_thinc_qq.f90:135-157): SDF proxy over the full halo array.     */
+int cansfz_acdi_cmpt_phi(cansfz_ctx* ctx, double seps, const double* psi, double* phi);
+int cansfz_vof_thinc_cmpt_phi(cansfz_ctx* ctx, double beta, const double* psi, double* phi);
+
+/* acdi_set_gamma (src/acdi.f90:32-62): returns Gamma = sqrt(max|u_c|^2)*gam_factor */
+int cansfz_acdi_set_gamma(cansfz_ctx* ctx, double gam_factor, const double* u,
+                          const double* v, const double* w, double* gam);
+
+/* cmpt_norm_curv_youngs (src/two_fluid.f90:60-175) */
+int cansfz_cmpt_norm_curv_youngs(cansfz_ctx* ctx, const double* psi,
+                                 double* normx, double* normy, double* normz,
+                                 double* kappa);
+
+/* clip_field (src/two_fluid.f90:35-58), full halo array */
+int cansfz_clip_field(cansfz_ctx* ctx, double rmin, double rmax, double* p);
+
+/* rk (src/rk.f90:16-131): momentum AB2 with the density ratio, then the
+ * pressure-split, surface-tension, gravity and body-force terms.  Keeps
+ * the d?dtrk/d?dtrko histories in ctx.                                     */
+int cansfz_rk(cansfz_ctx* ctx, const double rkpar[2], double dt, double dt_r,
+              const double rho_av[3], const double* psi, const double* kappa,
+              const double* p, const double* pn, const double* po,
+              const double* psio, const double* psiflx_x, const double* psiflx_y,
+              const double* psiflx_z, double* u, double* v, double* w);
+
+/* mom_xyz_ad (src/mom.f90:505-851) and mom_xyz_oth (src/mom.f90:853-1039):
+ * interior-only tendencies.                                               */
+int cansfz_mom_xyz_ad(cansfz_ctx* ctx, const double* psiflx_x, const double* psiflx_y,
+                      const double* psiflx_z, const double* u, const double* v,
+                      const double* w, const double* psi,
+                      double* dudt, double* dvdt, double* dwdt);
+int cansfz_mom_xyz_oth(cansfz_ctx* ctx, double dt_r, const double rho_av[3],
+                       const double* p, const double* psi, const double* kappa,
+                       const double* pn, const double* po,
+                       double* dudt, double* dvdt, double* dwdt);
+
+/* fillps (src/fillps.f90:13-51): p = rho0*div(u)/dt on the interior */
+int cansfz_fillps(cansfz_ctx* ctx, double dti, const double* u, const double* v,
+                  const double* w, double* p);
+
+/* updt_rhs_b (src/bound.f90:341-396) with the context's rhsb planes */
+int cansfz_updt_rhs_b(cansfz_ctx* ctx, double* p);
+
+/* solver_gpu (src/solver_gpu.f90:31-163): constant-coefficient Poisson
+ * solve in place on the interior of p (halo layout), 1x1 pencil, in-HBM
+ * transforms; plans, eigenvalues and tridiagonal coefficients come from
+ * the context (initsolver, src/initsolver.f90:15-79).                      */
+int cansfz_solver(cansfz_ctx* ctx, double* p);
+
+/* correc (src/correc.f90:13-67), updatep (src/updatep.f90:13-24) */
+int cansfz_correc(cansfz_ctx* ctx, double dt, const double* p,
+                  double* u, double* v, double* w);
+int cansfz_updatep(cansfz_ctx* ctx, const double* pp, double* p);
+
+/* boundp / bounduvw (src/bound.f90:15-124) with the context's BCs.
+ * which: 0 = cbcpre, 1 = cbcpsi, 2 = cbccur (kappa), 3..5 = cbcnor(:,:,1..3) */
+int cansfz_boundp(cansfz_ctx* ctx, int which, double* p);
+int cansfz_bounduvw(cansfz_ctx* ctx, int is_correc, double* u, double* v, double* w);
+
+/* chkdt (src/chkdt.f90:15-94), chkdiv (src/chkdiv.f90:15-49),
+ * bulk_mean_12_stag (src/utils.f90:68-136), cmpt_mean_mass
+ * (src/output.f90:759-790)                                                */
+int cansfz_chkdt(cansfz_ctx* ctx, const double* u, const double* v, const double* w,
+                 double gam, double seps, double* dtmax);
+int cansfz_chkdiv(cansfz_ctx* ctx, const double* u, const double* v, const double* w,
+                  double* divtot, double* divmax);
+int cansfz_bulk_mean_12_stag(cansfz_ctx* ctx, int idir, const double* psi, double* mean);
+int cansfz_cmpt_mean_mass(cansfz_ctx* ctx, const double* psi, double mass12[2]);
+
+/* ---- grid and solver set-up (host arrays) ------------------------------- */
+/* initgrid (src/initgrid.f90:14-78): dzc,dzf,zc,zf of size nz+2 */
+int cansfz_initgrid(int gtype, int nz, double gr, double lz,
+                    double* dzc, double* dzf, double* zc, double* zf);
+/* The context's z metrics (host copies, nz+2 each) */
+int cansfz_get_grid(cansfz_ctx* ctx, double* dzc, double* dzf, double* zc,
+                    double* zf, double* dzci, double* dzfi);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CANSFZ_H */

@@ -1,0 +1,235 @@
+"""Pins of the CPU oracle (oracle/cansfz_oracle.cpp) before it is trusted as
+the parity checker of the CUDA path.
+
+* FFTW r2r kinds restated vs scipy.fft (FFTW's published definitions).
+* Known-answer tests built from the reference's own checks: the discrete
+  Poisson residual (chk_poisson, src/debug.f90:81-114) and the projection
+  test that the reference keeps disabled (src/sanity.f90:211-242).
+* The reference's regression tests tests/rising_bubble and
+  tests/lid_driven_cavity, run through the oracle with the reference's own
+  input files and acceptance criteria (read from the reference checkout at
+  test time; skipped where it is absent).
+"""
+import os
+
+import numpy as np
+import pytest
+import scipy.fft as sf
+from scipy.spatial.distance import directed_hausdorff
+
+import oracle as O
+from cansfz import namelist, params
+
+# FFTW kind numbers (src/fftw.f90:39-62)
+R2HC, HC2R, REDFT01, REDFT10, REDFT11, RODFT01, RODFT10, RODFT11 = 0, 1, 4, 5, 6, 8, 9, 10
+SMALL = np.finfo(np.float64).eps * 1e7   # src/param.f90:21
+
+
+@pytest.mark.parametrize("n", [2, 4, 6, 12, 32, 48, 64, 96, 128, 256])
+def test_r2r_kinds_vs_scipy(n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((5, n))
+    X = np.fft.fft(x, axis=-1)
+    hc = np.zeros_like(x)
+    hc[:, : n // 2 + 1] = X[:, : n // 2 + 1].real
+    for k in range(1, (n + 1) // 2):
+        hc[:, n - k] = X[:, k].imag
+    tol = 1e-13 * n
+    assert np.abs(O.r2r(R2HC, x) - hc).max() <= tol * np.abs(hc).max()
+    assert np.abs(O.r2r(HC2R, hc) - n * x).max() <= tol * n * np.abs(x).max()
+    assert np.abs(O.r2r(REDFT10, x) - sf.dct(x, type=2)).max() <= tol
+    assert np.abs(O.r2r(REDFT01, x) - sf.dct(x, type=3)).max() <= tol
+    assert np.abs(O.r2r(RODFT10, x) - sf.dst(x, type=2)).max() <= tol
+    assert np.abs(O.r2r(RODFT01, x) - sf.dst(x, type=3)).max() <= tol
+    assert np.abs(O.r2r(REDFT11, x) - sf.dct(x, type=4)).max() <= tol
+    assert np.abs(O.r2r(RODFT11, x) - sf.dst(x, type=4)).max() <= tol
+
+
+def test_initgrid_uniform_and_stretched():
+    nz, lz = 96, 2.0
+    dzc, dzf, zc, zf = (np.zeros(nz + 2) for _ in range(4))
+    O.lib().orc_initgrid(1, nz, 0.0, lz, *[O.ptr(a) for a in (dzc, dzf, zc, zf)])
+    # z0 = (k-0.)/(1.*n) is a default-kind (single) quotient in the reference
+    z0 = (np.arange(1, nz + 1, dtype=np.float32) / np.float32(nz)).astype(np.float64)
+    assert np.array_equal(zf[1:nz + 1], z0 * lz)
+    O.lib().orc_initgrid(1, nz, 1.5, lz, *[O.ptr(a) for a in (dzc, dzf, zc, zf)])
+    assert abs(zf[nz] - lz) < 1e-14 and np.all(np.diff(zf[: nz + 1]) > 0)
+    assert dzf[1] < dzf[nz // 2]  # clustered at the two walls
+
+
+def _case(nx, ny, nz, cbcpre="PPPPNN", l=(1.0, 1.0, 1.0), gr=0.0):
+    nl = namelist.defaults()
+    nl.set("ng", np.array([nx, ny, nz]))
+    nl.set("l", np.array(l, dtype=float))
+    nl.set("gr", gr)
+    cp = np.array(list(cbcpre), dtype=object).reshape((2, 3), order="F")
+    nl.set("cbcpre", cp)
+    cv = np.empty((2, 3, 3), dtype=object)
+    for d in range(3):
+        pp = cp[0, d] == "P"
+        for ivel in range(3):
+            cv[:, d, ivel] = "P" if pp else ("D" if ivel == d else ("D" if cp[0, d] == "N" else "N"))
+    nl.set("cbcvel", cv)
+    nl.set("cbcpsi", cp.copy())
+    return O.Case(params.from_namelist(nl)), nl
+
+
+def _laplacian(c, f):
+    """7-point Laplacian of the reference (chk_poisson, src/debug.f90:100-106)."""
+    g = c.grid()
+    nx, ny, nz = c.n
+    dxi, dyi = nx / c.params.l[0], ny / c.params.l[1]
+    dzci, dzfi = g["dzci"], g["dzfi"]
+    lap = np.zeros_like(f)
+    ff = f
+    lap[1:-1, 1:-1, 1:-1] = (
+        (ff[2:, 1:-1, 1:-1] - 2 * ff[1:-1, 1:-1, 1:-1] + ff[:-2, 1:-1, 1:-1]) * dxi**2
+        + (ff[1:-1, 2:, 1:-1] - 2 * ff[1:-1, 1:-1, 1:-1] + ff[1:-1, :-2, 1:-1]) * dyi**2
+        + ((ff[1:-1, 1:-1, 2:] - ff[1:-1, 1:-1, 1:-1]) * dzci[None, None, 1:-1]
+           - (ff[1:-1, 1:-1, 1:-1] - ff[1:-1, 1:-1, :-2]) * dzci[None, None, :-2]) * dzfi[None, None, 1:-1]
+    )
+    return lap
+
+
+@pytest.mark.parametrize("cbcpre,gr", [("PPPPNN", 0.0), ("PPPPPP", 0.0), ("NNPPNN", 0.0),
+                                        ("PPNNNN", 0.0), ("PPPPNN", 1.5), ("DDPPNN", 0.0)])
+def test_poisson_known_answer(cbcpre, gr):
+    """Solve lap(p) = lap(f) for a random f with the BC ghosts of cbcpre:
+    the solution is f up to the constant of the all-Neumann/periodic null
+    space; the residual is checked the way chk_poisson does."""
+    c, _ = _case(24, 16, 20, cbcpre, l=(1.0, 0.75, 1.2), gr=gr)
+    rng = np.random.default_rng(7)
+    f = c.empty()
+    f[1:-1, 1:-1, 1:-1] = rng.standard_normal(c.n)
+    c.call("boundp", 0, f)
+    rhs = _laplacian(c, f)
+    p = rhs.copy(order="F")
+    c.call("solver", p)
+    c.call("boundp", 0, p)
+    inner = (slice(1, -1),) * 3
+    singular = "D" not in cbcpre
+    e = p[inner] - f[inner]
+    if singular:
+        e = e - e.mean()
+    assert np.abs(e).max() < 1e-10 * np.abs(f).max()
+    res = np.abs(_laplacian(c, p)[inner] - rhs[inner]).max()
+    assert res < 1e-9 * np.abs(rhs).max()
+
+
+def test_projection_known_answer():
+    """fillps -> solver -> correc leaves max|div| below `small`
+    (the disabled test_sanity_solver, src/sanity.f90:211-242)."""
+    c, _ = _case(32, 24, 16, "PPPPNN")
+    rng = np.random.default_rng(11)
+    u, v, w = (c.empty() for _ in range(3))
+    for a in (u, v, w):
+        a[1:-1, 1:-1, 1:-1] = rng.uniform(-0.5, 0.5, c.n)
+    c.call("bounduvw", 0, u, v, w)
+    d0t, d0m = np.zeros(1), np.zeros(1)
+    c.call("chkdiv_fields", u, v, w, d0t, d0m)
+    dt = np.pi
+    p = c.empty()
+    c.call("fillps", 1.0 / dt, u, v, w, p)
+    c.call("updt_rhs_b", p)
+    c.call("solver", p)
+    c.call("boundp", 0, p)
+    c.call("correc", dt, p, u, v, w)
+    c.call("bounduvw", 1, u, v, w)
+    divtot, divmax = np.zeros(1), np.zeros(1)
+    c.call("chkdiv_fields", u, v, w, divtot, divmax)
+    assert divmax[0] < SMALL
+    assert divmax[0] < 1e-12 * d0m[0]  # round-off of the FP64 solve
+
+
+def test_uniform_phase_known_answers():
+    """psi = const: zero normals/curvature/phase RHS; u = 0: zero advection."""
+    c, _ = _case(16, 16, 16, "PPPPNN")
+    psi = c.empty() + 0.3
+    phi = c.empty()
+    c.call("acdi_cmpt_phi", c.seps, psi, phi)
+    nx, ny, nz, kap = (c.empty() for _ in range(4))
+    c.call("cmpt_norm_curv_youngs", phi, nx, ny, nz, kap)
+    for a in (nx, ny, nz, kap):
+        assert np.abs(a[1:-1, 1:-1, 1:-1]).max() == 0.0
+    u, v, w = (c.empty() for _ in range(3))
+    dpsidt = np.zeros(c.n, order="F")
+    fx, fy, fz = (c.empty() for _ in range(3))
+    c.call("acdi_transport_pf", 1.0, c.seps, u, v, w, nx, ny, nz, phi, psi, dpsidt, fx, fy, fz)
+    assert np.abs(dpsidt).max() == 0.0
+
+
+def _run_reference_case(case_dir):
+    nl = namelist.read(os.path.join(case_dir, "input.nml"))
+    p = params.from_namelist(nl)
+    c = O.Case(p)
+    sph_file = os.path.join(case_dir, "spheres.in")
+    sph = np.loadtxt(sph_file, ndmin=2) if os.path.exists(sph_file) else None
+    c.init2fl(str(nl["inipsi"]), sph)
+    c.initflow(str(nl["inivel"]))
+    c.prepare()
+    stop = nl["stop_type"]
+    while True:
+        rc = c.step(1)
+        d = c.diag()
+        assert rc == 0, f"oracle aborted with status {rc} at step {d.istep}"
+        if (stop[0] and d.istep >= nl["nstep"]) or (stop[1] and d.time >= nl["time_max"]):
+            break
+    return c, nl, d
+
+
+def _zero_level_points(f, xs, zs):
+    """psi = 0.5 crossings on grid edges (the vertices matplotlib's contour
+    puts on its path), linear interpolation."""
+    g = f - 0.5
+    pts = []
+    for i in range(len(xs) - 1):
+        s = g[i] * g[i + 1] < 0
+        t = g[i][s] / (g[i][s] - g[i + 1][s])
+        pts += list(zip(xs[i] + t * (xs[i + 1] - xs[i]), zs[s]))
+    for k in range(len(zs) - 1):
+        s = g[:, k] * g[:, k + 1] < 0
+        t = g[s, k] / (g[s, k] - g[s, k + 1])
+        pts += list(zip(xs[s], zs[k] + t * (zs[k + 1] - zs[k])))
+    return np.array(pts)
+
+
+@pytest.mark.slow
+def test_reference_rising_bubble(reference_dir):
+    """tests/rising_bubble of the reference: 2-D bubble, t = 3 (6000 steps);
+    psi = 0.5 contour within directed Hausdorff distance 0.1 of the
+    benchmark contour shipped with that test (its test.py criterion)."""
+    case = os.path.join(reference_dir, "tests", "rising_bubble")
+    c, nl, d = _run_reference_case(case)
+    assert d.istep == 6000 and abs(d.time - 3.0) < 1e-9
+    psi = c.get("psi")[1:-1, 1, 1:-1]
+    nx = c.n[0]
+    xs = (np.arange(nx) + 0.5) * c.params.l[0] / nx
+    zs = c.grid()["zc"][1:-1]
+    pts = _zero_level_points(psi, xs, zs)
+    ref = np.loadtxt(os.path.join(case, "c1g2l3s.txt"))
+    err = directed_hausdorff(pts, ref)[0]
+    assert err < 1e-1
+    assert err < 2e-2  # what this restatement achieves (0.0088)
+
+
+@pytest.mark.slow
+def test_reference_lid_driven_cavity(reference_dir):
+    """tests/lid_driven_cavity of the reference (20000 steps): centre-line
+    velocity profiles vs the tables shipped with that test, rtol/atol 0.1."""
+    case = os.path.join(reference_dir, "tests", "lid_driven_cavity")
+    c, nl, d = _run_reference_case(case)
+    v = c.get("v")[1:-1, 1:-1, 1:-1]
+    w = c.get("w")[1:-1, 1:-1, 1:-1]
+    ny, nz = c.n[1], c.n[2]
+    yp = (np.arange(ny) + 0.5) / ny * c.params.l[1]
+    zp = c.grid()["zc"][1:-1]
+    islice = nz // 2
+    ref_u = np.loadtxt(os.path.join(case, "ghiau.txt"))
+    data = v[0]
+    interp = np.interp(ref_u[:, 0], zp, 0.5 * (data[islice, :] + data[islice + 1, :]))
+    np.testing.assert_allclose(interp, ref_u[:, 1], rtol=1e-1, atol=1e-1)
+    islice = ny // 2
+    ref_v = np.loadtxt(os.path.join(case, "ghiav.txt"))
+    data = w[0]
+    interp = np.interp(ref_v[:, 0], yp, 0.5 * (data[:, islice] + data[:, islice + 1]))
+    np.testing.assert_allclose(interp, ref_v[:, 1], rtol=1e-1, atol=1e-1)
