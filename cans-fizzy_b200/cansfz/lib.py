@@ -1,0 +1,103 @@
+"""ctypes binding of libcansfz.so (the C ABI of include/cansfz.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+from .params import Params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libcansfz.so")
+
+D = ct.c_double
+I = ct.c_int
+V = ct.c_void_p          # device or host pointer
+PD = ct.POINTER(ct.c_double)
+
+OK = 0
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA runtime error", 3: "bounded device wait ran out",
+    4: "NaN in the divergence check", 5: "maximum divergence too large", 6: "time step too small",
+    7: "unsupported on the GPU path", 8: "device allocation failed", 9: "no CUDA device",
+}
+
+
+class Diag(ct.Structure):
+    _fields_ = [("time", D), ("istep", ct.c_int64), ("dt", D), ("dto", D), ("dt_cfl", D),
+                ("gam", D), ("seps", D), ("divtot", D), ("divmax", D), ("mass12", D * 2),
+                ("status", ct.c_int32), ("reserved", ct.c_int32 * 7)]
+
+
+SIGNATURES = {
+    "cansfz_version": (I, []),
+    "cansfz_status_string": (ct.c_char_p, [I]),
+    "cansfz_create": (I, [ct.POINTER(Params), V, ct.POINTER(V)]),
+    "cansfz_destroy": (I, [V]),
+    "cansfz_stream": (V, [V]),
+    "cansfz_set_fields": (I, [V, V, V, V, V, V, I]),
+    "cansfz_get_fields": (I, [V, V, V, V, V, V, I]),
+    "cansfz_get_aux": (I, [V, ct.c_char_p, V, I]),
+    "cansfz_prepare": (I, [V]),
+    "cansfz_step": (I, [V, I]),
+    "cansfz_get_diag": (I, [V, ct.POINTER(Diag)]),
+    "cansfz_rk_2fl": (I, [V, PD, D, D, D, D] + [V] * 10),
+    "cansfz_acdi_transport_pf": (I, [V, D, D] + [V] * 12),
+    "cansfz_vof_thinc_transport_psi": (I, [V, D] + [V] * 12),
+    "cansfz_acdi_cmpt_phi": (I, [V, D, V, V]),
+    "cansfz_vof_thinc_cmpt_phi": (I, [V, D, V, V]),
+    "cansfz_acdi_set_gamma": (I, [V, D, V, V, V, PD]),
+    "cansfz_cmpt_norm_curv_youngs": (I, [V] + [V] * 5),
+    "cansfz_clip_field": (I, [V, D, D, V]),
+    "cansfz_rk": (I, [V, PD, D, D, PD] + [V] * 11),
+    "cansfz_mom_xyz_ad": (I, [V] + [V] * 10),
+    "cansfz_mom_xyz_oth": (I, [V, D, PD] + [V] * 8),
+    "cansfz_fillps": (I, [V, D, V, V, V, V]),
+    "cansfz_updt_rhs_b": (I, [V, V]),
+    "cansfz_solver": (I, [V, V]),
+    "cansfz_correc": (I, [V, D, V, V, V, V]),
+    "cansfz_updatep": (I, [V, V, V]),
+    "cansfz_boundp": (I, [V, I, V]),
+    "cansfz_bounduvw": (I, [V, I, V, V, V]),
+    "cansfz_chkdt": (I, [V, V, V, V, D, D, PD]),
+    "cansfz_chkdiv": (I, [V, V, V, V, PD, PD]),
+    "cansfz_bulk_mean_12_stag": (I, [V, I, V, PD]),
+    "cansfz_cmpt_mean_mass": (I, [V, V, PD]),
+    "cansfz_initgrid": (I, [I, I, D, D, PD, PD, PD, PD]),
+    "cansfz_get_grid": (I, [V, PD, PD, PD, PD, PD, PD]),
+    # library controls (no reference counterpart)
+    "cansfz_set_time": (I, [V, D, ct.c_longlong]),
+    "cansfz_set_inivel": (I, [V, ct.c_char_p]),
+}
+
+_lib = None
+
+
+class CansfzError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        super().__init__(f"{what}: status {status} ({STATUS.get(status, 'unknown')})")
+        self.status = status
+
+
+def load():
+    """Load libcansfz.so from the source tree (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"{LIBPATH} is not built: run `python cans-fizzy_b200/build.py` "
+                               "(or __graft_entry__.build()); there is no CPU fallback")
+        L = ct.CDLL(LIBPATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "cansfz"):
+    if rc != OK:
+        raise CansfzError(rc, what)
+    return rc

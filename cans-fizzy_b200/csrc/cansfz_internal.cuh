@@ -1,0 +1,219 @@
+// Internal definitions of libcansfz (sm_100a).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cansfz.h"
+
+#define CANSFZ_EPS 2.220446049250313e-16  // epsilon(1._rp), src/param.f90:18
+
+namespace cansfz {
+
+// ---------------------------------------------------------------------------
+// geometry of one case on the device: the 1x1 pencil, halo strides, z metrics
+// ---------------------------------------------------------------------------
+struct Geo {
+  int nx, ny, nz;     // interior sizes
+  int sx, sxy;        // halo-layout strides: (i,j,k) -> i + sx*j + sxy*k
+  double dxi, dyi;    // dli(1:2)
+  double dx, dy;      // dl(1:2)
+  const double* dzci; // (0:nz+1)
+  const double* dzfi; // (0:nz+1)
+  const double* dzc;  // (0:nz+1)
+  const double* dzf;  // (0:nz+1)
+  __host__ __device__ inline int h(int i, int j, int k) const { return i + sx * j + sxy * k; }
+  __host__ __device__ inline int t(int i, int j, int k) const {
+    return (i - 1) + nx * ((j - 1) + ny * (k - 1));
+  }
+  __host__ __device__ inline int hsize() const { return sxy * (nz + 2); }
+  __host__ __device__ inline int tsize() const { return nx * ny * nz; }
+};
+
+// ---------------------------------------------------------------------------
+// per-step scalars kept on the device so a whole step is graph-capturable.
+// Names follow program cans (src/main.f90:414-562).
+// ---------------------------------------------------------------------------
+struct DevScalars {
+  double time, dt, dto, dt_r, dti;   // dti = dtrki = 1/dt
+  double tm1, tm2;                   // tm_coeff = [1+dt_r/2, -dt_r/2]
+  double f1, f2, f12;                // factor1, factor2, factor12 of rk/rk_2fl
+  double gam, seps, beta;            // ACDI Gamma, epsilon; THINC beta
+  double rho_av[3];                  // bulk_mean_12_stag results
+  double dt_cfl, divtot, divmax;
+  double mass12[2];
+  long long istep;
+  int status;                        // CANSFZ_OK or the abort reason
+  int halted;                        // 1 after an abort: later steps do nothing
+  int first_rk, first_rk2fl;         // is_first of rk and rk_2fl (save attribute)
+  int check_now;                     // 1 on icheck steps
+  // reduction slots
+  unsigned long long max_bits[4];    // non-negative doubles as ordered bits
+  double pad[4];
+};
+
+// ---------------------------------------------------------------------------
+// run constants (set once)
+// ---------------------------------------------------------------------------
+struct Phys {
+  double rho12[2], mu12[2];
+  double rho0;
+  double sigma, surf_factor;   // sigma or sigma*2/(rho1+rho2) (Brackbill)
+  double bforce[3], gacc[3];
+  double gam_factor, gam_min;
+  double cfl, dtmax, dt_f;
+  double dlmin;
+  double small;
+  int icheck;
+  int brackbill;   // _CAPILLARY_BRACKBILL_NORMALIZATION
+  int acdi;        // 1: ACDI, 0: THINC
+  int sdf;         // _SDF_NORMALS
+  int solve_ns, track;
+  double mu_over_rho_max, rho_min, gmax;   // chkdt constants
+};
+
+// ---------------------------------------------------------------------------
+// boundary fills (src/bound.f90).  One BcField describes one field: the face
+// rules of set_bc in each direction, precomputed on the host exactly as
+// set_bc derives factor and sgn.
+// ---------------------------------------------------------------------------
+enum BcType : int { BC_NONE = 0, BC_P = 1, BC_D = 2, BC_N = 3 };
+struct BcFace {
+  int type;        // BcType; BC_NONE: face not bounded (periodic halo) or skipped
+  int centered;
+  double factor;   // as computed by set_bc
+  double sgn;
+};
+struct BcField {
+  double* p;
+  BcFace face[3][2];     // [idir][ibound]
+  int halo_periodic[3];  // y/z periodic self-exchange (updthalo)
+};
+#define BC_MAXF 6
+struct BcGroup {
+  int nf;
+  BcField f[BC_MAXF];
+};
+
+// ---------------------------------------------------------------------------
+// Poisson solver plan (initsolver + fftini), device side
+// ---------------------------------------------------------------------------
+#define FFT_MAXSTAGES 16
+struct LinePlan {
+  int n;          // real length
+  int kind;       // 0: periodic (R2HC/HC2R packed), 1: NN (DCT-II/III), 2: DD (DST-II/III)
+  int m;          // complex FFT length (n/2)
+  int nst;        // number of radix stages
+  int radix[FFT_MAXSTAGES];
+  const double2* tw;    // exp(-2 pi i q / m), q = 0..m-1
+  const double2* tw2;   // exp(-2 pi i k / n), k = 0..n/2 (real-transform post twiddle)
+  const double2* twc;   // exp(-i pi k / (2n)), k = 0..n (DCT/DST twiddle)
+};
+
+struct PoissonPlan {
+  LinePlan px, py;
+  const double* lam;     // eigenvalues in the packed spectral layout, nx*ny
+  const double* a;       // tridiagonal coefficients (1:nz)
+  const double* b;
+  const double* c;
+  double normfft;
+  int zper;              // periodic z: Sherman-Morrison variant
+  double* work;          // nx*ny*nz spectral buffer
+  double* work2;         // second buffer (periodic z, DCT remaps)
+};
+
+// ---------------------------------------------------------------------------
+// kernel launchers (host functions), all on `st`
+// ---------------------------------------------------------------------------
+struct Launch {
+  cudaStream_t st;
+  int nsm;
+};
+
+// k_stencil.cu
+void launch_acdi_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                           const double* u, const double* v, const double* w,
+                           const double* nx, const double* ny, const double* nz,
+                           const double* phi, const double* psi, double* dpsidt,
+                           double* fx, double* fy, double* fz);
+void launch_thinc_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                            const double* u, const double* v, const double* w,
+                            const double* nx, const double* ny, const double* nz,
+                            const double* phi, const double* psi, double* dpsidt,
+                            double* fx, double* fy, double* fz);
+void launch_acdi_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                      const double* u, const double* v, const double* w, const double* nx,
+                      const double* ny, const double* nz, const double* phi, const double* psi,
+                      double* psi_out, double* hist, double* fx, double* fy, double* fz);
+void launch_thinc_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                       const double* u, const double* v, const double* w, const double* nx,
+                       const double* ny, const double* nz, const double* phi, const double* psi,
+                       double* psi_out, double* hist, double* fx, double* fy, double* fz);
+void launch_psi_update(const Launch& L, const Geo& g, const DevScalars* sc,
+                       const double* psi_in, double* psi_out, double* dpsidt, double* dpsidto);
+void launch_cmpt_phi(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi,
+                     const double* psi, double* phi);
+void launch_youngs(const Launch& L, const Geo& g, const DevScalars* sc, const double* psi,
+                   double* nx, double* ny, double* nz, double* kappa);
+void launch_clip(const Launch& L, const Geo& g, double rmin, double rmax, double* p);
+void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* fx,
+                   const double* fy, const double* fz, const double* u, const double* v,
+                   const double* w, const double* psi, double* du, double* dv, double* dw);
+void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                    const double* p, const double* psi, const double* kappa, const double* pn,
+                    const double* po, double* du, double* dv, double* dw);
+void launch_rk_update1(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                       const double* psio, const double* psi, const double* du,
+                       const double* dv, const double* dw, double* duo, double* dvo,
+                       double* dwo, double* u, double* v, double* w);
+void launch_rk_update2(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                       const double* psi, const double* du, const double* dv,
+                       const double* dw, double* u, double* v, double* w);
+void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                           const double* u, const double* v, const double* w,
+                           const double* psi, const double* psio, const double* fx,
+                           const double* fy, const double* fz, const double* p,
+                           const double* po, const double* kappa, double* duo,
+                           double* dvo, double* dwo, double* uo, double* vo, double* wo);
+void launch_fillps(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                   const double* u, const double* v, const double* w, double* p);
+void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
+                   const double* p, double* u, double* v, double* w);
+void launch_updatep_interior(const Launch& L, const Geo& g, const DevScalars* sc,
+                             const double* phi, const double* pp, double* pout);
+void launch_updatep_full(const Launch& L, const Geo& g, const double* pp, double* p);
+void launch_copy(const Launch& L, size_t n, const double* src, double* dst);
+void launch_fill(const Launch& L, size_t n, double val, double* dst);
+
+// reductions: results land in DevScalars
+void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
+                  const double* u, const double* v, const double* w, bool apply_floor);
+void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
+                  const double* u, const double* v, const double* w, bool only_on_check);
+void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial,
+                   const double* u, const double* v, const double* w, bool only_on_check);
+void launch_bulk_mean(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
+                      double* partial, int idir, const double* gvr, const double* psi);
+void launch_mass(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
+                 const double* psi, double vol);
+
+// step bookkeeping kernels
+void launch_step_begin(const Launch& L, DevScalars* sc, int icheck);
+void launch_step_end(const Launch& L, const Phys& ph, DevScalars* sc);
+
+// k_bc.cu
+void launch_bc_group(const Launch& L, const Geo& g, const BcGroup& grp, const DevScalars* sc);
+void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
+                       const double* rhsbx, const double* rhsby, const double* rhsbz,
+                       double* p);
+
+// k_poisson.cu
+void poisson_set_attributes();
+void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                    double* p);
+void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& pl,
+                              const Phys& ph, const DevScalars* sc, const double* u,
+                              const double* v, const double* w, const double* rhsb_planes,
+                              double* phi);
+
+}  // namespace cansfz

@@ -1,0 +1,1081 @@
+// libcansfz context: set-up of program cans (src/main.f90:147-412) for one
+// GPU and a 1x1 pencil, the per-step sequence (src/main.f90:414-562) as two
+// CUDA graphs (the double-buffer parities), and the C ABI of
+// include/cansfz.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cansfz_internal.cuh"
+
+using namespace cansfz;
+
+#define CK(x)                                                                  \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (e_ != cudaSuccess) {                                                   \
+      std::fprintf(stderr, "cansfz: %s failed: %s\n", #x, cudaGetErrorString(e_)); \
+      return CANSFZ_ERR_CUDA;                                                  \
+    }                                                                          \
+  } while (0)
+
+namespace {
+
+const double PI_D = 3.14159265358979323846;
+
+// initgrid, src/initgrid.f90:14-78 (z0 is a default-kind real quotient)
+void host_initgrid(int gtype, int n, double gr, double lz, double* dzc, double* dzf, double* zc, double* zf) {
+  zf[0] = 0.;
+  for (int k = 1; k <= n; ++k) {
+    const float z0f = ((float)k - 0.f) / (1.f * (float)n);
+    const double z0 = (double)z0f, alpha = gr;
+    double z;
+    if (alpha == 0.) z = z0;
+    else if (gtype == 2) z = 1.0 * (1. + std::tanh((z0 - 1.0) * alpha) / std::tanh(alpha / 1.));
+    else if (gtype == 3) z = 1. - 1.0 * (1. + std::tanh((1. - z0 - 1.0) * alpha) / std::tanh(alpha / 1.));
+    else if (gtype == 4) {
+      if (z0 <= 0.5) z = 0.5 * (1. - 1. + std::tanh(2. * alpha * (z0 - 0.)) / std::tanh(alpha));
+      else z = 0.5 * (1. + 1. + std::tanh(2. * alpha * (z0 - 1.)) / std::tanh(alpha));
+    } else z = 0.5 * (1. + std::tanh((z0 - 0.5) * alpha) / std::tanh(alpha / 2.));
+    zf[k] = z * lz;
+  }
+  for (int k = 1; k <= n; ++k) dzf[k] = zf[k] - zf[k - 1];
+  dzf[0] = dzf[1];
+  dzf[n + 1] = dzf[n];
+  for (int k = 0; k <= n; ++k) dzc[k] = .5 * (dzf[k] + dzf[k + 1]);
+  dzc[n + 1] = dzc[n];
+  zc[0] = -dzc[0] / 2.;
+  zf[0] = 0.;
+  for (int k = 1; k <= n + 1; ++k) {
+    zc[k] = zc[k - 1] + dzc[k - 1];
+    zf[k] = zf[k - 1] + dzf[k];
+  }
+}
+
+bool is_pp(const char c[2]) { return c[0] == 'P' && c[1] == 'P'; }
+std::string bc2(const char c[2]) { return std::string{c[0], c[1]}; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the context
+// ---------------------------------------------------------------------------
+struct cansfz_ctx {
+  cansfz_params P{};
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  Launch L{};
+  Geo g{};
+  Phys ph{};
+  int n[3]{};
+  double dl[3]{}, dli[3]{};
+  std::vector<double> dzc, dzf, zc, zf, dzci, dzfi, gvr_c, gvr_f;
+  double* d_grid = nullptr;  // dzc,dzf,dzci,dzfi,gvr_c,gvr_f on the device
+  int is_bound[3][2]{};
+  int halo_periodic[3]{};
+  char cbccur[3][2]{};
+  double bccur[3][2]{};
+  double seps = 0., beta = 1.;
+  // fields (halo layout unless noted)
+  double *u[2]{}, *v[2]{}, *w[2]{}, *psi[2]{}, *p[2]{};
+  double *phip = nullptr, *phi = nullptr, *kappa = nullptr, *nx = nullptr, *ny = nullptr, *nz = nullptr;
+  double *fx = nullptr, *fy = nullptr, *fz = nullptr;
+  double *hpsi = nullptr, *hu = nullptr, *hv = nullptr, *hw = nullptr;       // AB2 histories (interior)
+  double *tu = nullptr, *tv = nullptr, *tw_ = nullptr, *tpsi = nullptr;     // per-procedure scratch (interior)
+  int cur = 0;  // index of the current u,v,w,psi and of p (= pn); po = p[cur^1]
+  // Poisson solver (initsolver)
+  PoissonPlan pl{};
+  double* d_solver = nullptr;  // lam, a, b, c, twiddles, rhsb
+  std::vector<double> lam_h, a_h, b_h, c_h;
+  double* rhsbx = nullptr; double* rhsby = nullptr; double* rhsbz = nullptr;
+  bool rhsb_zero = true;
+  double* d_work = nullptr;
+  // reductions, scalars
+  double* partial = nullptr;
+  DevScalars* sc = nullptr;       // the step scalars (device)
+  DevScalars* sc_call = nullptr;  // scalars of a per-procedure call (device)
+  DevScalars* sc_host = nullptr;  // pinned mirror
+  bool first_rk_call = true, first_rk2fl_call = true;
+  // graphs
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool prepared = false;
+  int last_status = CANSFZ_OK;
+  std::vector<void*> allocs;
+  char inivel[8] = "zer";
+};
+
+namespace {
+
+template <typename T>
+int dalloc(cansfz_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, n * sizeof(T) + 256) != cudaSuccess) return CANSFZ_ERR_NOMEM;
+  if (cudaMemset(q, 0, n * sizeof(T) + 256) != cudaSuccess) return CANSFZ_ERR_CUDA;
+  c->allocs.push_back(q);
+  *p = (T*)q;
+  return CANSFZ_OK;
+}
+
+// set_bc's factor/sgn for one face (src/bound.f90:138-152)
+BcFace make_face(char ctype, int ib, bool centered, double rvalue, double dr) {
+  BcFace f{};
+  f.centered = centered ? 1 : 0;
+  double factor = rvalue, sgn = 0.;
+  if (ctype == 'D' && centered) { factor = 2. * factor; sgn = -1.; }
+  if (ctype == 'N') {
+    if (ib == 0) factor = -dr * factor;
+    else factor = dr * factor;
+    sgn = 1.;
+  }
+  f.factor = factor;
+  f.sgn = sgn;
+  f.type = ctype == 'P' ? BC_P : (ctype == 'D' ? BC_D : (ctype == 'N' ? BC_N : BC_NONE));
+  return f;
+}
+
+// boundp for one scalar field, src/bound.f90:81-124
+BcField bc_scalar(const cansfz_ctx* c, const char cbc[3][2], const double bc[3][2], double* p) {
+  BcField F{};
+  F.p = p;
+  for (int d = 0; d < 3; ++d) F.halo_periodic[d] = c->halo_periodic[d];
+  for (int d = 0; d < 3; ++d)
+    for (int ib = 0; ib < 2; ++ib) {
+      if (!c->is_bound[d][ib]) continue;
+      double dr = d == 0 ? c->dl[0] : (d == 1 ? c->dl[1] : (ib == 0 ? c->dzc[0] : c->dzc[c->n[2]]));
+      F.face[d][ib] = make_face(cbc[d][ib], ib, true, bc[d][ib], dr);
+    }
+  return F;
+}
+
+// bounduvw, src/bound.f90:15-79: the three velocity components
+void bc_vel(const cansfz_ctx* c, bool is_correc, double* u, double* v, double* w, BcField out[3]) {
+  const cansfz_params& P = c->P;
+  double* fld[3] = {u, v, w};
+  for (int ivel = 0; ivel < 3; ++ivel) {
+    BcField& F = out[ivel];
+    F = BcField{};
+    F.p = fld[ivel];
+    for (int d = 0; d < 3; ++d) F.halo_periodic[d] = c->halo_periodic[d];
+    for (int d = 0; d < 3; ++d) {
+      const bool normal = (ivel == d);
+      const bool imp = (!is_correc) || is_pp(P.cbcvel[d][d]);
+      if (normal && !imp) continue;
+      for (int ib = 0; ib < 2; ++ib) {
+        if (!c->is_bound[d][ib]) continue;
+        double dr;
+        if (d == 0) dr = c->dl[0];
+        else if (d == 1) dr = c->dl[1];
+        else {
+          const int kk = ib == 0 ? 0 : c->n[2];
+          dr = normal ? c->dzf[kk] : c->dzc[kk];
+        }
+        F.face[d][ib] = make_face(P.cbcvel[ivel][d][ib], ib, !normal, P.bcvel[ivel][d][ib], dr);
+      }
+    }
+  }
+}
+
+// which: 0 cbcpre, 1 cbcpsi, 2 cbccur, 3..5 cbcnor(:,:,1..3)
+void scalar_bc_spec(const cansfz_ctx* c, int which, const char (**cbc)[2], const double (**bc)[2]) {
+  const cansfz_params& P = c->P;
+  *cbc = P.cbcpre; *bc = P.bcpre;
+  if (which == 1) { *cbc = P.cbcpsi; *bc = P.bcpsi; }
+  else if (which == 2) { *cbc = c->cbccur; *bc = c->bccur; }
+  else if (which >= 3 && which <= 5) { *cbc = P.cbcnor[which - 3]; *bc = P.bcnor[which - 3]; }
+}
+
+void run_bc(cansfz_ctx* c, std::initializer_list<BcField> fields, const DevScalars* sc) {
+  BcGroup grp{};
+  for (const BcField& f : fields) {
+    if (grp.nf == BC_MAXF) { launch_bc_group(c->L, c->g, grp, sc); grp.nf = 0; }
+    grp.f[grp.nf++] = f;
+  }
+  launch_bc_group(c->L, c->g, grp, sc);
+}
+
+void run_bcp(cansfz_ctx* c, int which, double* p, const DevScalars* sc) {
+  const char(*cbc)[2];
+  const double(*bc)[2];
+  scalar_bc_spec(c, which, &cbc, &bc);
+  run_bc(c, {bc_scalar(c, cbc, bc, p)}, sc);
+}
+
+void run_bcuvw(cansfz_ctx* c, bool is_correc, double* u, double* v, double* w, const DevScalars* sc) {
+  BcField F[3];
+  bc_vel(c, is_correc, u, v, w, F);
+  run_bc(c, {F[0], F[1], F[2]}, sc);
+}
+
+// ---------------------------------------------------------------------------
+// initsolver + fftini (src/initsolver.f90:15-228, src/fft.f90:20-140) for the
+// packed spectral layout of the transforms in k_poisson.cu
+// ---------------------------------------------------------------------------
+int line_kind(const char c[2]) {
+  const std::string s = bc2(c);
+  if (s == "PP") return 0;
+  if (s == "NN") return 1;
+  if (s == "DD") return 2;
+  return -1;
+}
+
+// eigenvalues (src/initsolver.f90:81-139) in the order of the device layout
+void eigen_device_order(int n, int kind, std::vector<double>& lam) {
+  lam.assign(n, 0.);
+  if (kind == 0) {
+    // packed (r0, r_{n/2}, r1, i1, ...).  The reference's CPU order is the
+    // half-complex one: index m <= n/2 is r_m, index n-k is i_k, with
+    // lambda(l) = -2(1-cos(2(l-1)pi/n)); the same expression is evaluated
+    // at the same l for each slot.
+    auto lamhc = [&](int m) { return -2. * (1. - std::cos((double)(2 * m) * PI_D / (1. * n))); };
+    const int h = n / 2;
+    lam[0] = lamhc(0);
+    if (n > 1) lam[1] = lamhc(h);
+    for (int k = 1; k < h; ++k) {
+      lam[2 * k] = lamhc(k);
+      lam[2 * k + 1] = lamhc(n - k);
+    }
+  } else if (kind == 1) {
+    for (int l = 1; l <= n; ++l) lam[l - 1] = -2. * (1. - std::cos((double)(l - 1) * PI_D / (1. * n)));
+  } else {
+    for (int l = 1; l <= n; ++l) lam[l - 1] = -2. * (1. - std::cos((double)l * PI_D / (1. * n)));
+  }
+}
+
+bool factorize(int m, int radix[FFT_MAXSTAGES], int* nst) {
+  int k = 0;
+  while (m % 4 == 0 && m > 4) { radix[k++] = 4; m /= 4; }
+  for (int r : {4, 2, 3, 5, 7}) while (m % r == 0) { radix[k++] = r; m /= r; }
+  *nst = k;
+  return m == 1 && k <= FFT_MAXSTAGES;
+}
+
+int setup_solver(cansfz_ctx* c) {
+  const cansfz_params& P = c->P;
+  const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+  const int kx = line_kind(P.cbcpre[0]), ky = line_kind(P.cbcpre[1]);
+  if (kx < 0 || ky < 0) return CANSFZ_ERR_UNSUPPORTED;  // ND/DN in x,y (also rejected by the reference GPU path)
+  if ((nx & 1) || (ny & 1)) return CANSFZ_ERR_UNSUPPORTED;
+  // eigenvalues
+  std::vector<double> lx, ly;
+  eigen_device_order(nx, kx, lx);
+  eigen_device_order(ny, ky, ly);
+  for (auto& x : lx) x = x * (c->dli[0] * c->dli[0]);
+  for (auto& x : ly) x = x * (c->dli[1] * c->dli[1]);
+  c->lam_h.resize((size_t)nx * ny);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) c->lam_h[i + (size_t)nx * j] = lx[i] + ly[j];
+  // tridmatrix, src/initsolver.f90:141-183 (c_or_f = 'c')
+  c->a_h.resize(nz); c->b_h.resize(nz); c->c_h.resize(nz);
+  for (int k = 1; k <= nz; ++k) {
+    c->a_h[k - 1] = c->dzfi[k] * c->dzci[k - 1];
+    c->c_h[k - 1] = c->dzfi[k] * c->dzci[k];
+  }
+  for (int k = 0; k < nz; ++k) c->b_h[k] = -(c->a_h[k] + c->c_h[k]);
+  double factor[2];
+  for (int ib = 0; ib < 2; ++ib) {
+    const char t = P.cbcpre[2][ib];
+    factor[ib] = t == 'P' ? 0. : (t == 'D' ? -1. : 1.);
+  }
+  c->b_h[0] = c->b_h[0] + factor[0] * c->a_h[0];
+  c->b_h[nz - 1] = c->b_h[nz - 1] + factor[1] * c->c_h[nz - 1];
+  // bc_rhs (src/initsolver.f90:185-228)
+  std::vector<double> dzc_(nz + 2), dzf_(nz + 2);
+  for (int k = 0; k <= nz + 1; ++k) { dzc_[k] = 1. / c->dzci[k]; dzf_[k] = 1. / c->dzfi[k]; }
+  auto bcr = [&](const char cbc[2], const double bcv[2], const double dlc[2], const double dlf[2], size_t plane,
+                 std::vector<double>& rhs) {
+    double f[2];
+    for (int ib = 0; ib < 2; ++ib) {
+      if (cbc[ib] == 'P') f[ib] = 0.;
+      else if (cbc[ib] == 'D') f[ib] = -2. * bcv[ib];
+      else f[ib] = (ib == 0 ? 1. : -1.) * dlc[ib] * bcv[ib];
+    }
+    rhs.assign(plane * 2, 0.);
+    for (int ib = 0; ib < 2; ++ib)
+      for (size_t q = 0; q < plane; ++q) rhs[q + plane * ib] = f[ib] / dlc[ib] / dlf[ib];
+  };
+  std::vector<double> rx, ry, rz;
+  {
+    const double dlx[2] = {c->dl[0], c->dl[0]}, dly[2] = {c->dl[1], c->dl[1]};
+    const double dlcz[2] = {dzc_[0], dzc_[nz]}, dlfz[2] = {dzf_[1], dzf_[nz]};
+    bcr(P.cbcpre[0], P.bcpre[0], dlx, dlx, (size_t)ny * nz, rx);
+    bcr(P.cbcpre[1], P.bcpre[1], dly, dly, (size_t)nx * nz, ry);
+    bcr(P.cbcpre[2], P.bcpre[2], dlcz, dlfz, (size_t)nx * ny, rz);
+  }
+  c->rhsb_zero = true;
+  for (auto* r : {&rx, &ry, &rz})
+    for (double x : *r) if (x != 0.) c->rhsb_zero = false;
+  // normfft (src/fft.f90:96,133,139): PP -> n, NN/DD -> 2n
+  double normfft = 1.;
+  normfft = normfft * (kx == 0 ? 1. : 2.) * (nx + 0.);
+  normfft = normfft * (ky == 0 ? 1. : 2.) * (ny + 0.);
+  // line plans
+  LinePlan* lps[2] = {&c->pl.px, &c->pl.py};
+  const int ns[2] = {nx, ny}, kinds[2] = {kx, ky};
+  std::vector<double> host;  // everything device-side for the solver, packed
+  size_t off_lam = 0, off_a, off_b, off_c, off_tw[2], off_tw2[2], off_twc[2], off_rx, off_ry, off_rz;
+  host.insert(host.end(), c->lam_h.begin(), c->lam_h.end());
+  off_a = host.size(); host.insert(host.end(), c->a_h.begin(), c->a_h.end());
+  off_b = host.size(); host.insert(host.end(), c->b_h.begin(), c->b_h.end());
+  off_c = host.size(); host.insert(host.end(), c->c_h.begin(), c->c_h.end());
+  for (int d = 0; d < 2; ++d) {
+    LinePlan& lp = *lps[d];
+    lp.n = ns[d];
+    lp.kind = kinds[d];
+    lp.m = ns[d] / 2;
+    if (!factorize(lp.m, lp.radix, &lp.nst)) return CANSFZ_ERR_UNSUPPORTED;
+    const long double pi = 3.14159265358979323846264338327950288L;
+    auto pad2 = [&]() { if (host.size() & 1) host.push_back(0.); };  // double2 alignment
+    pad2();
+    off_tw[d] = host.size();
+    for (int q = 0; q < lp.m; ++q) {
+      const long double a = -2.0L * pi * q / (long double)lp.m;
+      host.push_back((double)cosl(a)); host.push_back((double)sinl(a));
+    }
+    off_tw2[d] = host.size();
+    for (int k = 0; k <= lp.m; ++k) {
+      const long double a = -2.0L * pi * k / (long double)lp.n;
+      host.push_back((double)cosl(a)); host.push_back((double)sinl(a));
+    }
+    off_twc[d] = host.size();
+    for (int k = 0; k <= lp.n; ++k) {
+      const long double a = -pi * k / (2.0L * lp.n);
+      host.push_back((double)cosl(a)); host.push_back((double)sinl(a));
+    }
+  }
+  off_rx = host.size(); host.insert(host.end(), rx.begin(), rx.end());
+  off_ry = host.size(); host.insert(host.end(), ry.begin(), ry.end());
+  off_rz = host.size(); host.insert(host.end(), rz.begin(), rz.end());
+  int rc = dalloc(c, &c->d_solver, host.size() + 2);
+  if (rc) return rc;
+  CK(cudaMemcpy(c->d_solver, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice));
+  double* D = c->d_solver;
+  c->pl.lam = D + off_lam;
+  c->pl.a = D + off_a;
+  c->pl.b = D + off_b;
+  c->pl.c = D + off_c;
+  for (int d = 0; d < 2; ++d) {
+    lps[d]->tw = (const double2*)(D + off_tw[d]);
+    lps[d]->tw2 = (const double2*)(D + off_tw2[d]);
+    lps[d]->twc = (const double2*)(D + off_twc[d]);
+  }
+  c->rhsbx = D + off_rx; c->rhsby = D + off_ry; c->rhsbz = D + off_rz;
+  c->pl.normfft = 1. / normfft;
+  c->pl.zper = is_pp(P.cbcpre[2]) ? 1 : 0;
+  const size_t nint = (size_t)nx * ny * nz;
+  rc = dalloc(c, &c->pl.work, nint);
+  if (rc) return rc;
+  if (c->pl.zper) {
+    rc = dalloc(c, &c->pl.work2, nint);
+    if (rc) return rc;
+  }
+  return CANSFZ_OK;
+}
+
+int upload_scalars(cansfz_ctx* c, DevScalars* dst, const DevScalars& h) {
+  CK(cudaMemcpyAsync(dst, &h, sizeof(DevScalars), cudaMemcpyHostToDevice, c->st));
+  return CANSFZ_OK;
+}
+
+// scalars for one per-procedure call: a copy of the step scalars with overrides
+int call_scalars(cansfz_ctx* c, DevScalars& h) {
+  h.halted = 0;
+  h.status = 0;
+  return upload_scalars(c, c->sc_call, h);
+}
+
+int sync_status(cansfz_ctx* c) {
+  CK(cudaMemcpyAsync(c->sc_host, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CANSFZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// prescribed velocity for is_solve_ns = F ('voy'/'vox'/'zer' of initflow,
+// src/initflow.f90:242-275), evaluated at the step's time
+// ---------------------------------------------------------------------------
+__global__ void k_prescribed_vel(Geo g, const DevScalars* __restrict__ sc, int which, double lx, double ly,
+                                 double lz, const double* __restrict__ zc, const double* __restrict__ zf,
+                                 double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+                                 double* __restrict__ p) {
+  if (sc->halted) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > g.nx) return;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  const double pi = 3.14159265358979323846;
+  const double time = sc->time;
+  const double zcc = zc[k] / lz, zff = zf[k] / lz;
+  const double yc = ((double)j - .5) * g.dy / ly, yf = ((double)j - .0) * g.dy / ly;
+  const double xc = ((double)i - .5) * g.dx / lx, xf = ((double)i - .0) * g.dx / lx;
+  const int c = g.h(i, j, k);
+  const double ct = cos(pi * time / 4.);
+  if (which == 1) {  // voy
+    const double sx = sin(pi * xf), sz = sin(pi * zff);
+    u[c] = sx * sx * sin(2 * pi * zcc) * ct;
+    v[c] = 0.;
+    w[c] = -(sz * sz) * sin(2 * pi * xc) * ct;
+  } else if (which == 2) {  // vox
+    const double sy = sin(pi * yf), sz = sin(pi * zff);
+    u[c] = 0.;
+    v[c] = sy * sy * sin(2 * pi * zcc) * ct;
+    w[c] = -(sz * sz) * sin(2 * pi * yc) * ct;
+  } else {
+    u[c] = 0.; v[c] = 0.; w[c] = 0.;
+  }
+  p[c] = 0.;
+}
+
+// ---------------------------------------------------------------------------
+// one time step (src/main.f90:422-529) on the current parity `c->cur`
+// ---------------------------------------------------------------------------
+void enqueue_step(cansfz_ctx* c) {
+  const cansfz_params& P = c->P;
+  const Launch& L = c->L;
+  const Geo& g = c->g;
+  const int a = c->cur, b = a ^ 1;
+  DevScalars* sc = c->sc;
+  launch_step_begin(L, sc, P.icheck);
+  // phase field: rk_2fl + boundary fills + phi + normals/curvature
+  if (P.is_track_interface) {
+    if (c->ph.acdi)
+      launch_acdi_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
+                       c->psi[a], c->psi[b], c->hpsi, c->fx, c->fy, c->fz);
+    else
+      launch_thinc_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
+                        c->psi[a], c->psi[b], c->hpsi, c->fx, c->fy, c->fz);
+    BcField F[3];
+    bc_vel(c, false, c->fx, c->fy, c->fz, F);
+    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc);
+    if (c->ph.sdf) launch_cmpt_phi(L, g, sc, c->ph.acdi != 0, c->psi[b], c->phi);
+    launch_youngs(L, g, sc, c->ph.sdf ? c->phi : c->psi[b], c->nx, c->ny, c->nz, c->kappa);
+    run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
+               bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
+           sc);
+  } else {
+    launch_copy(L, (size_t)g.hsize(), c->psi[a], c->psi[b]);
+    launch_fill(L, (size_t)g.hsize(), 0., c->fx);
+    launch_fill(L, (size_t)g.hsize(), 0., c->fy);
+    launch_fill(L, (size_t)g.hsize(), 0., c->fz);
+  }
+  if (!P.is_solve_ns) {
+    const std::string iv(c->inivel);
+    const int which = iv == "voy" ? 1 : (iv == "vox" ? 2 : 0);
+    dim3 bb(g.nx >= 128 ? 128 : 64), gg((g.nx + bb.x - 1) / bb.x, g.ny, g.nz);
+    k_prescribed_vel<<<gg, bb, 0, L.st>>>(g, sc, which, P.l[0], P.l[1], P.l[2], c->d_grid + 6 * (g.nz + 2),
+                                          c->d_grid + 7 * (g.nz + 2), c->u[b], c->v[b], c->w[b], c->p[a]);
+    run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
+    launch_copy(L, (size_t)g.hsize(), c->p[a], c->p[b]);
+  } else {
+    // bulk_mean_12_stag for periodic gravity directions (src/main.f90:470-477)
+    for (int d = 0; d < 3; ++d)
+      if (std::fabs(P.gacc[d]) > 0. && is_pp(P.cbcpre[d]))
+        launch_bulk_mean(L, g, c->ph, sc, c->partial, d + 1, c->d_grid + (d == 2 ? 5 : 4) * (g.nz + 2), c->psi[b]);
+    // rk: the whole momentum update in one pass
+    launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy, c->fz,
+                          c->p[a], c->p[b], c->kappa, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
+    run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
+    // fillps + updt_rhs_b + solver
+    if (c->rhsb_zero) {
+      launch_poisson_fused_rhs(L, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip);
+    } else {
+      launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->phip);
+      launch_updt_rhs_b(L, g, c->is_bound, c->rhsbx, c->rhsby, c->rhsbz, c->phip);
+      launch_poisson(L, g, c->pl, sc, c->phip);
+    }
+    run_bcp(c, 0, c->phip, sc);
+    launch_correc(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b]);
+    run_bcuvw(c, true, c->u[b], c->v[b], c->w[b], sc);
+    // updatep: p_new = phi + p into the po slot, then po <- p by the parity flip
+    launch_updatep_interior(L, g, sc, c->phip, c->p[a], c->p[b]);
+    run_bcp(c, 0, c->p[b], sc);
+  }
+  launch_step_end(L, c->ph, sc);
+  if (c->ph.acdi) launch_gamma(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
+  launch_chkdt(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
+  launch_chkdiv(L, g, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int cansfz_version(void) { return 100; }
+
+const char* cansfz_status_string(int s) {
+  switch (s) {
+    case CANSFZ_OK: return "ok";
+    case CANSFZ_ERR_ARG: return "invalid argument";
+    case CANSFZ_ERR_CUDA: return "CUDA runtime error";
+    case CANSFZ_ERR_TIMEOUT: return "bounded device wait ran out";
+    case CANSFZ_ERR_NAN: return "ERROR: maximum divergence is too large (NaN)";
+    case CANSFZ_ERR_DIVERGENCE: return "ERROR: maximum divergence is too large.";
+    case CANSFZ_ERR_DT: return "ERROR: time step is too small / fixed time step exceeds the stability limit";
+    case CANSFZ_ERR_UNSUPPORTED: return "boundary condition or option not supported on the GPU path";
+    case CANSFZ_ERR_NOMEM: return "device allocation failed";
+    case CANSFZ_ERR_NOT_FOUND: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
+  if (!prm || !out) return CANSFZ_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CANSFZ_ERR_NOT_FOUND;
+  const cansfz_params& P = *prm;
+  for (int d = 0; d < 3; ++d)
+    if (P.ng[d] < 2) return CANSFZ_ERR_ARG;
+  if (P.ng[2] < 3) return CANSFZ_ERR_ARG;
+  if ((double)(P.ng[0] + 2) * (P.ng[1] + 2) * (P.ng[2] + 2) > 2.0e9) return CANSFZ_ERR_ARG;
+  cansfz_ctx* c = new cansfz_ctx();
+  c->P = P;
+  int rc = CANSFZ_OK;
+  auto fail = [&](int r) { cansfz_destroy(c); return r; };
+  if (stream) c->st = (cudaStream_t)stream;
+  else {
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return fail(CANSFZ_ERR_CUDA);
+    c->own_stream = true;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&c->L.nsm, cudaDevAttrMultiProcessorCount, dev);
+  c->L.st = c->st;
+  poisson_set_attributes();
+  for (int d = 0; d < 3; ++d) c->n[d] = P.ng[d];
+  const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+  for (int d = 0; d < 3; ++d) {
+    c->dl[d] = P.l[d] / (1. * P.ng[d]);
+    c->dli[d] = 1. / c->dl[d];
+  }
+  // initgrid and the z metrics (src/main.f90:230-272)
+  c->dzc.assign(nz + 2, 0.); c->dzf = c->dzc; c->zc = c->dzc; c->zf = c->dzc; c->dzci = c->dzc; c->dzfi = c->dzc;
+  host_initgrid(P.gtype, nz, P.gr, P.l[2], c->dzc.data(), c->dzf.data(), c->zc.data(), c->zf.data());
+  for (int k = 0; k <= nz + 1; ++k) { c->dzci[k] = 1. / c->dzc[k]; c->dzfi[k] = 1. / c->dzf[k]; }
+  c->gvr_c.resize(nz + 2); c->gvr_f.resize(nz + 2);
+  for (int k = 0; k <= nz + 1; ++k) {
+    c->gvr_c[k] = c->dl[0] * c->dl[1] * c->dzc[k] / (P.l[0] * P.l[1] * P.l[2]);
+    c->gvr_f[k] = c->dl[0] * c->dl[1] * c->dzf[k] / (P.l[0] * P.l[1] * P.l[2]);
+  }
+  {
+    std::vector<double> gh;
+    for (auto* v : {&c->dzc, &c->dzf, &c->dzci, &c->dzfi, &c->gvr_c, &c->gvr_f, &c->zc, &c->zf})
+      gh.insert(gh.end(), v->begin(), v->end());
+    if ((rc = dalloc(c, &c->d_grid, gh.size()))) return fail(rc);
+    if (cudaMemcpy(c->d_grid, gh.data(), gh.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(CANSFZ_ERR_CUDA);
+  }
+  const int S = nz + 2;
+  Geo& g = c->g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.sx = nx + 2; g.sxy = (nx + 2) * (ny + 2);
+  g.dxi = c->dli[0]; g.dyi = c->dli[1];
+  g.dx = c->dl[0]; g.dy = c->dl[1];
+  g.dzc = c->d_grid; g.dzf = c->d_grid + S; g.dzci = c->d_grid + 2 * S; g.dzfi = c->d_grid + 3 * S;
+  // topology of the 1x1 pencil (src/initmpi.f90:148-183)
+  for (int d = 0; d < 3; ++d) {
+    const bool per = is_pp(P.cbcpre[d]);
+    c->halo_periodic[d] = (d > 0 && per) ? 1 : 0;
+    c->is_bound[d][0] = c->is_bound[d][1] = (d == 0) ? 1 : (per ? 0 : 1);
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int ib = 0; ib < 2; ++ib) { c->cbccur[d][ib] = P.cbcpsi[d][ib]; c->bccur[d][ib] = P.bcpre[d][ib]; }
+  // physics constants (src/param.f90:170-178)
+  Phys& ph = c->ph;
+  for (int q = 0; q < 2; ++q) { ph.rho12[q] = P.rho12[q]; ph.mu12[q] = P.mu12[q]; }
+  ph.rho0 = std::min(P.rho12[0], P.rho12[1]);
+  ph.sigma = P.sigma;
+  ph.brackbill = P.brackbill ? 1 : 0;
+  ph.surf_factor = ph.brackbill ? P.sigma * 2. / (P.rho12[0] + P.rho12[1]) : P.sigma;
+  for (int d = 0; d < 3; ++d) { ph.bforce[d] = P.bforce[d]; ph.gacc[d] = P.gacc[d]; }
+  ph.gam_factor = P.acdi_gam_factor;
+  ph.gam_min = P.acdi_gam_min;
+  ph.cfl = P.cfl; ph.dtmax = P.dtmax; ph.dt_f = P.dt_f;
+  ph.small = CANSFZ_EPS * 1.0e7;
+  ph.icheck = P.icheck;
+  ph.acdi = P.interface_capturing == CANSFZ_ACDI ? 1 : 0;
+  ph.sdf = P.sdf_normals ? 1 : 0;
+  ph.solve_ns = P.is_solve_ns ? 1 : 0;
+  ph.track = P.is_track_interface ? 1 : 0;
+  ph.dlmin = std::min(c->dl[0], c->dl[1]);
+  for (int k = 0; k <= nz + 1; ++k) ph.dlmin = std::min(ph.dlmin, 1. / c->dzfi[k]);
+  ph.mu_over_rho_max = std::max(P.mu12[0] / P.rho12[0], P.mu12[1] / P.rho12[1]);
+  ph.rho_min = std::min(P.rho12[0], P.rho12[1]);
+  ph.gmax = std::max(std::fabs(P.gacc[0]), std::max(std::fabs(P.gacc[1]), std::fabs(P.gacc[2])));
+  // acdi_set_epsilon (src/acdi.f90:16-30) and the THINC beta (src/param.f90:178)
+  double dlmax = std::max(c->dl[0], c->dl[1]);
+  for (int k = 0; k <= nz + 1; ++k) dlmax = std::max(dlmax, 1. / c->dzfi[k]);
+  c->seps = dlmax * P.psi_thickness_factor;
+  c->beta = 1. / (2. * P.psi_thickness_factor);
+  // device fields
+  const size_t H = (size_t)g.hsize(), I = (size_t)g.tsize();
+  for (int q = 0; q < 2; ++q)
+    for (double** f : {&c->u[q], &c->v[q], &c->w[q], &c->psi[q], &c->p[q]})
+      if ((rc = dalloc(c, f, H))) return fail(rc);
+  for (double** f : {&c->phip, &c->phi, &c->kappa, &c->nx, &c->ny, &c->nz, &c->fx, &c->fy, &c->fz})
+    if ((rc = dalloc(c, f, H))) return fail(rc);
+  for (double** f : {&c->hpsi, &c->hu, &c->hv, &c->hw, &c->tu, &c->tv, &c->tw_, &c->tpsi})
+    if ((rc = dalloc(c, f, I))) return fail(rc);
+  if ((rc = setup_solver(c))) return fail(rc);
+  // reductions: partial sums of one launch over the interior blocks
+  const int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
+  const size_t nblk = (size_t)((nx + bx - 1) / bx) * ny * nz;
+  if ((rc = dalloc(c, &c->partial, 2 * nblk + 64))) return fail(rc);
+  if ((rc = dalloc(c, &c->sc, 1))) return fail(rc);
+  if ((rc = dalloc(c, &c->sc_call, 1))) return fail(rc);
+  if (cudaMallocHost(&c->sc_host, sizeof(DevScalars)) != cudaSuccess) return fail(CANSFZ_ERR_NOMEM);
+  std::memset(c->sc_host, 0, sizeof(DevScalars));
+  DevScalars h{};
+  h.seps = c->seps;
+  h.beta = c->beta;
+  h.first_rk = 1;
+  h.first_rk2fl = 1;
+  if ((rc = upload_scalars(c, c->sc, h))) return fail(rc);
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) return fail(CANSFZ_ERR_CUDA);
+  *out = c;
+  return CANSFZ_OK;
+}
+
+int cansfz_destroy(cansfz_ctx* c) {
+  if (!c) return CANSFZ_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& ge : c->gexec)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  for (void* q : c->allocs) cudaFree(q);
+  if (c->sc_host) cudaFreeHost(c->sc_host);
+  if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return CANSFZ_OK;
+}
+
+void* cansfz_stream(cansfz_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int cansfz_set_fields(cansfz_ctx* c, const double* u, const double* v, const double* w, const double* p,
+                      const double* psi, int on_device) {
+  if (!c) return CANSFZ_ERR_ARG;
+  const size_t bytes = (size_t)c->g.hsize() * sizeof(double);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const int a = c->cur;
+  const double* src[5] = {u, v, w, p, psi};
+  double* dst[5] = {c->u[a], c->v[a], c->w[a], c->p[a], c->psi[a]};
+  for (int q = 0; q < 5; ++q)
+    if (src[q]) CK(cudaMemcpyAsync(dst[q], src[q], bytes, kind, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->prepared = false;
+  return CANSFZ_OK;
+}
+
+int cansfz_get_fields(cansfz_ctx* c, double* u, double* v, double* w, double* p, double* psi, int on_device) {
+  if (!c) return CANSFZ_ERR_ARG;
+  const size_t bytes = (size_t)c->g.hsize() * sizeof(double);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const int a = c->cur;
+  double* dst[5] = {u, v, w, p, psi};
+  const double* src[5] = {c->u[a], c->v[a], c->w[a], c->p[a], c->psi[a]};
+  for (int q = 0; q < 5; ++q)
+    if (dst[q]) CK(cudaMemcpyAsync(dst[q], src[q], bytes, kind, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CANSFZ_OK;
+}
+
+int cansfz_get_aux(cansfz_ctx* c, const char* name, double* out, int on_device) {
+  if (!c || !name || !out) return CANSFZ_ERR_ARG;
+  const std::string s(name);
+  const int a = c->cur;
+  const double* src = nullptr;
+  size_t n = (size_t)c->g.hsize();
+  if (s == "phi") src = c->phi;
+  else if (s == "kappa") src = c->kappa;
+  else if (s == "normx") src = c->nx;
+  else if (s == "normy") src = c->ny;
+  else if (s == "normz") src = c->nz;
+  else if (s == "psiflx_x") src = c->fx;
+  else if (s == "psiflx_y") src = c->fy;
+  else if (s == "psiflx_z") src = c->fz;
+  else if (s == "psio") src = c->psi[a ^ 1];
+  else if (s == "pn") src = c->p[a];
+  else if (s == "po") src = c->p[a ^ 1];
+  else if (s == "pcorr") src = c->phip;
+  else if (s == "dpsidtrko") { src = c->hpsi; n = c->g.tsize(); }
+  else if (s == "dudtrko") { src = c->hu; n = c->g.tsize(); }
+  else if (s == "dvdtrko") { src = c->hv; n = c->g.tsize(); }
+  else if (s == "dwdtrko") { src = c->hw; n = c->g.tsize(); }
+  else return CANSFZ_ERR_ARG;
+  CK(cudaMemcpyAsync(out, src, n * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CANSFZ_OK;
+}
+
+int cansfz_prepare(cansfz_ctx* c) {
+  if (!c) return CANSFZ_ERR_ARG;
+  const cansfz_params& P = c->P;
+  const int a = c->cur;
+  DevScalars* sc = c->sc;
+  const Launch& L = c->L;
+  // src/main.f90:337-412
+  run_bcuvw(c, false, c->u[a], c->v[a], c->w[a], sc);
+  run_bcp(c, 0, c->p[a], sc);
+  launch_copy(L, (size_t)c->g.hsize(), c->p[a], c->p[a ^ 1]);  // po = pn = p
+  run_bcp(c, 1, c->psi[a], sc);
+  if (c->ph.sdf) launch_cmpt_phi(L, c->g, sc, c->ph.acdi != 0, c->psi[a], c->phi);
+  launch_youngs(L, c->g, sc, c->ph.sdf ? c->phi : c->psi[a], c->nx, c->ny, c->nz, c->kappa);
+  run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
+             bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
+         sc);
+  if (c->ph.acdi) launch_gamma(L, c->g, c->ph, sc, c->u[a], c->v[a], c->w[a], true);
+  launch_chkdt(L, c->g, c->ph, sc, c->u[a], c->v[a], c->w[a], false);
+  // dto = dt (src/main.f90:409)
+  if (int rc = sync_status(c)) return rc;
+  c->sc_host->dto = c->sc_host->dt;
+  if (int rc = upload_scalars(c, sc, *c->sc_host)) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  c->prepared = true;
+  return CANSFZ_OK;
+}
+
+int cansfz_step(cansfz_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return CANSFZ_ERR_ARG;
+  if (!c->prepared) {
+    int rc = cansfz_prepare(c);
+    if (rc) return rc;
+  }
+  if (c->last_status != CANSFZ_OK) return c->last_status;
+  if (int rc = sync_status(c)) return rc;
+  const long long istep0 = c->sc_host->istep;
+  for (int s = 0; s < nsteps; ++s) {
+    const int par = c->cur;
+    if (!c->gexec[par]) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      enqueue_step(c);
+      CK(cudaStreamEndCapture(c->st, &graph));
+      CK(cudaGraphInstantiate(&c->gexec[par], graph, 0));
+      cudaGraphDestroy(graph);
+    }
+    CK(cudaGraphLaunch(c->gexec[par], c->st));
+    c->cur ^= 1;
+  }
+  if (int rc = sync_status(c)) return rc;
+  // steps after an abort did nothing: put the parity back to the executed count
+  const long long done = c->sc_host->istep - istep0;
+  if ((long long)nsteps != done) c->cur ^= (int)((nsteps - done) & 1);
+  c->last_status = c->sc_host->status;
+  return c->last_status;
+}
+
+int cansfz_get_diag(cansfz_ctx* c, cansfz_diag* d) {
+  if (!c || !d) return CANSFZ_ERR_ARG;
+  launch_mass(c->L, c->g, c->ph, c->sc, c->partial, c->psi[c->cur], c->P.l[0] * c->P.l[1] * c->P.l[2]);
+  if (int rc = sync_status(c)) return rc;
+  const DevScalars& h = *c->sc_host;
+  std::memset(d, 0, sizeof(*d));
+  d->time = h.time; d->istep = h.istep; d->dt = h.dt; d->dto = h.dto; d->dt_cfl = h.dt_cfl;
+  d->gam = h.gam; d->seps = h.seps; d->divtot = h.divtot; d->divmax = h.divmax;
+  d->mass12[0] = h.mass12[0]; d->mass12[1] = h.mass12[1];
+  d->status = h.status;
+  return CANSFZ_OK;
+}
+
+int cansfz_initgrid(int gtype, int nz, double gr, double lz, double* dzc, double* dzf, double* zc, double* zf) {
+  if (nz < 1 || !dzc || !dzf || !zc || !zf) return CANSFZ_ERR_ARG;
+  host_initgrid(gtype, nz, gr, lz, dzc, dzf, zc, zf);
+  return CANSFZ_OK;
+}
+
+int cansfz_get_grid(cansfz_ctx* c, double* dzc, double* dzf, double* zc, double* zf, double* dzci, double* dzfi) {
+  if (!c) return CANSFZ_ERR_ARG;
+  const size_t m = c->dzc.size() * sizeof(double);
+  if (dzc) std::memcpy(dzc, c->dzc.data(), m);
+  if (dzf) std::memcpy(dzf, c->dzf.data(), m);
+  if (zc) std::memcpy(zc, c->zc.data(), m);
+  if (zf) std::memcpy(zf, c->zf.data(), m);
+  if (dzci) std::memcpy(dzci, c->dzci.data(), m);
+  if (dzfi) std::memcpy(dzfi, c->dzfi.data(), m);
+  return CANSFZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-procedure drop-in entries
+// ---------------------------------------------------------------------------
+int cansfz_acdi_transport_pf(cansfz_ctx* c, double gam, double seps, const double* u, const double* v,
+                             const double* w, const double* normx, const double* normy, const double* normz,
+                             const double* phi, const double* psi, double* dpsidt, double* fx, double* fy,
+                             double* fz) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.gam = gam; h.seps = seps;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_acdi_transport(c->L, c->g, c->sc_call, c->ph.sdf != 0, u, v, w, normx, normy, normz, phi, psi, dpsidt, fx,
+                        fy, fz);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_vof_thinc_transport_psi(cansfz_ctx* c, double beta, const double* u, const double* v, const double* w,
+                                   const double* normx, const double* normy, const double* normz, const double* phi,
+                                   const double* psi, double* dpsidt, double* fx, double* fy, double* fz) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.beta = beta;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_thinc_transport(c->L, c->g, c->sc_call, c->ph.sdf != 0, u, v, w, normx, normy, normz, phi, psi, dpsidt,
+                         fx, fy, fz);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_rk_2fl(cansfz_ctx* c, const double rkpar[2], double dt, double gam, double seps, double beta,
+                  const double* u, const double* v, const double* w, const double* normx, const double* normy,
+                  const double* normz, const double* phi, double* psi, double* fx, double* fy, double* fz) {
+  if (!c || !rkpar) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.gam = gam; h.seps = seps; h.beta = beta;
+  h.f1 = rkpar[0] * dt; h.f2 = rkpar[1] * dt; h.f12 = h.f1 + h.f2;
+  h.first_rk2fl = c->first_rk2fl_call ? 1 : 0;
+  if (int rc = call_scalars(c, h)) return rc;
+  if (c->ph.acdi)
+    launch_acdi_transport(c->L, c->g, c->sc_call, c->ph.sdf != 0, u, v, w, normx, normy, normz, phi, psi, c->tpsi,
+                          fx, fy, fz);
+  else
+    launch_thinc_transport(c->L, c->g, c->sc_call, c->ph.sdf != 0, u, v, w, normx, normy, normz, phi, psi, c->tpsi,
+                           fx, fy, fz);
+  // psi += f1*d + f2*d_old (in place), d_old <- d; then clip_field (whole array)
+  launch_psi_update(c->L, c->g, c->sc_call, psi, psi, c->tpsi, c->hpsi);
+  launch_copy(c->L, (size_t)c->g.tsize(), c->tpsi, c->hpsi);
+  launch_clip(c->L, c->g, 0., 1., psi);
+  c->first_rk2fl_call = false;
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_acdi_cmpt_phi(cansfz_ctx* c, double seps, const double* psi, double* phi) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.seps = seps;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_cmpt_phi(c->L, c->g, c->sc_call, true, psi, phi);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_vof_thinc_cmpt_phi(cansfz_ctx* c, double beta, const double* psi, double* phi) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.beta = beta;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_cmpt_phi(c->L, c->g, c->sc_call, false, psi, phi);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_acdi_set_gamma(cansfz_ctx* c, double gam_factor, const double* u, const double* v, const double* w,
+                          double* gam) {
+  if (!c || !gam) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  if (int rc = call_scalars(c, h)) return rc;
+  Phys ph = c->ph;
+  ph.gam_factor = gam_factor;
+  launch_gamma(c->L, c->g, ph, c->sc_call, u, v, w, false);
+  DevScalars r{};
+  CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *gam = r.gam;
+  return CANSFZ_OK;
+}
+
+int cansfz_cmpt_norm_curv_youngs(cansfz_ctx* c, const double* psi, double* normx, double* normy, double* normz,
+                                 double* kappa) {
+  if (!c) return CANSFZ_ERR_ARG;
+  launch_youngs(c->L, c->g, nullptr, psi, normx, normy, normz, kappa);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_clip_field(cansfz_ctx* c, double rmin, double rmax, double* p) {
+  if (!c) return CANSFZ_ERR_ARG;
+  launch_clip(c->L, c->g, rmin, rmax, p);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_mom_xyz_ad(cansfz_ctx* c, const double* fx, const double* fy, const double* fz, const double* u,
+                      const double* v, const double* w, const double* psi, double* dudt, double* dvdt,
+                      double* dwdt) {
+  if (!c) return CANSFZ_ERR_ARG;
+  launch_mom_ad(c->L, c->g, c->ph, fx, fy, fz, u, v, w, psi, dudt, dvdt, dwdt);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_mom_xyz_oth(cansfz_ctx* c, double dt_r, const double rho_av[3], const double* p, const double* psi,
+                       const double* kappa, const double* pn, const double* po, double* dudt, double* dvdt,
+                       double* dwdt) {
+  if (!c || !rho_av) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.dt_r = dt_r;
+  for (int d = 0; d < 3; ++d) h.rho_av[d] = rho_av[d];
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_mom_oth(c->L, c->g, c->ph, c->sc_call, p, psi, kappa, pn, po, dudt, dvdt, dwdt);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_rk(cansfz_ctx* c, const double rkpar[2], double dt, double dt_r, const double rho_av[3], const double* psi,
+              const double* kappa, const double* p, const double* pn, const double* po, const double* psio,
+              const double* fx, const double* fy, const double* fz, double* u, double* v, double* w) {
+  if (!c || !rkpar || !rho_av) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.f1 = rkpar[0] * dt; h.f2 = rkpar[1] * dt; h.f12 = h.f1 + h.f2;
+  h.dt_r = dt_r;
+  for (int d = 0; d < 3; ++d) h.rho_av[d] = rho_av[d];
+  h.first_rk = c->first_rk_call ? 1 : 0;
+  if (int rc = call_scalars(c, h)) return rc;
+  const Launch& L = c->L;
+  // src/rk.f90:72-130: mom_xyz_ad -> update 1 (history in place) -> mom_xyz_oth -> update 2
+  launch_mom_ad(L, c->g, c->ph, fx, fy, fz, u, v, w, psi, c->tu, c->tv, c->tw_);
+  launch_rk_update1(L, c->g, c->ph, c->sc_call, psio, psi, c->tu, c->tv, c->tw_, c->hu, c->hv, c->hw, u, v, w);
+  launch_copy(L, (size_t)c->g.tsize(), c->tu, c->hu);
+  launch_copy(L, (size_t)c->g.tsize(), c->tv, c->hv);
+  launch_copy(L, (size_t)c->g.tsize(), c->tw_, c->hw);
+  launch_mom_oth(L, c->g, c->ph, c->sc_call, p, psi, kappa, pn, po, c->tu, c->tv, c->tw_);
+  launch_rk_update2(L, c->g, c->ph, c->sc_call, psi, c->tu, c->tv, c->tw_, u, v, w);
+  c->first_rk_call = false;
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_fillps(cansfz_ctx* c, double dti, const double* u, const double* v, const double* w, double* p) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.dti = dti;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_fillps(c->L, c->g, c->ph, c->sc_call, u, v, w, p);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_updt_rhs_b(cansfz_ctx* c, double* p) {
+  if (!c) return CANSFZ_ERR_ARG;
+  if (!c->rhsb_zero) launch_updt_rhs_b(c->L, c->g, c->is_bound, c->rhsbx, c->rhsby, c->rhsbz, p);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_solver(cansfz_ctx* c, double* p) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_poisson(c->L, c->g, c->pl, c->sc_call, p);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_correc(cansfz_ctx* c, double dt, const double* p, double* u, double* v, double* w) {
+  if (!c) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.dt = dt;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_correc(c->L, c->g, c->ph, c->sc_call, p, u, v, w);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_updatep(cansfz_ctx* c, const double* pp, double* p) {
+  if (!c) return CANSFZ_ERR_ARG;
+  launch_updatep_full(c->L, c->g, pp, p);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_boundp(cansfz_ctx* c, int which, double* p) {
+  if (!c || which < 0 || which > 5) return CANSFZ_ERR_ARG;
+  run_bcp(c, which, p, nullptr);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_bounduvw(cansfz_ctx* c, int is_correc, double* u, double* v, double* w) {
+  if (!c) return CANSFZ_ERR_ARG;
+  run_bcuvw(c, is_correc != 0, u, v, w, nullptr);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_chkdt(cansfz_ctx* c, const double* u, const double* v, const double* w, double gam, double seps,
+                 double* dtmax) {
+  if (!c || !dtmax) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  h.gam = gam; h.seps = seps;
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_chkdt(c->L, c->g, c->ph, c->sc_call, u, v, w, false);
+  DevScalars r{};
+  CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *dtmax = r.dt_cfl;
+  return CANSFZ_OK;
+}
+
+int cansfz_chkdiv(cansfz_ctx* c, const double* u, const double* v, const double* w, double* divtot, double* divmax) {
+  if (!c || !divtot || !divmax) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  if (int rc = call_scalars(c, h)) return rc;
+  launch_chkdiv(c->L, c->g, c->sc_call, c->partial, u, v, w, false);
+  DevScalars r{};
+  CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *divtot = r.divtot;
+  *divmax = r.divmax;
+  return CANSFZ_OK;
+}
+
+int cansfz_bulk_mean_12_stag(cansfz_ctx* c, int idir, const double* psi, double* mean) {
+  if (!c || !mean || idir < 1 || idir > 3) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  if (int rc = call_scalars(c, h)) return rc;
+  const double* gvr = c->d_grid + (idir == 3 ? 5 : 4) * (c->g.nz + 2);
+  launch_bulk_mean(c->L, c->g, c->ph, c->sc_call, c->partial, idir, gvr, psi);
+  DevScalars r{};
+  CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *mean = r.rho_av[idir - 1];
+  return CANSFZ_OK;
+}
+
+int cansfz_cmpt_mean_mass(cansfz_ctx* c, const double* psi, double mass12[2]) {
+  if (!c || !mass12) return CANSFZ_ERR_ARG;
+  launch_mass(c->L, c->g, c->ph, c->sc_call, c->partial, psi, c->P.l[0] * c->P.l[1] * c->P.l[2]);
+  DevScalars r{};
+  CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  mass12[0] = r.mass12[0];
+  mass12[1] = r.mass12[1];
+  return CANSFZ_OK;
+}
+
+// Library-only controls used by the Python host (not reference procedures).
+int cansfz_set_time(cansfz_ctx* c, double time, long long istep) {
+  if (!c) return CANSFZ_ERR_ARG;
+  if (int rc = sync_status(c)) return rc;
+  c->sc_host->time = time;
+  c->sc_host->istep = istep;
+  if (int rc = upload_scalars(c, c->sc, *c->sc_host)) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return CANSFZ_OK;
+}
+
+int cansfz_set_inivel(cansfz_ctx* c, const char* inivel) {
+  if (!c || !inivel) return CANSFZ_ERR_ARG;
+  std::snprintf(c->inivel, sizeof(c->inivel), "%s", inivel);
+  for (auto& ge : c->gexec)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  return CANSFZ_OK;
+}
+
+}  // extern "C"

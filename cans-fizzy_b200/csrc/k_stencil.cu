@@ -1,0 +1,1025 @@
+// Stencil, update and reduction kernels of the per-step hot path (FP64).
+//
+// Index convention: Fortran indices of the reference, interior 1..n, ghosts
+// 0 and n+1, halo-layout strides from Geo.  Each kernel cites the reference
+// loop it computes; expressions keep the reference's operation order.
+#include <cfloat>
+
+#include "cansfz_internal.cuh"
+
+namespace cansfz {
+
+#define HALTED(sc) ((sc) != nullptr && (sc)->halted)
+
+static inline dim3 blk_interior(const Geo& g) {
+  int bx = g.nx >= 128 ? 128 : (g.nx >= 64 ? 64 : 32);
+  return dim3(bx);
+}
+static inline dim3 grd_interior(const Geo& g, dim3 b) {
+  return dim3((g.nx + b.x - 1) / b.x, g.ny, g.nz);
+}
+#define INTERIOR_IJK(g)                                   \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1; \
+  if (i > (g).nx) return;                                 \
+  const int j = blockIdx.y + 1;                           \
+  const int k = blockIdx.z + 1;
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+#define LD(p, q) __ldg((p) + (q))
+
+// ---------------------------------------------------------------------------
+// acdi_transport_pf, src/acdi.f90:64-225
+// ---------------------------------------------------------------------------
+// UPD: rk_2fl fused in (src/rk.f90:234-248): psi_out = clip(psi + f1*d + f2*d_old),
+// the history slot `dpsidt` holds d_old on entry and d on exit.
+template <bool SDF, bool UPD>
+__global__ void __launch_bounds__(128) k_acdi_transport(Geo g, const DevScalars* __restrict__ sc,
+    const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+    const double* __restrict__ nx_, const double* __restrict__ ny_, const double* __restrict__ nz_,
+    const double* __restrict__ phi, const double* __restrict__ psi, double* __restrict__ dpsidt,
+    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ psi_out) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const double gam = sc->gam, seps = sc->seps;
+  const double dxi = g.dxi, dyi = g.dyi;
+  const double dzfi_c = g.dzfi[k], dzci_c = g.dzci[k], dzci_m = g.dzci[k - 1];
+  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
+  const double psi_ccm = LD(psi, c - sxy), psi_cmc = LD(psi, c - sx), psi_mcc = LD(psi, c - 1),
+               psi_ccc = LD(psi, c), psi_pcc = LD(psi, c + 1), psi_cpc = LD(psi, c + sx),
+               psi_ccp = LD(psi, c + sxy);
+  const double u_mcc = LD(u, c - 1), u_ccc = LD(u, c);
+  const double v_cmc = LD(v, c - sx), v_ccc = LD(v, c);
+  const double w_ccm = LD(w, c - sxy), w_ccc = LD(w, c);
+  const double nxc = LD(nx_, c), nyc = LD(ny_, c), nzc = LD(nz_, c);
+  const int off[6] = {-1, 1, -sx, sx, -sxy, sxy};
+  double nxf[6], nyf[6], nzf[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    nxf[q] = 0.5 * (LD(nx_, c + off[q]) + nxc);
+    nyf[q] = 0.5 * (LD(ny_, c + off[q]) + nyc);
+    nzf[q] = 0.5 * (LD(nz_, c + off[q]) + nzc);
+  }
+  // advection
+  const double upsiim = 0.5 * (psi_mcc + psi_ccc) * u_mcc;
+  const double upsiip = 0.5 * (psi_pcc + psi_ccc) * u_ccc;
+  const double vpsijm = 0.5 * (psi_cmc + psi_ccc) * v_cmc;
+  const double vpsijp = 0.5 * (psi_cpc + psi_ccc) * v_ccc;
+  const double wpsikm = 0.5 * (psi_ccm + psi_ccc) * w_ccm;
+  const double wpsikp = 0.5 * (psi_ccp + psi_ccc) * w_ccc;
+  const double adv = dxi * (upsiip - upsiim) + dyi * (vpsijp - vpsijm) + dzfi_c * (wpsikp - wpsikm);
+  // diffusion
+  const double gs = gam * seps;
+  const double dpsidxm = gs * (psi_ccc - psi_mcc) * dxi;
+  const double dpsidxp = gs * (psi_pcc - psi_ccc) * dxi;
+  const double dpsidym = gs * (psi_ccc - psi_cmc) * dyi;
+  const double dpsidyp = gs * (psi_cpc - psi_ccc) * dyi;
+  const double dpsidzm = gs * (psi_ccc - psi_ccm) * dzci_m;
+  const double dpsidzp = gs * (psi_ccp - psi_ccc) * dzci_c;
+  // sharpening: face-normal component of the averaged normal, normalised
+  const double rn_01 = nxf[0] / (sqrt(sq(nxf[0]) + sq(nyf[0]) + sq(nzf[0])) + CANSFZ_EPS);
+  const double rn_11 = nxf[1] / (sqrt(sq(nxf[1]) + sq(nyf[1]) + sq(nzf[1])) + CANSFZ_EPS);
+  const double rn_02 = nyf[2] / (sqrt(sq(nxf[2]) + sq(nyf[2]) + sq(nzf[2])) + CANSFZ_EPS);
+  const double rn_12 = nyf[3] / (sqrt(sq(nxf[3]) + sq(nyf[3]) + sq(nzf[3])) + CANSFZ_EPS);
+  const double rn_03 = nzf[4] / (sqrt(sq(nxf[4]) + sq(nyf[4]) + sq(nzf[4])) + CANSFZ_EPS);
+  const double rn_13 = nzf[5] / (sqrt(sq(nxf[5]) + sq(nyf[5]) + sq(nzf[5])) + CANSFZ_EPS);
+  double sharpxm, sharpxp, sharpym, sharpyp, sharpzm, sharpzp;
+  if (SDF) {
+    const double phi_ccc = LD(phi, c);
+    const double qg = 0.25 * gam;
+    sharpxm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - 1)) / seps))) * rn_01);
+    sharpxp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + 1) + phi_ccc) / seps))) * rn_11);
+    sharpym = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sx)) / seps))) * rn_02);
+    sharpyp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sx) + phi_ccc) / seps))) * rn_12);
+    sharpzm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sxy)) / seps))) * rn_03);
+    sharpzp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sxy) + phi_ccc) / seps))) * rn_13);
+  } else {
+    const double psi_xm = 0.5 * (psi_ccc + psi_mcc), psi_xp = 0.5 * (psi_pcc + psi_ccc);
+    const double psi_ym = 0.5 * (psi_ccc + psi_cmc), psi_yp = 0.5 * (psi_cpc + psi_ccc);
+    const double psi_zm = 0.5 * (psi_ccc + psi_ccm), psi_zp = 0.5 * (psi_ccp + psi_ccc);
+    sharpxm = gam * psi_xm * (1. - psi_xm) * rn_01;
+    sharpxp = gam * psi_xp * (1. - psi_xp) * rn_11;
+    sharpym = gam * psi_ym * (1. - psi_ym) * rn_02;
+    sharpyp = gam * psi_yp * (1. - psi_yp) * rn_12;
+    sharpzm = gam * psi_zm * (1. - psi_zm) * rn_03;
+    sharpzp = gam * psi_zp * (1. - psi_zp) * rn_13;
+  }
+  const double rglrxm = dpsidxm - sharpxm, rglrxp = dpsidxp - sharpxp;
+  const double rglrym = dpsidym - sharpym, rglryp = dpsidyp - sharpyp;
+  const double rglrzm = dpsidzm - sharpzm, rglrzp = dpsidzp - sharpzp;
+  const double rglr = (rglrxp - rglrxm) * dxi + (rglryp - rglrym) * dyi + (rglrzp - rglrzm) * dzfi_c;
+  const double d = -adv + rglr;
+  if (UPD) {
+    const int t = g.t(i, j, k);
+    const double dO = sc->first_rk2fl ? d : dpsidt[t];
+    psi_out[c] = fmin(fmax(0., psi_ccc + sc->f1 * d + sc->f2 * dO), 1.);
+    dpsidt[t] = d;
+  } else {
+    dpsidt[g.t(i, j, k)] = d;
+  }
+  fx[c] = upsiip - rglrxp;
+  fy[c] = vpsijp - rglryp;
+  fz[c] = wpsikp - rglrzp;
+}
+
+void launch_acdi_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                           const double* u, const double* v, const double* w, const double* nx,
+                           const double* ny, const double* nz, const double* phi, const double* psi,
+                           double* dpsidt, double* fx, double* fy, double* fz) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  if (sdf)
+    k_acdi_transport<true, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, dpsidt, fx, fy, fz,
+                                                      nullptr);
+  else
+    k_acdi_transport<false, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, dpsidt, fx, fy, fz,
+                                                       nullptr);
+}
+
+void launch_acdi_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
+                      const double* v, const double* w, const double* nx, const double* ny, const double* nz,
+                      const double* phi, const double* psi, double* psi_out, double* hist, double* fx, double* fy,
+                      double* fz) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  if (sdf)
+    k_acdi_transport<true, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz,
+                                                     psi_out);
+  else
+    k_acdi_transport<false, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz,
+                                                      psi_out);
+}
+
+// ---------------------------------------------------------------------------
+// vof_thinc_transport_psi, src/vof_thinc_qq.f90:39-133: fluxes over faces
+// 0..n, then the flux divergence on the interior.
+// ---------------------------------------------------------------------------
+template <bool SDF>
+__global__ void k_thinc_flux(Geo g, const DevScalars* __restrict__ sc,
+    const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+    const double* __restrict__ nx_, const double* __restrict__ ny_, const double* __restrict__ nz_,
+    const double* __restrict__ phi, const double* __restrict__ psi,
+    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0..n
+  if (i > g.nx) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const double beta = sc->beta;
+  const int c = g.h(i, j, k);
+  const double vel_x = LD(u, c), vel_y = LD(v, c), vel_z = LD(w, c);
+  int ci, cj, ck;
+  double xx, yy, zz;
+  if (vel_x > 0.) { ci = c; xx = 0.5; } else { ci = c + 1; xx = -0.5; }
+  if (vel_y > 0.) { cj = c; yy = 0.5; } else { cj = c + g.sx; yy = -0.5; }
+  if (vel_z > 0.) { ck = c; zz = 0.5; } else { ck = c + g.sxy; zz = -0.5; }
+  const double lnormx_x = LD(nx_, ci), lnormy_y = LD(ny_, cj), lnormz_z = LD(nz_, ck);
+  double d_x, d_y, d_z;
+  if (SDF) {
+    d_x = LD(phi, ci); d_y = LD(phi, cj); d_z = LD(phi, ck);
+  } else {
+    const double hb = -.5 / beta;
+    d_x = hb * log(1. / (LD(psi, ci) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
+    d_y = hb * log(1. / (LD(psi, cj) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
+    d_z = hb * log(1. / (LD(psi, ck) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
+  }
+  const double m2b = -2. * beta;
+  fx[c] = vel_x * (1. / (1. + exp(m2b * (lnormx_x * xx + d_x))));
+  fy[c] = vel_y * (1. / (1. + exp(m2b * (lnormy_y * yy + d_y))));
+  fz[c] = vel_z * (1. / (1. + exp(m2b * (lnormz_z * zz + d_z))));
+}
+
+__global__ void k_thinc_div(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ fx,
+                            const double* __restrict__ fy, const double* __restrict__ fz,
+                            double* __restrict__ dpsidt) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k);
+  dpsidt[g.t(i, j, k)] = -(g.dxi * (LD(fx, c) - LD(fx, c - 1)) + g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
+                           g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
+}
+
+// flux divergence + rk_2fl update (history in place), src/vof_thinc_qq.f90:122-132, src/rk.f90:240-248
+__global__ void k_thinc_div_update(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ fx,
+                                   const double* __restrict__ fy, const double* __restrict__ fz,
+                                   const double* __restrict__ psi, double* __restrict__ hist,
+                                   double* __restrict__ psi_out) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double d = -(g.dxi * (LD(fx, c) - LD(fx, c - 1)) + g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
+                     g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
+  const double dO = sc->first_rk2fl ? d : hist[t];
+  psi_out[c] = fmin(fmax(0., LD(psi, c) + sc->f1 * d + sc->f2 * dO), 1.);
+  hist[t] = d;
+}
+
+void launch_thinc_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
+                       const double* v, const double* w, const double* nx, const double* ny, const double* nz,
+                       const double* phi, const double* psi, double* psi_out, double* hist, double* fx, double* fy,
+                       double* fz) {
+  dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
+  if (sdf) k_thinc_flux<true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  else k_thinc_flux<false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
+  k_thinc_div_update<<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, psi, hist, psi_out);
+}
+
+void launch_thinc_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
+                            const double* u, const double* v, const double* w, const double* nx,
+                            const double* ny, const double* nz, const double* phi, const double* psi,
+                            double* dpsidt, double* fx, double* fy, double* fz) {
+  dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
+  if (sdf) k_thinc_flux<true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  else k_thinc_flux<false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
+  k_thinc_div<<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, dpsidt);
+}
+
+// ---------------------------------------------------------------------------
+// rk_2fl update + clip, src/rk.f90:234-248 (the clip of the halo is dropped:
+// every ghost cell is overwritten by boundp(psi) right after)
+// ---------------------------------------------------------------------------
+__global__ void k_psi_update(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ psi_in,
+                             double* __restrict__ psi_out, const double* __restrict__ dn,
+                             double* __restrict__ dold) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double d = dn[t];
+  const double dO = sc->first_rk2fl ? d : dold[t];
+  const double val = LD(psi_in, c) + sc->f1 * d + sc->f2 * dO;
+  psi_out[c] = fmin(fmax(0., val), 1.);
+}
+
+void launch_psi_update(const Launch& L, const Geo& g, const DevScalars* sc, const double* psi_in,
+                       double* psi_out, double* dpsidt, double* dpsidto) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_psi_update<<<gr, b, 0, L.st>>>(g, sc, psi_in, psi_out, dpsidt, dpsidto);
+}
+
+// ---------------------------------------------------------------------------
+// acdi_cmpt_phi (src/acdi.f90:227-248), vof_thinc_cmpt_phi
+// (src/vof_thinc_qq.f90:135-157): whole halo array
+// ---------------------------------------------------------------------------
+template <bool ACDI>
+__global__ void k_cmpt_phi(int n, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
+                           double* __restrict__ phi) {
+  if (HALTED(sc)) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const double ps = LD(psi, q);
+  if (ACDI) {
+    phi[q] = sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS));
+  } else {
+    const double pa = fmin(fmax(ps, CANSFZ_EPS), 1. - CANSFZ_EPS);
+    phi[q] = 0.5 / sc->beta * log(pa / (1. - pa));
+  }
+}
+
+void launch_cmpt_phi(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
+                     double* phi) {
+  const int n = g.hsize();
+  if (acdi) k_cmpt_phi<true><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  else k_cmpt_phi<false><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+}
+
+// ---------------------------------------------------------------------------
+// cmpt_norm_curv_youngs, src/two_fluid.f90:60-175
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_youngs(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
+                                                double* __restrict__ normx, double* __restrict__ normy,
+                                                double* __restrict__ normz, double* __restrict__ kappa) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
+#define PS(a, b, cc) LD(psi, c + (a) + (b) * sx + (cc) * sxy)
+  const double psimmm = PS(-1, -1, -1), psimcm = PS(-1, 0, -1), psimpm = PS(-1, 1, -1),
+               psicmm = PS(0, -1, -1), psiccm = PS(0, 0, -1), psicpm = PS(0, 1, -1),
+               psipmm = PS(1, -1, -1), psipcm = PS(1, 0, -1), psippm = PS(1, 1, -1),
+               psimmc = PS(-1, -1, 0), psimcc = PS(-1, 0, 0), psimpc = PS(-1, 1, 0),
+               psicmc = PS(0, -1, 0), psiccc = PS(0, 0, 0), psicpc = PS(0, 1, 0),
+               psipmc = PS(1, -1, 0), psipcc = PS(1, 0, 0), psippc = PS(1, 1, 0),
+               psimmp = PS(-1, -1, 1), psimcp = PS(-1, 0, 1), psimpp = PS(-1, 1, 1),
+               psicmp = PS(0, -1, 1), psiccp = PS(0, 0, 1), psicpp = PS(0, 1, 1),
+               psipmp = PS(1, -1, 1), psipcp = PS(1, 0, 1), psippp = PS(1, 1, 1);
+#undef PS
+  const double d1 = g.dxi, d2 = g.dyi, zc = g.dzci[k], zm = g.dzci[k - 1];
+  double mx[8], my[8], mz[8];
+  mx[0] = 0.25 * ((psipcc + psippc + psipcp + psippp) - (psiccc + psicpc + psiccp + psicpp)) * d1;
+  mx[1] = 0.25 * ((psipcc + psipmc + psipcp + psipmp) - (psiccc + psicmc + psiccp + psicmp)) * d1;
+  mx[2] = 0.25 * ((psipcc + psippc + psipcm + psippm) - (psiccc + psicpc + psiccm + psicpm)) * d1;
+  mx[3] = 0.25 * ((psipcc + psipmc + psipcm + psipmm) - (psiccc + psicmc + psiccm + psicmm)) * d1;
+  mx[4] = 0.25 * ((psiccc + psicpc + psiccp + psicpp) - (psimcc + psimpc + psimcp + psimpp)) * d1;
+  mx[5] = 0.25 * ((psiccc + psicmc + psiccp + psicmp) - (psimcc + psimmc + psimcp + psimmp)) * d1;
+  mx[6] = 0.25 * ((psiccc + psicpc + psiccm + psicpm) - (psimcc + psimpc + psimcm + psimpm)) * d1;
+  mx[7] = 0.25 * ((psiccc + psicmc + psiccm + psicmm) - (psimcc + psimmc + psimcm + psimmm)) * d1;
+  my[0] = 0.25 * ((psicpc + psippc + psicpp + psippp) - (psiccc + psipcc + psiccp + psipcp)) * d2;
+  my[1] = 0.25 * ((psiccc + psipcc + psiccp + psipcp) - (psicmc + psipmc + psicmp + psipmp)) * d2;
+  my[2] = 0.25 * ((psicpc + psippc + psicpm + psippm) - (psiccc + psipcc + psiccm + psipcm)) * d2;
+  my[3] = 0.25 * ((psiccc + psipcc + psiccm + psipcm) - (psicmc + psipmc + psicmm + psipmm)) * d2;
+  my[4] = 0.25 * ((psicpc + psimpc + psicpp + psimpp) - (psiccc + psimcc + psiccp + psimcp)) * d2;
+  my[5] = 0.25 * ((psiccc + psimcc + psiccp + psimcp) - (psicmc + psimmc + psicmp + psimmp)) * d2;
+  my[6] = 0.25 * ((psicpc + psimpc + psicpm + psimpm) - (psiccc + psimcc + psiccm + psimcm)) * d2;
+  my[7] = 0.25 * ((psiccc + psimcc + psiccm + psimcm) - (psicmc + psimmc + psicmm + psimmm)) * d2;
+  mz[0] = 0.25 * ((psiccp + psipcp + psicpp + psippp) - (psiccc + psipcc + psicpc + psippc)) * zc;
+  mz[1] = 0.25 * ((psiccp + psipcp + psicmp + psipmp) - (psiccc + psipcc + psicmc + psipmc)) * zc;
+  mz[2] = 0.25 * ((psiccc + psipcc + psicpc + psippc) - (psiccm + psipcm + psicpm + psippm)) * zm;
+  mz[3] = 0.25 * ((psiccc + psipcc + psicmc + psipmc) - (psiccm + psipcm + psicmm + psipmm)) * zm;
+  mz[4] = 0.25 * ((psiccp + psimcp + psicpp + psimpp) - (psiccc + psimcc + psicpc + psimpc)) * zc;
+  mz[5] = 0.25 * ((psiccp + psimcp + psicmp + psimmp) - (psiccc + psimcc + psicmc + psimmc)) * zc;
+  mz[6] = 0.25 * ((psiccc + psimcc + psicpc + psimpc) - (psiccm + psimcm + psicpm + psimpm)) * zm;
+  mz[7] = 0.25 * ((psiccc + psimcc + psicmc + psimmc) - (psiccm + psimcm + psicmm + psimmm)) * zm;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const double norm = sqrt(sq(mx[q]) + sq(my[q]) + sq(mz[q])) + CANSFZ_EPS;
+    mx[q] = mx[q] / norm; my[q] = my[q] / norm; mz[q] = mz[q] / norm;
+  }
+  const double norm_x = .125 * (mx[0] + mx[1] + mx[2] + mx[3] + mx[4] + mx[5] + mx[6] + mx[7]);
+  const double norm_y = .125 * (my[0] + my[1] + my[2] + my[3] + my[4] + my[5] + my[6] + my[7]);
+  const double norm_z = .125 * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
+  const double norm = sqrt(sq(norm_x) + sq(norm_y) + sq(norm_z)) + CANSFZ_EPS;
+  normx[c] = norm_x / norm;
+  normy[c] = norm_y / norm;
+  normz[c] = norm_z / norm;
+  kappa[c] = -(0.25 * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
+               0.25 * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
+               0.25 * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * g.dzfi[k]);
+}
+
+void launch_youngs(const Launch& L, const Geo& g, const DevScalars* sc, const double* psi, double* nx, double* ny,
+                   double* nz, double* kappa) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_youngs<<<gr, b, 0, L.st>>>(g, sc, psi, nx, ny, nz, kappa);
+}
+
+// clip_field, src/two_fluid.f90:35-58 (whole halo array)
+__global__ void k_clip(int n, double rmin, double rmax, double* __restrict__ p) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) p[q] = fmin(fmax(rmin, p[q]), rmax);
+}
+void launch_clip(const Launch& L, const Geo& g, double rmin, double rmax, double* p) {
+  const int n = g.hsize();
+  k_clip<<<(n + 255) / 256, 256, 0, L.st>>>(n, rmin, rmax, p);
+}
+
+// ---------------------------------------------------------------------------
+// momentum: mom_xyz_ad (src/mom.f90:505-851, default diffusion branch)
+// ---------------------------------------------------------------------------
+struct AdOut { double du, dv, dw; };
+
+__device__ __forceinline__ AdOut mom_ad_cell(const Geo& g, const Phys& ph, int i, int j, int k,
+                                             const double* __restrict__ psiflx_x,
+                                             const double* __restrict__ psiflx_y,
+                                             const double* __restrict__ psiflx_z,
+                                             const double* __restrict__ u, const double* __restrict__ v,
+                                             const double* __restrict__ w, const double* __restrict__ psi) {
+  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
+  const double mu = ph.mu12[1], dmu = ph.mu12[0] - ph.mu12[1];
+  const double dxi = g.dxi, dyi = g.dyi;
+  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
+#define A_(f, a, b, cc) LD(f, c + (a) + (b) * sx + (cc) * sxy)
+  const double u_ccm = A_(u, 0, 0, -1), u_cmc = A_(u, 0, -1, 0), u_mcc = A_(u, -1, 0, 0),
+               u_ccc = A_(u, 0, 0, 0), u_pcc = A_(u, 1, 0, 0), u_mpc = A_(u, -1, 1, 0),
+               u_cpc = A_(u, 0, 1, 0), u_mcp = A_(u, -1, 0, 1), u_ccp = A_(u, 0, 0, 1);
+  const double v_ccm = A_(v, 0, 0, -1), v_cmc = A_(v, 0, -1, 0), v_pmc = A_(v, 1, -1, 0),
+               v_mcc = A_(v, -1, 0, 0), v_ccc = A_(v, 0, 0, 0), v_pcc = A_(v, 1, 0, 0),
+               v_cpc = A_(v, 0, 1, 0), v_cmp = A_(v, 0, -1, 1), v_ccp = A_(v, 0, 0, 1);
+  const double w_ccm = A_(w, 0, 0, -1), w_pcm = A_(w, 1, 0, -1), w_cpm = A_(w, 0, 1, -1),
+               w_cmc = A_(w, 0, -1, 0), w_mcc = A_(w, -1, 0, 0), w_ccc = A_(w, 0, 0, 0),
+               w_pcc = A_(w, 1, 0, 0), w_cpc = A_(w, 0, 1, 0), w_ccp = A_(w, 0, 0, 1);
+  const double c_ccm = A_(psi, 0, 0, -1), c_pcm = A_(psi, 1, 0, -1), c_cpm = A_(psi, 0, 1, -1),
+               c_cmc = A_(psi, 0, -1, 0), c_pmc = A_(psi, 1, -1, 0), c_mcc = A_(psi, -1, 0, 0),
+               c_ccc = A_(psi, 0, 0, 0), c_pcc = A_(psi, 1, 0, 0), c_mpc = A_(psi, -1, 1, 0),
+               c_cpc = A_(psi, 0, 1, 0), c_cmp = A_(psi, 0, -1, 1), c_mcp = A_(psi, -1, 0, 1),
+               c_ccp = A_(psi, 0, 0, 1), c_cpp = A_(psi, 0, 1, 1), c_ppc = A_(psi, 1, 1, 0),
+               c_pcp = A_(psi, 1, 0, 1);
+  const double flx_x_mcc = rho * u_mcc + drho * A_(psiflx_x, -1, 0, 0);
+  const double flx_x_ccc = rho * u_ccc + drho * A_(psiflx_x, 0, 0, 0);
+  const double flx_x_pcc = rho * u_pcc + drho * A_(psiflx_x, 1, 0, 0);
+  const double flx_x_mpc = rho * u_mpc + drho * A_(psiflx_x, -1, 1, 0);
+  const double flx_x_cpc = rho * u_cpc + drho * A_(psiflx_x, 0, 1, 0);
+  const double flx_x_mcp = rho * u_mcp + drho * A_(psiflx_x, -1, 0, 1);
+  const double flx_x_ccp = rho * u_ccp + drho * A_(psiflx_x, 0, 0, 1);
+  const double flx_y_cmc = rho * v_cmc + drho * A_(psiflx_y, 0, -1, 0);
+  const double flx_y_ccc = rho * v_ccc + drho * A_(psiflx_y, 0, 0, 0);
+  const double flx_y_cpc = rho * v_cpc + drho * A_(psiflx_y, 0, 1, 0);
+  const double flx_y_pmc = rho * v_pmc + drho * A_(psiflx_y, 1, -1, 0);
+  const double flx_y_pcc = rho * v_pcc + drho * A_(psiflx_y, 1, 0, 0);
+  const double flx_y_cmp = rho * v_cmp + drho * A_(psiflx_y, 0, -1, 1);
+  const double flx_y_ccp = rho * v_ccp + drho * A_(psiflx_y, 0, 0, 1);
+  const double flx_z_ccm = rho * w_ccm + drho * A_(psiflx_z, 0, 0, -1);
+  const double flx_z_ccc = rho * w_ccc + drho * A_(psiflx_z, 0, 0, 0);
+  const double flx_z_ccp = rho * w_ccp + drho * A_(psiflx_z, 0, 0, 1);
+  const double flx_z_pcm = rho * w_pcm + drho * A_(psiflx_z, 1, 0, -1);
+  const double flx_z_pcc = rho * w_pcc + drho * A_(psiflx_z, 1, 0, 0);
+  const double flx_z_cpm = rho * w_cpm + drho * A_(psiflx_z, 0, 1, -1);
+  const double flx_z_cpc = rho * w_cpc + drho * A_(psiflx_z, 0, 1, 0);
+#undef A_
+  const double dzci_c = g.dzci[k], dzci_m = g.dzci[k - 1], dzfi_c = g.dzfi[k], dzfi_p = g.dzfi[k + 1];
+  const double uuip = 0.25 * (flx_x_pcc + flx_x_ccc) * (u_ccc + u_pcc);
+  const double uuim = 0.25 * (flx_x_mcc + flx_x_ccc) * (u_ccc + u_mcc);
+  const double vujp = 0.25 * (flx_y_pcc + flx_y_ccc) * (u_ccc + u_cpc);
+  const double vujm = 0.25 * (flx_y_pmc + flx_y_cmc) * (u_ccc + u_cmc);
+  const double wukp = 0.25 * (flx_z_pcc + flx_z_ccc) * (u_ccc + u_ccp);
+  const double wukm = 0.25 * (flx_z_pcm + flx_z_ccm) * (u_ccc + u_ccm);
+  double dudt_aux = dxi * (-uuip + uuim) + dyi * (-vujp + vujm) + dzfi_c * (-wukp + wukm);
+  const double uvip = 0.25 * (flx_x_ccc + flx_x_cpc) * (v_ccc + v_pcc);
+  const double uvim = 0.25 * (flx_x_mcc + flx_x_mpc) * (v_ccc + v_mcc);
+  const double vvjp = 0.25 * (flx_y_ccc + flx_y_cpc) * (v_ccc + v_cpc);
+  const double vvjm = 0.25 * (flx_y_ccc + flx_y_cmc) * (v_ccc + v_cmc);
+  const double wvkp = 0.25 * (flx_z_ccc + flx_z_cpc) * (v_ccc + v_ccp);
+  const double wvkm = 0.25 * (flx_z_ccm + flx_z_cpm) * (v_ccc + v_ccm);
+  double dvdt_aux = dxi * (-uvip + uvim) + dyi * (-vvjp + vvjm) + dzfi_c * (-wvkp + wvkm);
+  const double uwip = 0.25 * (flx_x_ccc + flx_x_ccp) * (w_ccc + w_pcc);
+  const double uwim = 0.25 * (flx_x_mcc + flx_x_mcp) * (w_ccc + w_mcc);
+  const double vwjp = 0.25 * (flx_y_ccc + flx_y_ccp) * (w_ccc + w_cpc);
+  const double vwjm = 0.25 * (flx_y_cmc + flx_y_cmp) * (w_ccc + w_cmc);
+  const double wwkp = 0.25 * (flx_z_ccc + flx_z_ccp) * (w_ccc + w_ccp);
+  const double wwkm = 0.25 * (flx_z_ccc + flx_z_ccm) * (w_ccc + w_ccm);
+  double dwdt_aux = dxi * (-uwip + uwim) + dyi * (-vwjp + vwjm) + dzci_c * (-wwkp + wwkm);
+  {
+    const double dudxp = (u_pcc - u_ccc) * dxi, dudxm = (u_ccc - u_mcc) * dxi;
+    const double dvdxp = (v_pcc - v_ccc) * dxi, dvdxm = (v_pmc - v_cmc) * dxi;
+    const double dudyp = (u_cpc - u_ccc) * dyi, dudym = (u_ccc - u_cmc) * dyi;
+    const double dudzp = (u_ccp - u_ccc) * dzci_c, dudzm = (u_ccc - u_ccm) * dzci_m;
+    const double dwdxp = (w_pcc - w_ccc) * dxi, dwdxm = (w_pcm - w_ccm) * dxi;
+    const double muxp = mu + dmu * c_pcc, muxm = mu + dmu * c_ccc;
+    const double muyp = mu + dmu * 0.25 * (c_ccc + c_cpc + c_ppc + c_pcc);
+    const double muym = mu + dmu * 0.25 * (c_ccc + c_cmc + c_pmc + c_pcc);
+    const double muzp = mu + dmu * 0.25 * (c_ccc + c_pcc + c_ccp + c_pcp);
+    const double muzm = mu + dmu * 0.25 * (c_ccc + c_pcc + c_ccm + c_pcm);
+    dudt_aux = dudt_aux + dxi * ((dudxp + dudxp) * muxp - (dudxm + dudxm) * muxm) +
+               dyi * ((dudyp + dvdxp) * muyp - (dudym + dvdxm) * muym) +
+               dzfi_c * ((dudzp + dwdxp) * muzp - (dudzm + dwdxm) * muzm);
+  }
+  {
+    const double dvdxp = (v_pcc - v_ccc) * dxi, dvdxm = (v_ccc - v_mcc) * dxi;
+    const double dudyp = (u_cpc - u_ccc) * dyi, dudym = (u_mpc - u_mcc) * dyi;
+    const double dvdyp = (v_cpc - v_ccc) * dyi, dvdym = (v_ccc - v_cmc) * dyi;
+    const double dvdzp = (v_ccp - v_ccc) * dzci_c, dvdzm = (v_ccc - v_ccm) * dzci_m;
+    const double dwdyp = (w_cpc - w_ccc) * dyi, dwdym = (w_cpm - w_ccm) * dyi;
+    const double muxp = mu + dmu * 0.25 * (c_ccc + c_pcc + c_ppc + c_cpc);
+    const double muxm = mu + dmu * 0.25 * (c_ccc + c_mcc + c_mpc + c_cpc);
+    const double muyp = mu + dmu * c_cpc, muym = mu + dmu * c_ccc;
+    const double muzp = mu + dmu * 0.25 * (c_ccc + c_cpc + c_cpp + c_ccp);
+    const double muzm = mu + dmu * 0.25 * (c_ccc + c_cpc + c_cpm + c_ccm);
+    dvdt_aux = dvdt_aux + dxi * ((dvdxp + dudyp) * muxp - (dvdxm + dudym) * muxm) +
+               dyi * ((dvdyp + dvdyp) * muyp - (dvdym + dvdym) * muym) +
+               dzfi_c * ((dvdzp + dwdyp) * muzp - (dvdzm + dwdym) * muzm);
+  }
+  {
+    const double dwdxp = (w_pcc - w_ccc) * dxi, dwdxm = (w_ccc - w_mcc) * dxi;
+    const double dudzp = (u_ccp - u_ccc) * dzci_c, dudzm = (u_mcp - u_mcc) * dzci_c;
+    const double dwdyp = (w_cpc - w_ccc) * dyi, dwdym = (w_ccc - w_cmc) * dyi;
+    const double dvdzp = (v_ccp - v_ccc) * dzci_c, dvdzm = (v_cmp - v_cmc) * dzci_c;
+    const double dwdzp = (w_ccp - w_ccc) * dzfi_p, dwdzm = (w_ccc - w_ccm) * dzfi_c;
+    const double muxp = mu + dmu * 0.25 * (c_ccc + c_pcc + c_ccp + c_pcp);
+    const double muxm = mu + dmu * 0.25 * (c_ccc + c_mcc + c_ccp + c_mcp);
+    const double muyp = mu + dmu * 0.25 * (c_ccc + c_cpc + c_ccp + c_cpp);
+    const double muym = mu + dmu * 0.25 * (c_ccc + c_cmc + c_ccp + c_cmp);
+    const double muzp = mu + dmu * c_ccp, muzm = mu + dmu * c_ccc;
+    dwdt_aux = dwdt_aux + dxi * ((dwdxp + dudzp) * muxp - (dwdxm + dudzm) * muxm) +
+               dyi * ((dwdyp + dvdzp) * muyp - (dwdym + dvdzm) * muym) +
+               dzci_c * ((dwdzp + dwdzp) * muzp - (dwdzm + dwdzm) * muzm);
+  }
+  return {dudt_aux, dvdt_aux, dwdt_aux};
+}
+
+// mom_xyz_oth, src/mom.f90:912-1038 (CONSTANT_COEFFS_POISSON, Brackbill per Phys)
+__device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, double dt_r, const double* rho_av,
+                                              int i, int j, int k, const double* __restrict__ p,
+                                              const double* __restrict__ psi, const double* __restrict__ kappa,
+                                              const double* __restrict__ pn, const double* __restrict__ po) {
+  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
+  const double dxi = g.dxi, dyi = g.dyi, dzci_c = g.dzci[k];
+  const int ccc = g.h(i, j, k), pcc = ccc + 1, cpc = ccc + g.sx, ccp = ccc + g.sxy;
+  const double p_ccc = LD(p, ccc), p_pcc = LD(p, pcc), p_cpc = LD(p, cpc), p_ccp = LD(p, ccp);
+  const double q_ccc = (1. + dt_r) * LD(pn, ccc) - dt_r * LD(po, ccc);
+  const double q_pcc = (1. + dt_r) * LD(pn, pcc) - dt_r * LD(po, pcc);
+  const double q_cpc = (1. + dt_r) * LD(pn, cpc) - dt_r * LD(po, cpc);
+  const double q_ccp = (1. + dt_r) * LD(pn, ccp) - dt_r * LD(po, ccp);
+  const double k_ccc = LD(kappa, ccc), k_pcc = LD(kappa, pcc), k_cpc = LD(kappa, cpc), k_ccp = LD(kappa, ccp);
+  const double c_ccc = LD(psi, ccc), c_pcc = LD(psi, pcc), c_cpc = LD(psi, cpc), c_ccp = LD(psi, ccp);
+  const double psixp = 0.5 * (c_pcc + c_ccc), psiyp = 0.5 * (c_cpc + c_ccc), psizp = 0.5 * (c_ccp + c_ccc);
+  const double rhoxp = rho + drho * psixp, rhoyp = rho + drho * psiyp, rhozp = rho + drho * psizp;
+  const double dpdx = (p_pcc - p_ccc) * dxi, dpdy = (p_cpc - p_ccc) * dyi, dpdz = (p_ccp - p_ccc) * dzci_c;
+  double dudt_aux = ph.bforce[0] + (rhoxp - rho_av[0]) * ph.gacc[0];
+  double dvdt_aux = ph.bforce[1] + (rhoyp - rho_av[1]) * ph.gacc[1];
+  double dwdt_aux = ph.bforce[2] + (rhozp - rho_av[2]) * ph.gacc[2];
+  double skappaxp = 0.5 * (k_pcc + k_ccc) * ph.surf_factor;
+  double skappayp = 0.5 * (k_cpc + k_ccc) * ph.surf_factor;
+  double skappazp = 0.5 * (k_ccp + k_ccc) * ph.surf_factor;
+  if (ph.brackbill) {  // _CAPILLARY_BRACKBILL_NORMALIZATION
+    skappaxp = skappaxp * rhoxp; skappayp = skappayp * rhoyp; skappazp = skappazp * rhozp;
+  }
+  dudt_aux = dudt_aux + skappaxp * (c_pcc - c_ccc) * dxi;
+  dvdt_aux = dvdt_aux + skappayp * (c_cpc - c_ccc) * dyi;
+  dwdt_aux = dwdt_aux + skappazp * (c_ccp - c_ccc) * dzci_c;
+  const double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
+  dudt_aux = dudt_aux - (dpdx_e + rhoxp / ph.rho0 * (dpdx - dpdx_e));
+  dvdt_aux = dvdt_aux - (dpdy_e + rhoyp / ph.rho0 * (dpdy - dpdy_e));
+  dwdt_aux = dwdt_aux - (dpdz_e + rhozp / ph.rho0 * (dpdz - dpdz_e));
+  return {dudt_aux, dvdt_aux, dwdt_aux};
+}
+
+__global__ void __launch_bounds__(128) k_mom_ad(Geo g, Phys ph, const double* __restrict__ fx,
+    const double* __restrict__ fy, const double* __restrict__ fz, const double* __restrict__ u,
+    const double* __restrict__ v, const double* __restrict__ w, const double* __restrict__ psi,
+    double* __restrict__ du, double* __restrict__ dv, double* __restrict__ dw) {
+  INTERIOR_IJK(g)
+  const AdOut r = mom_ad_cell(g, ph, i, j, k, fx, fy, fz, u, v, w, psi);
+  const int t = g.t(i, j, k);
+  du[t] = r.du; dv[t] = r.dv; dw[t] = r.dw;
+}
+
+void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* fx, const double* fy,
+                   const double* fz, const double* u, const double* v, const double* w, const double* psi,
+                   double* du, double* dv, double* dw) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_mom_ad<<<gr, b, 0, L.st>>>(g, ph, fx, fy, fz, u, v, w, psi, du, dv, dw);
+}
+
+__global__ void k_mom_oth(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ p,
+                          const double* __restrict__ psi, const double* __restrict__ kappa,
+                          const double* __restrict__ pn, const double* __restrict__ po,
+                          double* __restrict__ du, double* __restrict__ dv, double* __restrict__ dw) {
+  INTERIOR_IJK(g)
+  const AdOut r = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, pn, po);
+  const int t = g.t(i, j, k);
+  du[t] = r.du; dv[t] = r.dv; dw[t] = r.dw;
+}
+
+void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
+                    const double* psi, const double* kappa, const double* pn, const double* po, double* du,
+                    double* dv, double* dw) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_mom_oth<<<gr, b, 0, L.st>>>(g, ph, sc, p, psi, kappa, pn, po, du, dv, dw);
+}
+
+// rk update 1 (src/rk.f90:86-101): u = u*rho_n/rho_p + (f1 R + f2 Ro)/rho_p; on the
+// first call Ro := R.  The new R is written into the history slot `duo`
+// (the swap of src/rk.f90:106-108 becomes the caller's pointer swap).
+__global__ void k_rk_update1(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ psio,
+                             const double* __restrict__ psi, const double* __restrict__ du,
+                             const double* __restrict__ dv, const double* __restrict__ dw,
+                             double* __restrict__ duo, double* __restrict__ dvo, double* __restrict__ dwo,
+                             double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
+  INTERIOR_IJK(g)
+  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double po_c = LD(psio, c), ps_c = LD(psi, c);
+  const double rhox_n = rho + drho * 0.5 * (po_c + LD(psio, c + 1));
+  const double rhoy_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sx));
+  const double rhoz_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sxy));
+  const double rhox_p = rho + drho * 0.5 * (ps_c + LD(psi, c + 1));
+  const double rhoy_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sx));
+  const double rhoz_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sxy));
+  const double Ru = du[t], Rv = dv[t], Rw = dw[t];
+  const bool first = sc->first_rk;
+  const double Ruo = first ? Ru : duo[t], Rvo = first ? Rv : dvo[t], Rwo = first ? Rw : dwo[t];
+  const double f1 = sc->f1, f2 = sc->f2;
+  u[c] = u[c] * rhox_n / rhox_p + (f1 * Ru + f2 * Ruo) / rhox_p;
+  v[c] = v[c] * rhoy_n / rhoy_p + (f1 * Rv + f2 * Rvo) / rhoy_p;
+  w[c] = w[c] * rhoz_n / rhoz_p + (f1 * Rw + f2 * Rwo) / rhoz_p;
+}
+
+void launch_rk_update1(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* psio,
+                       const double* psi, const double* du, const double* dv, const double* dw, double* duo,
+                       double* dvo, double* dwo, double* u, double* v, double* w) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_rk_update1<<<gr, b, 0, L.st>>>(g, ph, sc, psio, psi, du, dv, dw, duo, dvo, dwo, u, v, w);
+}
+
+// rk update 2 (src/rk.f90:118-130): u = u + f12*R/rho_p
+__global__ void k_rk_update2(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
+                             const double* __restrict__ du, const double* __restrict__ dv,
+                             const double* __restrict__ dw, double* __restrict__ u, double* __restrict__ v,
+                             double* __restrict__ w) {
+  INTERIOR_IJK(g)
+  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double ps_c = LD(psi, c);
+  const double rhox_p = rho + drho * 0.5 * (ps_c + LD(psi, c + 1));
+  const double rhoy_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sx));
+  const double rhoz_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sxy));
+  const double f12 = sc->f12;
+  u[c] = u[c] + f12 * du[t] / rhox_p;
+  v[c] = v[c] + f12 * dv[t] / rhoy_p;
+  w[c] = w[c] + f12 * dw[t] / rhoz_p;
+}
+
+void launch_rk_update2(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* psi,
+                       const double* du, const double* dv, const double* dw, double* u, double* v, double* w) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_rk_update2<<<gr, b, 0, L.st>>>(g, ph, sc, psi, du, dv, dw, u, v, w);
+}
+
+// ---------------------------------------------------------------------------
+// The whole of rk (src/rk.f90:16-131) in one pass per cell: mom_xyz_ad, the
+// first AB2 update with the density ratio, mom_xyz_oth, the second update.
+// Reads u,v,w (13-point), psi (16-point), psio, psiflx_x/y/z, p (= pn, as it
+// is when the driver calls rk), po, kappa and the AB2 history; writes the new
+// velocity into separate buffers and the new history over the old one.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_momentum_fused(Geo g, Phys ph, const DevScalars* __restrict__ sc,
+    const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+    const double* __restrict__ psi, const double* __restrict__ psio, const double* __restrict__ fx,
+    const double* __restrict__ fy, const double* __restrict__ fz, const double* __restrict__ p,
+    const double* __restrict__ po, const double* __restrict__ kappa, double* __restrict__ duo,
+    double* __restrict__ dvo, double* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo,
+    double* __restrict__ wo) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const AdOut r = mom_ad_cell(g, ph, i, j, k, fx, fy, fz, u, v, w, psi);
+  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double po_c = LD(psio, c), ps_c = LD(psi, c);
+  const double rhox_n = rho + drho * 0.5 * (po_c + LD(psio, c + 1));
+  const double rhoy_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sx));
+  const double rhoz_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sxy));
+  const double rhox_p = rho + drho * 0.5 * (ps_c + LD(psi, c + 1));
+  const double rhoy_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sx));
+  const double rhoz_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sxy));
+  const bool first = sc->first_rk;
+  const double Ruo = first ? r.du : duo[t], Rvo = first ? r.dv : dvo[t], Rwo = first ? r.dw : dwo[t];
+  const double f1 = sc->f1, f2 = sc->f2, f12 = sc->f12;
+  double un = LD(u, c) * rhox_n / rhox_p + (f1 * r.du + f2 * Ruo) / rhox_p;
+  double vn = LD(v, c) * rhoy_n / rhoy_p + (f1 * r.dv + f2 * Rvo) / rhoy_p;
+  double wn = LD(w, c) * rhoz_n / rhoz_p + (f1 * r.dw + f2 * Rwo) / rhoz_p;
+  duo[t] = r.du; dvo[t] = r.dv; dwo[t] = r.dw;
+  const AdOut s = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, p, po);
+  uo[c] = un + f12 * s.du / rhox_p;
+  vo[c] = vn + f12 * s.dv / rhoy_p;
+  wo[c] = wn + f12 * s.dw / rhoz_p;
+}
+
+void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
+                           const double* v, const double* w, const double* psi, const double* psio,
+                           const double* fx, const double* fy, const double* fz, const double* p,
+                           const double* po, const double* kappa, double* duo, double* dvo, double* dwo,
+                           double* uo, double* vo, double* wo) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_momentum_fused<<<gr, b, 0, L.st>>>(g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo,
+                                       uo, vo, wo);
+}
+
+// ---------------------------------------------------------------------------
+// fillps, src/fillps.f90:13-51
+// ---------------------------------------------------------------------------
+__global__ void k_fillps(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ u,
+                         const double* __restrict__ v, const double* __restrict__ w, double* __restrict__ p) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const double dti = sc->dti, dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
+  const int c = g.h(i, j, k);
+  p[c] = ph.rho0 * ((LD(w, c) - LD(w, c - g.sxy)) * dti * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * dtidyi +
+                    (LD(u, c) - LD(u, c - 1)) * dtidxi);
+}
+void launch_fillps(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
+                   const double* v, const double* w, double* p) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_fillps<<<gr, b, 0, L.st>>>(g, ph, sc, u, v, w, p);
+}
+
+// ---------------------------------------------------------------------------
+// correc, src/correc.f90:13-67: the three loops, ghost ranges included.
+// One thread per (i,j,k) of the halo array; each component updates over its
+// own index range.
+// ---------------------------------------------------------------------------
+__global__ void k_correc(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ p,
+                         double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > g.nx + 1) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const double dt = sc->dt, rhop = ph.rho0;
+  const int c = g.h(i, j, k);
+  const double pc = LD(p, c);
+  if (i <= g.nx) u[c] = u[c] - dt * g.dxi * (LD(p, c + 1) - pc) / rhop;
+  if (j <= g.ny) v[c] = v[c] - dt * g.dyi * (LD(p, c + g.sx) - pc) / rhop;
+  if (k <= g.nz) w[c] = w[c] - dt * g.dzci[k] * (LD(p, c + g.sxy) - pc) / rhop;
+}
+void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p, double* u,
+                   double* v, double* w) {
+  dim3 b(g.nx + 2 >= 128 ? 128 : 64), gr((g.nx + 2 + b.x - 1) / b.x, g.ny + 2, g.nz + 2);
+  k_correc<<<gr, b, 0, L.st>>>(g, ph, sc, p, u, v, w);
+}
+
+// updatep, src/updatep.f90:13-24
+__global__ void k_updatep_interior(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ phi,
+                                   const double* __restrict__ pp, double* __restrict__ pout) {
+  if (HALTED(sc)) return;
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k);
+  pout[c] = LD(phi, c) + LD(pp, c);
+}
+void launch_updatep_interior(const Launch& L, const Geo& g, const DevScalars* sc, const double* phi,
+                             const double* pp, double* pout) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_updatep_interior<<<gr, b, 0, L.st>>>(g, sc, phi, pp, pout);
+}
+__global__ void k_add_full(int n, const double* __restrict__ pp, double* __restrict__ p) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) p[q] = p[q] + pp[q];
+}
+void launch_updatep_full(const Launch& L, const Geo& g, const double* pp, double* p) {
+  const int n = g.hsize();
+  k_add_full<<<(n + 255) / 256, 256, 0, L.st>>>(n, pp, p);
+}
+__global__ void k_copy(size_t n, const double* __restrict__ s, double* __restrict__ d) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) d[q] = s[q];
+}
+void launch_copy(const Launch& L, size_t n, const double* src, double* dst) {
+  k_copy<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, src, dst);
+}
+__global__ void k_fillv(size_t n, double val, double* __restrict__ d) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) d[q] = val;
+}
+void launch_fill(const Launch& L, size_t n, double val, double* dst) {
+  k_fillv<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, val, dst);
+}
+
+// ---------------------------------------------------------------------------
+// reductions.  Maxima of non-negative doubles via atomicMax on the bit
+// pattern (order independent); sums via per-block partials reduced in a
+// fixed order (deterministic).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double s[32];
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s[wid] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? s[threadIdx.x] : 0.;
+  if (wid == 0) v = warp_max(v);
+  return v;
+}
+// deterministic block sum: fixed tree order for a given blockDim
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double s[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s[wid] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? s[threadIdx.x] : 0.;
+  if (wid == 0) v = warp_sum(v);
+  return v;
+}
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, double v) {
+  atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+// acdi_set_gamma, src/acdi.f90:32-62: max over the interior of |u_c|^2
+__global__ void k_gamma_max(Geo g, DevScalars* __restrict__ sc, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double vel = 0.;
+  if (i <= g.nx) {
+    const int c = g.h(i, j, k);
+    const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
+    const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
+    const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
+    vel = uc * uc + vc * vc + wc * wc;
+  }
+  vel = block_max(vel);
+  if (threadIdx.x == 0) atomic_max_nonneg(&sc->max_bits[0], vel);
+}
+__global__ void k_gamma_final(Phys ph, DevScalars* __restrict__ sc, int apply_floor) {
+  if (HALTED(sc)) return;
+  const double velmax = __longlong_as_double((long long)sc->max_bits[0]);
+  double gam = sqrt(velmax) * ph.gam_factor;
+  if (apply_floor) gam = fmax(gam, ph.gam_min);
+  sc->gam = gam;
+  sc->max_bits[0] = 0ull;
+}
+void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, const double* u, const double* v,
+                  const double* w, bool apply_floor) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_gamma_max<<<gr, b, 0, L.st>>>(g, sc, u, v, w);
+  k_gamma_final<<<1, 1, 0, L.st>>>(ph, sc, apply_floor ? 1 : 0);
+}
+
+// chkdt, src/chkdt.f90:15-94
+__global__ void k_chkdt_max(Geo g, DevScalars* __restrict__ sc, int only_on_check, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double dti = 0.;
+  if (i <= g.nx) {
+    const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
+    const double dxi = 1. / g.dx, dyi = 1. / g.dy;
+    const double ux = fabs(LD(u, c));
+    const double vx = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c + 1) + LD(v, c + 1 - sx));
+    const double wx = 0.25 * fabs(LD(w, c) + LD(w, c - sxy) + LD(w, c + 1) + LD(w, c + 1 - sxy));
+    const double dtix = ux * dxi + vx * dyi + wx * g.dzfi[k];
+    const double uy = 0.25 * fabs(LD(u, c) + LD(u, c + sx) + LD(u, c - 1 + sx) + LD(u, c - 1));
+    const double vy = fabs(LD(v, c));
+    const double wy = 0.25 * fabs(LD(w, c) + LD(w, c + sx) + LD(w, c + sx - sxy) + LD(w, c - sxy));
+    const double dtiy = uy * dxi + vy * dyi + wy * g.dzfi[k];
+    const double uz = 0.25 * fabs(LD(u, c) + LD(u, c - 1) + LD(u, c - 1 + sxy) + LD(u, c + sxy));
+    const double vz = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c - sx + sxy) + LD(v, c + sxy));
+    const double wz = fabs(LD(w, c));
+    const double dtiz = uz * dxi + vz * dyi + wz * g.dzci[k];
+    dti = fmax(dtix, fmax(dtiy, dtiz));
+  }
+  dti = block_max(dti);
+  if (threadIdx.x == 0) atomic_max_nonneg(&sc->max_bits[1], dti);
+}
+// completes chkdt and the dt update of src/main.f90:530-551
+__global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int in_loop) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  double dti = __longlong_as_double((long long)sc->max_bits[1]);
+  sc->max_bits[1] = 0ull;
+  double dtipsi;
+  if (ph.acdi) {
+    dtipsi = sc->gam * sc->seps / (ph.dlmin * ph.dlmin);
+    if (dtipsi == 0.) dtipsi = 1.;
+  } else {
+    dtipsi = dti;
+  }
+  double dtmax;
+  if (!ph.solve_ns) {
+    dtmax = fmin(1. / dti, 1. / dtipsi);
+  } else {
+    const double dtiv = ph.mu_over_rho_max * 2. * (3. / (ph.dlmin * ph.dlmin));
+    const double dtik = sqrt(ph.sigma / ph.rho_min / (ph.dlmin * ph.dlmin * ph.dlmin));
+    const double dtig = ph.gmax / ph.dlmin;
+    dti = 0.5 * (dti + dtiv + sqrt((dti + dtiv) * (dti + dtiv) + 4. * (dtig * dtig + dtik * dtik)));
+    if (dti == 0.) dti = 1.;
+    dtmax = 1. / dti;
+    if (ph.track) dtmax = fmin(dtmax, 1. / dtipsi);
+  }
+  sc->dt_cfl = dtmax;
+  double dt = fmin(ph.cfl * dtmax, ph.dtmax);
+  if (ph.dt_f > 0.) {
+    if (ph.dt_f > dt && in_loop) sc->status = CANSFZ_ERR_DT;
+    else dt = ph.dt_f;
+  }
+  sc->dt = dt;
+  sc->dti = 1. / dt;
+  if (in_loop && dtmax < ph.small) sc->status = CANSFZ_ERR_DT;
+}
+void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, const double* u, const double* v,
+                  const double* w, bool only_on_check) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_chkdt_max<<<gr, b, 0, L.st>>>(g, sc, only_on_check ? 1 : 0, u, v, w);
+  k_chkdt_final<<<1, 1, 0, L.st>>>(ph, sc, only_on_check ? 1 : 0, only_on_check ? 1 : 0);
+}
+
+// chkdiv, src/chkdiv.f90:15-49: per-block partial sums, max via atomics
+__global__ void k_chkdiv_part(Geo g, DevScalars* __restrict__ sc, int only_on_check, double* __restrict__ part,
+                              const double* __restrict__ u, const double* __restrict__ v,
+                              const double* __restrict__ w) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double div = 0.;
+  if (i <= g.nx) {
+    const int c = g.h(i, j, k);
+    div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +
+          (LD(u, c) - LD(u, c - 1)) * g.dxi;
+  }
+  const double m = block_max(fabs(div));
+  const double s = block_sum(div);
+  if (threadIdx.x == 0) {
+    atomic_max_nonneg(&sc->max_bits[2], m);
+    part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+  }
+}
+__global__ void k_sum_partials(int n, const double* __restrict__ part, double* __restrict__ out,
+                               DevScalars* __restrict__ sc, int only_on_check) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  double s = 0.;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) s += part[q];
+  s = block_sum(s);
+  if (threadIdx.x == 0) *out = s;
+}
+__global__ void k_chkdiv_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  sc->divmax = __longlong_as_double((long long)sc->max_bits[2]);
+  sc->max_bits[2] = 0ull;
+  if (only_on_check) {
+    if (isnan(sc->divtot)) sc->status = CANSFZ_ERR_NAN;
+    else if (sc->divmax > ph.small && sc->status == CANSFZ_OK) sc->status = CANSFZ_ERR_DIVERGENCE;
+  }
+}
+void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial, const double* u,
+                   const double* v, const double* w, bool only_on_check) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  const int oc = only_on_check ? 1 : 0;
+  k_chkdiv_part<<<gr, b, 0, L.st>>>(g, sc, oc, partial, u, v, w);
+  k_sum_partials<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, &sc->divtot, sc, oc);
+  Phys ph{};
+  ph.small = CANSFZ_EPS * 1.0e7;
+  k_chkdiv_final<<<1, 1, 0, L.st>>>(ph, sc, oc);
+}
+
+// bulk_mean_12_stag, src/utils.f90:68-136
+__global__ void k_bulk_part(Geo g, Phys ph, const DevScalars* __restrict__ sc, int idir,
+                            const double* __restrict__ gvr, const double* __restrict__ psi,
+                            double* __restrict__ part) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double s = 0.;
+  if (i <= g.nx) {
+    const int c = g.h(i, j, k);
+    double pl;
+    if (idir == 1) pl = 0.5 * (LD(psi, c + 1) + LD(psi, c));
+    else if (idir == 2) pl = 0.5 * (LD(psi, c + g.sx) + LD(psi, c));
+    else pl = 0.5 * (LD(psi, c + g.sxy) + LD(psi, c));
+    s = (pl * ph.rho12[0] + (1. - pl) * ph.rho12[1]) * gvr[k];
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+}
+void launch_bulk_mean(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, int idir,
+                      const double* gvr, const double* psi) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_bulk_part<<<gr, b, 0, L.st>>>(g, ph, sc, idir, gvr, psi, partial);
+  k_sum_partials<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, &sc->rho_av[idir - 1], sc, 0);
+}
+
+// cmpt_mean_mass, src/output.f90:759-790
+__global__ void k_mass_part(Geo g, Phys ph, const double* __restrict__ psi, double* __restrict__ part) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double m1 = 0., m2 = 0.;
+  if (i <= g.nx) {
+    const double vcell = g.dx * g.dy * g.dzf[k];
+    const double ps = LD(psi, g.h(i, j, k));
+    m1 = ph.rho12[0] * ps * vcell;
+    m2 = ph.rho12[1] * (1. - ps) * vcell;
+  }
+  m1 = block_sum(m1);
+  m2 = block_sum(m2);
+  if (threadIdx.x == 0) {
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    part[bid] = m1;
+    part[nb + bid] = m2;
+  }
+}
+__global__ void k_mass_final(int nb, const double* __restrict__ part, DevScalars* __restrict__ sc, double vol) {
+  double s1 = 0., s2 = 0.;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) { s1 += part[q]; s2 += part[nb + q]; }
+  s1 = block_sum(s1);
+  s2 = block_sum(s2);
+  if (threadIdx.x == 0) { sc->mass12[0] = s1 / vol; sc->mass12[1] = s2 / vol; }
+}
+void launch_mass(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, const double* psi,
+                 double vol) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_mass_part<<<gr, b, 0, L.st>>>(g, ph, psi, partial);
+  k_mass_final<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, sc, vol);
+}
+
+// ---------------------------------------------------------------------------
+// step bookkeeping, src/main.f90:414-425 and :515-529
+// ---------------------------------------------------------------------------
+__global__ void k_step_begin(DevScalars* sc, int icheck) {
+  if (sc->status != CANSFZ_OK) sc->halted = 1;
+  if (sc->halted) return;
+  sc->istep = sc->istep + 1;
+  sc->time = sc->time + sc->dt;
+  const double dt_r = sc->dt / sc->dto;
+  sc->dt_r = dt_r;
+  sc->tm1 = 1. + 0.5 * dt_r;
+  sc->tm2 = -0.5 * dt_r;
+  sc->f1 = sc->tm1 * sc->dt;
+  sc->f2 = sc->tm2 * sc->dt;
+  sc->f12 = sc->f1 + sc->f2;
+  sc->dti = 1. / sc->dt;
+  sc->check_now = (icheck > 0 && (sc->istep % icheck) == 0) ? 1 : 0;
+}
+void launch_step_begin(const Launch& L, DevScalars* sc, int icheck) {
+  k_step_begin<<<1, 1, 0, L.st>>>(sc, icheck);
+}
+__global__ void k_step_end(DevScalars* sc) {
+  if (sc->halted) return;
+  sc->dto = sc->dt;
+  sc->first_rk = 0;
+  sc->first_rk2fl = 0;
+}
+void launch_step_end(const Launch& L, const Phys& ph, DevScalars* sc) {
+  (void)ph;
+  k_step_end<<<1, 1, 0, L.st>>>(sc);
+}
+
+}  // namespace cansfz

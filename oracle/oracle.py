@@ -145,7 +145,8 @@ class Case:
 
     def init2fl(self, inipsi: str, spheres=None):
         sph = np.zeros((0, 4)) if spheres is None else np.ascontiguousarray(spheres, dtype=np.float64)
-        lib().orc_init2fl(self.h, inipsi.encode(), ptr(sph) if sph.size else None, int(sph.shape[0]))
+        lib().orc_init2fl(self.h, inipsi.encode(), sph.ctypes.data_as(P) if sph.size else None,  # rows (x,y,z,r)
+                          int(sph.shape[0]))
 
     def initflow(self, inivel: str, time: float = 0.0):
         lib().orc_initflow(self.h, inivel.encode(), float(time))

@@ -1,0 +1,314 @@
+"""Parity of the CUDA path (libcansfz, through the C ABI) against the oracle
+on the same seeded inputs.
+
+Tolerances (FP64): per-procedure stencils 1e-13 relative to the field's max;
+the Poisson solve 1e-11 (pressure compared minus its mean: the
+all-Neumann/periodic zero mode is fixed by the eps-shifted pivot, an
+implementation-dependent constant); whole steps 1e-11 relative in u, v, w,
+psi, p - mean(p) and in the SDF phi where 0.01 < psi < 0.99.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from cansfz import case as C
+from cansfz import init, namelist, params
+
+pytestmark = pytest.mark.gpu
+
+
+def _nml(nx, ny, nz, cbcpre="PPPPNN", l=(1.0, 1.0, 1.0), gr=0.0, extra2f="", vof=False, extra_dns=""):
+    cp = list(cbcpre)
+    lines = ["&dns", f"ng(1:3) = {nx}, {ny}, {nz}", f"l(1:3) = {l[0]}, {l[1]}, {l[2]}",
+             f"gr = {gr}", "cfl = 0.5, dtmax = 1.e9, icheck = 5", extra_dns]
+    for ivel in range(3):
+        vals = []
+        for d in range(3):
+            a, b = cp[2 * d], cp[2 * d + 1]
+            if a == "P":
+                vals += ["'P'", "'P'"]
+            else:
+                # walls: no-slip (D) for all components where the pressure is Neumann
+                t = "D" if a == "N" else ("D" if d == ivel else "N")
+                vals += [f"'{t}'", f"'{t}'"]
+        lines.append(f"cbcvel(0:1,1:3,{ivel + 1}) = " + ", ".join(vals))
+    lines.append("cbcpre(0:1,1:3) = " + ", ".join(f"'{c}'" for c in cp))
+    lines.append("gacc(1:3) = 0., 0., -0.98")
+    lines.append("/")
+    psibc = ["'P'" if c == "P" else "'N'" for c in cp]
+    nor = []
+    for comp in range(3):
+        vals = []
+        for d in range(3):
+            if cp[2 * d] == "P":
+                vals += ["'P'", "'P'"]
+            else:
+                t = "D" if d == comp else "N"
+                vals += [f"'{t}'", f"'{t}'"]
+        nor.append(f"cbcnor(0:1,1:3,{comp + 1}) = " + ", ".join(vals))
+    lines += ["&two_fluid", "inipsi = 'bub3'", "cbcpsi(0:1,1:3) = " + ", ".join(psibc)] + nor
+    lines += ["rho12(1:2) = 1000., 100.", "mu12(1:2) = 10., 1.", "sigma = 24.5",
+              "psi_thickness_factor = 0.51", extra2f, "/"]
+    if vof:
+        lines += ["&cansfz", "interface_capturing_vof = T", "/"]
+    return params.from_namelist(namelist.parse("\n".join(lines)))
+
+
+def _rel(a, b):
+    s = np.abs(b).max()
+    return np.abs(a - b).max() / (s if s > 0 else 1.0)
+
+
+def _rand_fields(p, seed=0, psi_band=True):
+    rng = np.random.default_rng(seed)
+    shp = tuple(x + 2 for x in p.n)
+    f = lambda s=1.0: np.asfortranarray(rng.standard_normal(shp) * s)  # noqa: E731
+    psi = np.asfortranarray(np.clip(0.5 + 0.45 * np.tanh(rng.standard_normal(shp)), 0, 1)) if psi_band else f()
+    return rng, f, psi
+
+
+@pytest.fixture(scope="module")
+def small():
+    p = _nml(24, 16, 20, "PPPPNN", l=(1.0, 0.75, 1.2))
+    return p, C.Case(p), O.Case(p)
+
+
+def test_stencil_procedures(small):
+    p, g, o = small
+    rng, f, psi = _rand_fields(p, 1)
+    u, v, w, nx, ny, nz, phi = f(), f(), f(), f(), f(), f(), f()
+    dpsidt_g, dpsidt_o = g.interior(), np.zeros(p.n, order="F")
+    fo = [o.empty() for _ in range(3)]
+    fg = [g.field() for _ in range(3)]
+    dev = {k: g.field(a) for k, a in dict(u=u, v=v, w=w, nx=nx, ny=ny, nz=nz, phi=phi, psi=psi).items()}
+    gam, seps = 0.7, 0.013
+    g.call("acdi_transport_pf", gam, seps, dev["u"], dev["v"], dev["w"], dev["nx"], dev["ny"], dev["nz"],
+           dev["phi"], dev["psi"], dpsidt_g, *fg)
+    o.call("acdi_transport_pf", gam, seps, u, v, w, nx, ny, nz, phi, psi, dpsidt_o, *fo)
+    assert _rel(dpsidt_g.get(), dpsidt_o) < 1e-13
+    for a, b in zip(fg, fo):
+        assert _rel(a.get()[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]) < 1e-13
+    # THINC
+    beta = 0.98
+    g.call("vof_thinc_transport_psi", beta, dev["u"], dev["v"], dev["w"], dev["nx"], dev["ny"], dev["nz"],
+           dev["phi"], dev["psi"], dpsidt_g, *fg)
+    o.call("vof_thinc_transport_psi", beta, u, v, w, nx, ny, nz, phi, psi, dpsidt_o, *fo)
+    assert _rel(dpsidt_g.get(), dpsidt_o) < 1e-13
+    for a, b in zip(fg, fo):
+        assert _rel(a.get()[:-1, :-1, :-1], b[:-1, :-1, :-1]) < 1e-13
+    # phi (whole halo)
+    phig, phio = g.field(), o.empty()
+    g.call("acdi_cmpt_phi", seps, dev["psi"], phig)
+    o.call("acdi_cmpt_phi", seps, psi, phio)
+    assert _rel(phig.get(), phio) < 1e-13
+    g.call("vof_thinc_cmpt_phi", beta, dev["psi"], phig)
+    o.call("vof_thinc_cmpt_phi", beta, psi, phio)
+    assert _rel(phig.get(), phio) < 1e-13
+    # Youngs normals + curvature
+    outs_g = [g.field() for _ in range(4)]
+    outs_o = [o.empty() for _ in range(4)]
+    g.call("cmpt_norm_curv_youngs", dev["phi"], *outs_g)
+    o.call("cmpt_norm_curv_youngs", phi, *outs_o)
+    for a, b in zip(outs_g, outs_o):
+        assert _rel(a.get()[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]) < 1e-13
+
+
+def test_momentum_procedures(small):
+    p, g, o = small
+    rng, f, psi = _rand_fields(p, 2)
+    u, v, w, fx, fy, fz, pp, pn, po, kap = (f() for _ in range(10))
+    dev = {k: g.field(a) for k, a in dict(u=u, v=v, w=w, fx=fx, fy=fy, fz=fz, p=pp, pn=pn, po=po, k=kap,
+                                           psi=psi).items()}
+    outg = [g.interior() for _ in range(3)]
+    outo = [np.zeros(p.n, order="F") for _ in range(3)]
+    g.call("mom_xyz_ad", dev["fx"], dev["fy"], dev["fz"], dev["u"], dev["v"], dev["w"], dev["psi"], *outg)
+    o.call("mom_xyz_ad", fx, fy, fz, u, v, w, psi, *outo)
+    for a, b in zip(outg, outo):
+        assert _rel(a.get(), b) < 1e-12
+    rho_av = [0.0, 0.0, 3.5]
+    g.call("mom_xyz_oth", 0.9, rho_av, dev["p"], dev["psi"], dev["k"], dev["pn"], dev["po"], *outg)
+    o.call("mom_xyz_oth", 0.9, np.array(rho_av), pp, psi, kap, pn, po, *outo)
+    for a, b in zip(outg, outo):
+        assert _rel(a.get(), b) < 1e-12
+
+
+def test_projection_procedures(small):
+    p, g, o = small
+    rng, f, psi = _rand_fields(p, 3)
+    u, v, w = f(), f(), f()
+    dg = [g.field(a) for a in (u, v, w)]
+    pg, po_ = g.field(), o.empty()
+    g.call("bounduvw", 0, *dg)
+    o.call("bounduvw", 0, u, v, w)
+    for a, b in zip(dg, (u, v, w)):
+        assert _rel(a.get(), b) == 0.0  # ghost fills are copies / exact arithmetic
+    g.call("fillps", 3.7, *dg, pg)
+    o.call("fillps", 3.7, u, v, w, po_)
+    assert _rel(pg.get()[1:-1, 1:-1, 1:-1], po_[1:-1, 1:-1, 1:-1]) < 1e-13
+    pg.set(po_)
+    g.call("solver", pg)
+    o.call("solver", po_)
+    a, b = pg.get()[1:-1, 1:-1, 1:-1], po_[1:-1, 1:-1, 1:-1]
+    assert _rel(a - a.mean(), b - b.mean()) < 1e-11
+    pg.set(po_)
+    g.call("boundp", 0, pg)
+    o.call("boundp", 0, po_)
+    assert _rel(pg.get(), po_) == 0.0
+    g.call("correc", 0.01, pg, *dg)
+    o.call("correc", 0.01, po_, u, v, w)
+    for a, b in zip(dg, (u, v, w)):
+        assert _rel(a.get(), b) < 1e-14
+    g.call("bounduvw", 1, *dg)
+    o.call("bounduvw", 1, u, v, w)
+    for a, b in zip(dg, (u, v, w)):
+        assert _rel(a.get(), b) < 1e-14
+    dt, dm = np.zeros(1), np.zeros(1)
+    g.call("chkdiv", *dg, dt, dm)
+    t2, m2 = np.zeros(1), np.zeros(1)
+    o.call("chkdiv_fields", u, v, w, t2, m2)
+    assert abs(dm[0] - m2[0]) <= 1e-13 * m2[0]
+    gam = np.zeros(1)
+    g.call("acdi_set_gamma", 1.0, *dg, gam)
+    assert abs(gam[0] - o.call("acdi_set_gamma", 1.0, u, v, w)) <= 1e-15 * gam[0]
+    dtm = np.zeros(1)
+    g.call("chkdt", *dg, 0.3, 0.01, dtm)
+    assert abs(dtm[0] - o.call("chkdt_fields", u, v, w, 0.3, 0.01)) <= 1e-14 * dtm[0]
+
+
+@pytest.mark.parametrize("cbcpre", ["PPPPNN", "NNPPNN", "DDPPNN", "PPNNNN", "PPPPPP", "NNNNNN"])
+def test_poisson_bcs(cbcpre):
+    p = _nml(24, 16, 20, cbcpre, l=(1.0, 0.75, 1.2))
+    g, o = C.Case(p), O.Case(p)
+    rng = np.random.default_rng(5)
+    rhs = o.empty()
+    rhs[1:-1, 1:-1, 1:-1] = rng.standard_normal(p.n)
+    if "D" not in cbcpre:
+        rhs[1:-1, 1:-1, 1:-1] -= rhs[1:-1, 1:-1, 1:-1].mean()
+    pg = g.field(rhs)
+    g.call("solver", pg)
+    o.call("solver", rhs)
+    a, b = pg.get()[1:-1, 1:-1, 1:-1], rhs[1:-1, 1:-1, 1:-1]
+    if "D" not in cbcpre:
+        a, b = a - a.mean(), b - b.mean()
+    assert _rel(a, b) < 1e-11, cbcpre
+
+
+@pytest.mark.parametrize("which", [0, 1, 2, 3, 4, 5])
+def test_boundp_all(small, which):
+    p, g, o = small
+    rng, f, psi = _rand_fields(p, 10 + which)
+    a = f()
+    ag = g.field(a)
+    g.call("boundp", which, ag)
+    o.call("boundp", which, a)
+    assert np.array_equal(ag.get(), a)
+
+
+def _run_pair(p, u, v, w, pr, psi, nsteps):
+    g, o = C.Case(p), O.Case(p)
+    g.set_fields(u, v, w, pr, psi)
+    for name, a in zip(("u", "v", "w", "p", "psi"), (u, v, w, pr, psi)):
+        o.set(name, a)
+    g.prepare()
+    o.prepare()
+    rg = g.step(nsteps)
+    ro = o.step(nsteps)
+    return g, o, rg, ro
+
+
+def _check_step(g, o, tol=1e-11):
+    errs = {}
+    for name in ("u", "v", "w", "psi"):
+        errs[name] = _rel(g.get(name), o.get(name))
+    pa, pb = g.get("p")[1:-1, 1:-1, 1:-1], o.get("p")[1:-1, 1:-1, 1:-1]
+    errs["p"] = _rel(pa - pa.mean(), pb - pb.mean())
+    psi = o.get("psi")
+    band = (psi > 0.01) & (psi < 0.99)
+    ph_g, ph_o = g.get("phi"), o.get("phi")
+    errs["phi"] = np.abs(ph_g - ph_o)[band].max() / np.abs(ph_o[band]).max()
+    for k, e in errs.items():
+        assert e < tol, f"{k}: rel err {e:.3e} ({errs})"
+    dg, do = g.diag(), o.diag()
+    assert dg.istep == do.istep and abs(dg.time - do.time) < 1e-14 * max(1.0, do.time)
+    assert abs(dg.dt - do.dt) <= 1e-13 * do.dt
+    return errs
+
+
+def test_step_bubble_3d():
+    """10 steps of a 3-D rising bubble (periodic x,y; walls z)."""
+    p = _nml(32, 32, 48, "PPPPNN", l=(1.0, 1.0, 1.5))
+    psi = init.init2fl(p, "bub3", np.array([[0.5, 0.5, 0.5, 0.25]]))
+    u, v, w, pr = init.initflow(p, "zer")
+    g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
+    assert rg == 0 and ro == 0
+    _check_step(g, o)
+
+
+def test_step_moving_droplets_divfree():
+    """10 steps from a random divergence-free velocity with droplets (dis3)."""
+    p = _nml(32, 32, 32, "PPPPNN")
+    rng = np.random.default_rng(3)
+    eps = init.seps(p)
+    sph = init.place_droplets(rng, 6, 0.08, 0.12, [1, 1, 1], eps)
+    psi = init.init2fl(p, "dis3", sph)
+    u, v, w = init.divfree_velocity(p, rng, 4, 0.1)
+    pr = np.zeros_like(u)
+    g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
+    assert rg == 0 and ro == 0
+    _check_step(g, o)
+
+
+def test_step_stretched_grid():
+    p = _nml(24, 24, 32, "PPPPNN", gr=1.5)
+    rng = np.random.default_rng(4)
+    psi = init.init2fl(p, "dis3", np.array([[0.5, 0.5, 0.5, 0.2]]))
+    u, v, w = init.divfree_velocity(p, rng, 3, 0.1)
+    g, o, rg, ro = _run_pair(p, u, v, w, np.zeros_like(u), psi, 10)
+    assert rg == 0 and ro == 0
+    _check_step(g, o)
+
+
+def test_step_thinc():
+    p = _nml(32, 32, 32, "PPPPNN", vof=True)
+    rng = np.random.default_rng(6)
+    psi = init.init2fl(p, "dis3", np.array([[0.5, 0.5, 0.5, 0.22]]))
+    u, v, w = init.divfree_velocity(p, rng, 3, 0.1)
+    g, o, rg, ro = _run_pair(p, u, v, w, np.zeros_like(u), psi, 10)
+    assert rg == 0 and ro == 0
+    _check_step(g, o)
+
+
+def test_step_rising_bubble_2d_nn_x():
+    """The reference's tests/rising_bubble set-up (64x2x128, Neumann pressure in
+    x -> cosine transforms) for 10 steps, GPU vs oracle."""
+    text = """
+&dns
+ng(1:3) = 64, 2, 128
+l(1:3)  = 1., 0.03125, 2.
+gtype = 1, gr = 0.
+cfl = 0.95, dtmax = 5.e-4, dt_f = -1.
+icheck = 10
+cbcvel(0:1,1:3,1) = 'D','D',  'P','P',  'D','D'
+cbcvel(0:1,1:3,2) = 'N','N',  'P','P',  'D','D'
+cbcvel(0:1,1:3,3) = 'N','N',  'P','P',  'D','D'
+cbcpre(0:1,1:3)   = 'N','N',  'P','P',  'N','N'
+gacc(1:3) = 0., 0., -0.98
+/
+&two_fluid
+inipsi            = 'bub2'
+cbcpsi(0:1,1:3)   = 'N','N',  'P','P',  'N','N'
+cbcnor(0:1,1:3,1) = 'D','D',  'P','P',  'N','N'
+cbcnor(0:1,1:3,2) = 'N','N',  'P','P',  'N','N'
+cbcnor(0:1,1:3,3) = 'N','N',  'P','P',  'D','D'
+rho12(1:2)        =  1000.,100.
+mu12(1:2)         =  10.,1.
+sigma             =  24.5
+psi_thickness_factor = 0.51
+/
+"""
+    p = params.from_namelist(namelist.parse(text))
+    psi = init.init2fl(p, "bub2", np.array([[0.5, 1.0, 0.5, 0.25]]))
+    u, v, w, pr = init.initflow(p, "zer")
+    g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
+    assert rg == 0 and ro == 0
+    _check_step(g, o)
