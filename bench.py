@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the per-time-step hot path: cell-steps/s on the 256^3 ACDI
+droplet workload (64 droplets, density ratio 1000, random divergence-free
+initial velocity), FP64 drop-in form, one GPU per process.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs under torchrun (one process per GPU, NCCL for the barrier and the
+max-over-ranks timing).  The case does not shard across GPUs in this build:
+each rank advances its own replica of the workload (weak scaling, no
+data-path collective).  `--impl reference` times the CPU restatement of the
+reference's algorithm (the reference itself needs a Fortran/MPI/FFTW build
+that this machine cannot make) on the host cores, rank 0 only.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cans-fizzy_b200"))
+
+METRIC = "cell-steps/s at 256^3 ACDI, mixed vs FP64 at stated error; ensemble cases/s"
+WORKLOAD = ("droplets_acdi: 256^3 cells, unit box, periodic x,y, no-slip z walls, 64 droplets R~U[0.03,0.06] "
+            "(seeded rejection sampler), rho 1000/1, mu 100/1, sigma 1, g 1, ACDI, random divergence-free "
+            "u0 (|k|<=4, rms 0.1); AB2 step with FFT Poisson solve")
+DATA = "synthetic (seeded generator, numpy default_rng(2026)); no dataset"
+
+# Algorithmic bytes per cell of each stage of the FP64 step (8 B per access of
+# the persistent state a stage must read or write once; neighbours reused).
+STAGE_BYTES = {
+    # psi, phi, u, v, w, normx/y/z, history (r) + psi_new, history, fx, fy, fz (w)
+    "phase_transport": 8 * (9 + 5),
+    "cmpt_phi": 8 * 2,
+    "youngs": 8 * (1 + 4),
+    # u,v,w, psi, psio, fx,fy,fz, p, po, kappa, 3 histories (r) + 3 histories, u,v,w (w)
+    "momentum": 8 * (14 + 6),
+    "poisson_x_fwd_fillps": 8 * (3 + 1),
+    "poisson_y_fwd": 8 * 2,
+    "poisson_z_solve": 8 * 2,
+    "poisson_y_bwd": 8 * 2,
+    "poisson_x_bwd": 8 * 2,
+    "correc": 8 * (1 + 6),
+    "updatep": 8 * 3,
+    "gamma": 8 * 3,
+}
+B_ALG_STEP = 232  # bytes per cell-step: 19 state accesses + 10 Poisson-pass accesses (FP64)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cansfz", choices=["cansfz", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of timed CPU work (reference arm)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of the SM clock and throttle reasons (200 ms)."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.splitlines():
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) < 9:
+                continue
+            if self.uuid and self.uuid not in cols[0]:
+                continue
+            try:
+                sm.append(float(cols[1]))
+                smax.append(float(cols[2]))
+                power.append(float(cols[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, cols[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        busy = [s for s, p in zip(sm, power) if p > 0.3 * max(power)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax), "samples": len(sm),
+                "power_w_max": max(power), "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus: int):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_run(p, fields, budget_s: float, warmup: int = 1, max_steps: int = 1000):
+    """The CPU restatement (oracle/) on the same workload: warm-up steps, then
+    timed steps until `budget_s` of CPU work; returns (cell-steps/s, steps, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = O.set_threads(os.cpu_count() or 1)
+    c = O.Case(p)
+    for name, a in zip(("u", "v", "w", "p", "psi"), fields):
+        c.set(name, a)
+    c.prepare()
+    if warmup:
+        c.step(warmup)
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps:
+        c.step(1)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    cells = p.ng[0] * p.ng[1] * p.ng[2]
+    return cells * n / dt, n, threads, dt
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+
+    from cansfz import case as C
+    from cansfz import lib as _L
+    from cansfz import workloads as W
+
+    rank, world, local = dist_setup(args.gpus)
+    p, fields = W.droplets_acdi(seed=2026)
+    nx, ny, nz = p.n
+    cells = nx * ny * nz
+    case = C.Case(p)
+    case.set_fields(*fields)
+    case.prepare()
+    rc = case.step(args.warmup)
+    if rc != 0:
+        raise RuntimeError(f"warm-up step failed with status {rc}")
+    stream = case.stream
+    kps = _L.ct.c_int(0)
+    _L.check(case.lib.cansfz_kernels_per_step(case.h, _L.ct.byref(kps)), "kernels_per_step")
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        pass
+    # ---- timed region: K graph-launched steps, device time, max over ranks
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = Clocks(uuid)
+    ev0.record(stream)
+    rc = case.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.stop()
+    if rc != 0:
+        raise RuntimeError(f"timed steps failed with status {rc}")
+    ms = allreduce_max(ev0.elapsed_time(ev1), world)
+    ms_step = ms / args.steps
+    value = cells * args.steps * world / (ms / 1e3)
+    d = case.diag()
+    # ---- stage profile (events between stages, outside the graph)
+    nprof = 5
+    buf = (_L.ct.c_double * 64)()
+    nst = _L.ct.c_int(0)
+    names = _L.ct.create_string_buffer(4096)
+    _L.check(case.lib.cansfz_profile_stages(case.h, nprof, buf, 64, _L.ct.byref(nst), names, 4096), "profile")
+    stage_names = names.value.decode().split(",")
+    stage_ms = {nm: buf[q] / nprof for q, nm in enumerate(stage_names)}
+    tot = sum(stage_ms.values())
+    heavy = [s for s in stage_ms if s in STAGE_BYTES]
+    dom = max(heavy, key=lambda s: stage_ms[s])
+    peak, peak_kind = measured_peaks()
+    bytes_launch = STAGE_BYTES[dom] * cells
+    achieved = bytes_launch / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        if dom in tj:
+            traffic = tj[dom]["bytes_per_cell"] * cells
+    out = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": WORKLOAD, "grid": [nx, ny, nz], "form": "fp64 (drop-in)",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (each FP64 field 137 MB > 126 MB)",
+                   "final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "bytes_per_launch": bytes_launch, "traffic": traffic,
+                     "step_frac": (B_ALG_STEP * cells / (ms_step * 1e-3) / 1e9) / peak},
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "stage_share": {k: round(v / tot, 4) for k, v in stage_ms.items()},
+        "gpu_launches": int(kps.value) * args.steps,
+        "clocks": clocks,
+    }
+    # ---- end to end through the C ABI with pinned host buffers
+    if not args.no_e2e:
+        hshape = tuple(x + 2 for x in p.n)
+        pin = [torch.empty(int(np.prod(hshape)), dtype=torch.float64).pin_memory() for _ in range(5)]
+        for t, a in zip(pin, fields):
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a.reshape(-1, order="F"))))
+        ptrs = [_L.ct.c_void_p(t.data_ptr()) for t in pin]
+        e2e_case = C.Case(p)
+        ksteps = args.steps
+        diag = _L.Diag()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _L.check(e2e_case.lib.cansfz_set_fields(e2e_case.h, *ptrs, 0), "set_fields")
+        _L.check(e2e_case.lib.cansfz_prepare(e2e_case.h), "prepare")
+        for _ in range(ksteps):
+            rc = e2e_case.lib.cansfz_step(e2e_case.h, 1)
+            _L.check(e2e_case.lib.cansfz_get_diag(e2e_case.h, _L.ct.byref(diag)), "get_diag")
+            if rc:
+                break
+        _L.check(e2e_case.lib.cansfz_get_fields(e2e_case.h, *ptrs, 0), "get_fields")
+        torch.cuda.synchronize()
+        te = allreduce_max(time.perf_counter() - t0, world)
+        fb = 8 * int(np.prod(hshape))
+        out["e2e"] = {"value": cells * ksteps * world / te, "unit": "cell-steps/s",
+                      "h2d_bytes_per_step": 5 * fb / ksteps,
+                      "d2h_bytes_per_step": (5 * fb + ksteps * _L.ct.sizeof(_L.Diag)) / ksteps,
+                      "what": "set_fields from pinned host, prepare, K x (cansfz_step(1) + cansfz_get_diag), "
+                              "get_fields to pinned host; wall clock, max over ranks"}
+        e2e_case.close()
+    # ---- CPU baseline (rank 0, N = 1)
+    if world == 1 and not args.no_cpu_baseline:
+        v, n, thr, dt = cpu_run(p, fields, budget_s=15.0, warmup=1, max_steps=20)
+        out["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": thr, "kind": "port",
+                               "sample": f"{n} steps of the same 256^3 workload after 1 warm-up step "
+                                         f"({dt:.1f} s), oracle/ C++ OpenMP restatement"}
+    case.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cansfz import workloads as W
+
+    p, fields = W.droplets_acdi(seed=2026)
+    v, n, thr, dt = cpu_run(p, fields, budget_s=args.cpu_budget, warmup=min(args.warmup, 1),
+                            max_steps=max(args.steps, 1))
+    out = {"metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": 0, "steps": n, "warmup": min(args.warmup, 1),
+           "ms_per_step": 1e3 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": DATA, "impl": "reference",
+           "config": {"workload": WORKLOAD, "grid": list(p.n), "form": "fp64"},
+           "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": thr, "kind": "port",
+                            "sample": f"{n} of the requested {args.steps} steps (time budget {args.cpu_budget:.0f} s)"
+                                      " of the 256^3 workload: the reference is Fortran+MPI+FFTW and cannot be built"
+                                      " here, so its CPU path runs as the C++ OpenMP restatement in oracle/"},
+           "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -198,19 +198,27 @@ def divfree_velocity(p: Params, rng: np.random.Generator, kmax: int = 4, rms: fl
     yf = (np.arange(ny) + 1.0) * dl[1]
     zc = g["zc"][1:-1]
     zf = g["zf"]  # 0..nz+1, zf[0] = 0, zf[nz] = lz
-    A = [np.zeros((nx, ny, nz + 1)), np.zeros((nx, ny, nz + 1)), np.zeros((nx, ny, nz))]
-    modes = [(kx, ky, kz) for kx in range(-kmax, kmax + 1) for ky in range(-kmax, kmax + 1)
-             for kz in range(0, kmax + 1) if 0 < kx * kx + ky * ky + kz * kz <= kmax * kmax]
-    for kx, ky, kz in modes:
-        amp = rng.standard_normal(3) / (1.0 + kx * kx + ky * ky + kz * kz)
-        ph = rng.uniform(0, 2 * np.pi, 3)
-        fx = lambda x, ph_: np.cos(2 * np.pi * kx * x / l[0] + ph_)  # noqa: E731
-        fy = lambda y: np.cos(2 * np.pi * ky * y / l[1])  # noqa: E731
-        szf = np.sin(np.pi * max(kz, 1) * zf[: nz + 1] / l[2])      # 0 on both walls
-        czc = np.cos(np.pi * kz * zc / l[2])
-        A[0] += amp[0] * fx(xc, ph[0])[:, None, None] * fy(yf)[None, :, None] * szf[None, None, :]
-        A[1] += amp[1] * fx(xf, ph[1])[:, None, None] * fy(yc)[None, :, None] * szf[None, None, :]
-        A[2] += amp[2] * fx(xf, ph[2])[:, None, None] * fy(yf)[None, :, None] * czc[None, None, :]
+    # A_c = Re sum_{kx,ky,kz} C_c exp(2 pi i (kx x/Lx + ky y/Ly)) S_c,kz(z): for each
+    # kz the (x,y) sum is two small matrix products, then one outer product in z.
+    ks = np.arange(-kmax, kmax + 1)
+    Ex = {nm: np.exp(2j * np.pi * np.outer(xs, ks) / l[0]) for nm, xs in (("c", xc), ("f", xf))}
+    Ey = {nm: np.exp(2j * np.pi * np.outer(ys, ks) / l[1]) for nm, ys in (("c", yc), ("f", yf))}
+    kk = ks[:, None] ** 2 + ks[None, :] ** 2
+    grids = (("c", "f", zf[: nz + 1], "s"), ("f", "c", zf[: nz + 1], "s"), ("f", "f", zc, "c"))
+    A = []
+    for comp, (gx, gy, zs, kind) in enumerate(grids):
+        acc = np.zeros((nx, ny, zs.size))
+        for kz in range(0, kmax + 1):
+            mask = (kk + kz * kz <= kmax * kmax) & (kk + kz * kz > 0)
+            coef = (rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)) / (1.0 + kk + kz * kz)
+            coef = np.where(mask, coef, 0.0)
+            plane = np.real(Ex[gx] @ coef @ Ey[gy].T)  # (nx, ny)
+            if kind == "s":
+                prof = np.sin(np.pi * max(kz, 1) * zs / l[2])  # vanishes on both walls
+            else:
+                prof = np.cos(np.pi * kz * zs / l[2])
+            acc += plane[:, :, None] * prof[None, None, :]
+        A.append(acc)
     Ax, Ay, Az = A
     dzf = g["dzf"][1:-1]
     dzc = g["dzc"]

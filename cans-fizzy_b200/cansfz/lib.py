@@ -70,6 +70,8 @@ SIGNATURES = {
     # library controls (no reference counterpart)
     "cansfz_set_time": (I, [V, D, ct.c_longlong]),
     "cansfz_set_inivel": (I, [V, ct.c_char_p]),
+    "cansfz_kernels_per_step": (I, [V, ct.POINTER(I)]),
+    "cansfz_profile_stages": (I, [V, I, PD, I, ct.POINTER(I), ct.c_char_p, I]),
 }
 
 _lib = None

@@ -130,6 +130,13 @@ struct Launch {
   int nsm;
 };
 
+// optional stage marker of the step profiler (CUDA events between stages)
+struct StageMark {
+  void (*fn)(void* arg, const char* name);
+  void* arg;
+  void mark(const char* name) const { fn(arg, name); }
+};
+
 // k_stencil.cu
 void launch_acdi_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
                            const double* u, const double* v, const double* w,
@@ -210,10 +217,10 @@ void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
 // k_poisson.cu
 void poisson_set_attributes();
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
-                    double* p);
+                    double* p, const StageMark* mk = nullptr);
 void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& pl,
                               const Phys& ph, const DevScalars* sc, const double* u,
                               const double* v, const double* w, const double* rhsb_planes,
-                              double* phi);
+                              double* phi, const StageMark* mk = nullptr);
 
 }  // namespace cansfz

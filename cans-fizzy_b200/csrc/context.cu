@@ -432,13 +432,15 @@ __global__ void k_prescribed_vel(Geo g, const DevScalars* __restrict__ sc, int w
 // ---------------------------------------------------------------------------
 // one time step (src/main.f90:422-529) on the current parity `c->cur`
 // ---------------------------------------------------------------------------
-void enqueue_step(cansfz_ctx* c) {
+void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
+#define MARK(nm) do { if (mk) mk->mark(nm); } while (0)
   const cansfz_params& P = c->P;
   const Launch& L = c->L;
   const Geo& g = c->g;
   const int a = c->cur, b = a ^ 1;
   DevScalars* sc = c->sc;
   launch_step_begin(L, sc, P.icheck);
+  MARK("step_begin");
   // phase field: rk_2fl + boundary fills + phi + normals/curvature
   if (P.is_track_interface) {
     if (c->ph.acdi)
@@ -447,14 +449,19 @@ void enqueue_step(cansfz_ctx* c) {
     else
       launch_thinc_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
                         c->psi[a], c->psi[b], c->hpsi, c->fx, c->fy, c->fz);
+    MARK("phase_transport");
     BcField F[3];
     bc_vel(c, false, c->fx, c->fy, c->fz, F);
     run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc);
+    MARK("bc_phase");
     if (c->ph.sdf) launch_cmpt_phi(L, g, sc, c->ph.acdi != 0, c->psi[b], c->phi);
+    MARK("cmpt_phi");
     launch_youngs(L, g, sc, c->ph.sdf ? c->phi : c->psi[b], c->nx, c->ny, c->nz, c->kappa);
+    MARK("youngs");
     run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
                bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
            sc);
+    MARK("bc_normals");
   } else {
     launch_copy(L, (size_t)g.hsize(), c->psi[a], c->psi[b]);
     launch_fill(L, (size_t)g.hsize(), 0., c->fx);
@@ -477,26 +484,36 @@ void enqueue_step(cansfz_ctx* c) {
     // rk: the whole momentum update in one pass
     launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy, c->fz,
                           c->p[a], c->p[b], c->kappa, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
+    MARK("momentum");
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
+    MARK("bc_uvw");
     // fillps + updt_rhs_b + solver
     if (c->rhsb_zero) {
-      launch_poisson_fused_rhs(L, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip);
+      launch_poisson_fused_rhs(L, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip, mk);
     } else {
       launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->phip);
       launch_updt_rhs_b(L, g, c->is_bound, c->rhsbx, c->rhsby, c->rhsbz, c->phip);
-      launch_poisson(L, g, c->pl, sc, c->phip);
+      launch_poisson(L, g, c->pl, sc, c->phip, mk);
     }
     run_bcp(c, 0, c->phip, sc);
+    MARK("bc_pcorr");
     launch_correc(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b]);
+    MARK("correc");
     run_bcuvw(c, true, c->u[b], c->v[b], c->w[b], sc);
+    MARK("bc_uvw_correc");
     // updatep: p_new = phi + p into the po slot, then po <- p by the parity flip
     launch_updatep_interior(L, g, sc, c->phip, c->p[a], c->p[b]);
+    MARK("updatep");
     run_bcp(c, 0, c->p[b], sc);
+    MARK("bc_p");
   }
   launch_step_end(L, c->ph, sc);
   if (c->ph.acdi) launch_gamma(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
+  MARK("gamma");
   launch_chkdt(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
   launch_chkdiv(L, g, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
+  MARK("chkdt_chkdiv");
+#undef MARK
 }
 
 }  // namespace
@@ -1076,6 +1093,94 @@ int cansfz_set_inivel(cansfz_ctx* c, const char* inivel) {
   for (auto& ge : c->gexec)
     if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
   return CANSFZ_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// library-only measurement helpers (no reference counterpart)
+// ---------------------------------------------------------------------------
+// Number of kernel nodes in the captured step graph of the current parity.
+int cansfz_kernels_per_step(cansfz_ctx* c, int* count) {
+  if (!c || !count) return CANSFZ_ERR_ARG;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(c);
+  CK(cudaStreamEndCapture(c->st, &graph));
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  int k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    cudaGraphNodeGetType(nd, &t);
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  cudaGraphDestroy(graph);
+  *count = k;
+  return CANSFZ_OK;
+}
+
+namespace {
+struct ProfState {
+  cansfz_ctx* c;
+  std::vector<cudaEvent_t>* ev;
+  std::vector<std::string>* names;
+  size_t idx;
+};
+void prof_mark(void* arg, const char* name) {
+  ProfState* s = (ProfState*)arg;
+  if (s->idx >= s->ev->size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    s->ev->push_back(e);
+  }
+  cudaEventRecord((*s->ev)[s->idx], s->c->st);
+  if (s->names->size() < s->idx + 1) s->names->push_back(name);
+  ++s->idx;
+}
+}  // namespace
+
+// Run nsteps time steps without the graph, with CUDA events between the
+// stages; returns per stage the summed milliseconds (ms[i]) and the stage
+// names as a comma-separated list in `names` (capacity `cap` bytes).
+int cansfz_profile_stages(cansfz_ctx* c, int nsteps, double* ms, int maxstages, int* nstages, char* names,
+                          int cap) {
+  if (!c || !ms || !names || !nstages || nsteps < 1) return CANSFZ_ERR_ARG;
+  if (!c->prepared) {
+    int rc = cansfz_prepare(c);
+    if (rc) return rc;
+  }
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::string> nm;
+  cudaEvent_t e0;
+  CK(cudaEventCreate(&e0));
+  std::vector<double> acc;
+  for (int s = 0; s < nsteps; ++s) {
+    ProfState st{c, &ev, &nm, 0};
+    StageMark mk{prof_mark, &st};
+    CK(cudaEventRecord(e0, c->st));
+    enqueue_step(c, &mk);
+    CK(cudaStreamSynchronize(c->st));
+    c->cur ^= 1;
+    if (acc.size() < st.idx) acc.resize(st.idx, 0.);
+    for (size_t q = 0; q < st.idx; ++q) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, q == 0 ? e0 : ev[q - 1], ev[q]));
+      acc[q] += t;
+    }
+  }
+  std::string all;
+  const int ns = std::min<int>((int)acc.size(), maxstages);
+  for (int q = 0; q < ns; ++q) {
+    ms[q] = acc[q];
+    all += (q ? "," : "") + nm[q];
+  }
+  std::snprintf(names, cap, "%s", all.c_str());
+  for (auto e : ev) cudaEventDestroy(e);
+  cudaEventDestroy(e0);
+  *nstages = ns;
+  return sync_status(c);
 }
 
 }  // extern "C"

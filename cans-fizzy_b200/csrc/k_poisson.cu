@@ -538,25 +538,36 @@ static void x_backward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, co
 }
 
 // solver_gpu on the interior of the halo-layout field p (in place)
-void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* p) {
+void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* p,
+                    const StageMark* mk) {
   x_forward(L, g, pl, sc, p, nullptr, nullptr, nullptr, nullptr, false);
+  if (mk) mk->mark("poisson_x_fwd");
   y_pass(L, g, pl, sc, +1);
+  if (mk) mk->mark("poisson_y_fwd");
   z_pass(L, g, pl, sc);
+  if (mk) mk->mark("poisson_z_solve");
   y_pass(L, g, pl, sc, -1);
+  if (mk) mk->mark("poisson_y_bwd");
   x_backward(L, g, pl, sc, p);
+  if (mk) mk->mark("poisson_x_bwd");
 }
 
 // fillps + solver_gpu: the RHS is formed inside the x transform from u, v, w;
 // phi (the interior of a halo-layout field) receives the solution.
 void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& pl, const Phys& ph,
                               const DevScalars* sc, const double* u, const double* v, const double* w,
-                              const double* rhsb_planes, double* phi) {
+                              const double* rhsb_planes, double* phi, const StageMark* mk) {
   (void)rhsb_planes;
   x_forward(L, g, pl, sc, nullptr, u, v, w, &ph, true);
+  if (mk) mk->mark("poisson_x_fwd_fillps");
   y_pass(L, g, pl, sc, +1);
+  if (mk) mk->mark("poisson_y_fwd");
   z_pass(L, g, pl, sc);
+  if (mk) mk->mark("poisson_z_solve");
   y_pass(L, g, pl, sc, -1);
+  if (mk) mk->mark("poisson_y_bwd");
   x_backward(L, g, pl, sc, phi);
+  if (mk) mk->mark("poisson_x_bwd");
 }
 
 }  // namespace cansfz

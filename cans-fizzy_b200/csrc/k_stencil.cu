@@ -914,9 +914,10 @@ __global__ void k_chkdiv_final(Phys ph, DevScalars* __restrict__ sc, int only_on
   if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
   sc->divmax = __longlong_as_double((long long)sc->max_bits[2]);
   sc->max_bits[2] = 0ull;
-  if (only_on_check) {
+  // src/main.f90:552-561, after the dt checks (an earlier dt abort is kept)
+  if (only_on_check && sc->status == CANSFZ_OK) {
     if (isnan(sc->divtot)) sc->status = CANSFZ_ERR_NAN;
-    else if (sc->divmax > ph.small && sc->status == CANSFZ_OK) sc->status = CANSFZ_ERR_DIVERGENCE;
+    else if (sc->divmax > ph.small) sc->status = CANSFZ_ERR_DIVERGENCE;
   }
 }
 void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial, const double* u,

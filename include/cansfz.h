@@ -240,6 +240,21 @@ int cansfz_initgrid(int gtype, int nz, double gr, double lz,
 int cansfz_get_grid(cansfz_ctx* ctx, double* dzc, double* dzf, double* zc,
                     double* zf, double* dzci, double* dzfi);
 
+/* ---- library controls and measurement (no reference counterpart) -------- */
+/* Time and step counter of the next step (restart: the [time, istep] pair
+ * stored at the end of a checkpoint file, src/load.f90:94-134).            */
+int cansfz_set_time(cansfz_ctx* ctx, double time, long long istep);
+/* Prescribed velocity of is_solve_ns = .false. runs ('voy', 'vox', 'zer'
+ * of initflow, src/initflow.f90:242-275), re-evaluated every step.         */
+int cansfz_set_inivel(cansfz_ctx* ctx, const char* inivel);
+/* Kernel launches per captured time step. */
+int cansfz_kernels_per_step(cansfz_ctx* ctx, int* count);
+/* Run nsteps steps outside the graph with CUDA events between the stages:
+ * ms[i] = summed milliseconds of stage i, *nstages stages, names written
+ * comma-separated into `names` (cap bytes).  Advances the state.          */
+int cansfz_profile_stages(cansfz_ctx* ctx, int nsteps, double* ms, int maxstages,
+                          int* nstages, char* names, int cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,155 @@
+"""Whole-run GPU checks that do not need the oracle at every cell:
+
+* deformation and return of a circle in the reference's serpentine vortex
+  ('voy' prescribed velocity, src/initflow.f90:242-258), ACDI transport only:
+  after one period the interface must return to its initial position;
+* full-size (256^3) properties of the FP64 step on the droplet workload:
+  max divergence after the projection, phase-mass drift, and the same
+  drift as the oracle over the first steps at a reduced size;
+* the reference's abort conditions (src/main.f90:534-561) reported as
+  status codes, triggered from the host (a NaN planted in an input field,
+  a fixed dt above the stability limit) -- no GPU fault is involved.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from cansfz import case as C
+from cansfz import init, namelist, params, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _vortex_params(n=128, dtmax=1.0e-3):
+    text = f"""
+&dns
+ng(1:3) = {n}, 2, {n}
+l(1:3) = 1., {2.0 / n}, 1.
+cfl = 0.5, dtmax = {dtmax}, icheck = 50
+is_solve_ns = F, is_track_interface = T
+inivel = 'voy'
+cbcvel(0:1,1:3,1) = 'D','D', 'P','P', 'D','D'
+cbcvel(0:1,1:3,2) = 'D','D', 'P','P', 'D','D'
+cbcvel(0:1,1:3,3) = 'D','D', 'P','P', 'D','D'
+cbcpre(0:1,1:3)   = 'N','N', 'P','P', 'N','N'
+/
+&two_fluid
+cbcpsi(0:1,1:3)   = 'N','N', 'P','P', 'N','N'
+cbcnor(0:1,1:3,1) = 'D','D', 'P','P', 'N','N'
+cbcnor(0:1,1:3,2) = 'N','N', 'P','P', 'N','N'
+cbcnor(0:1,1:3,3) = 'N','N', 'P','P', 'D','D'
+rho12(1:2) = 1., 1.
+mu12(1:2) = 1., 1.
+psi_thickness_factor = 0.51
+/
+"""
+    return params.from_namelist(namelist.parse(text))
+
+
+def _vortex_case(p, backend):
+    psi = init.init2fl(p, "bub2", np.array([[0.5, 0.0, 0.7, 0.18]]))
+    u, v, w, pr = init.initflow(p, "voy", 0.0)
+    if backend == "gpu":
+        c = C.Case(p)
+        c.set_inivel("voy")
+        c.set_fields(u, v, w, pr, psi)
+    else:
+        c = O.Case(p)
+        c.set_inivel("voy")
+        for nm, a in zip(("u", "v", "w", "p", "psi"), (u, v, w, pr, psi)):
+            c.set(nm, a)
+    c.prepare()
+    return c, psi
+
+
+def test_vortex_parity_with_oracle():
+    p = _vortex_params(64, 2.0e-3)
+    g, _ = _vortex_case(p, "gpu")
+    o, _ = _vortex_case(p, "cpu")
+    assert g.step(100) == 0 and o.step(100) == 0
+    a, b = g.get("psi"), o.get("psi")
+    assert np.abs(a - b).max() < 1e-11
+    assert abs(g.diag().time - o.diag().time) < 1e-13
+
+
+def test_vortex_deformation_and_return():
+    p = _vortex_params(128, 1.0e-3)
+    g, psi0 = _vortex_case(p, "gpu")
+    # one period of cos(pi t / 4): t = 4 at the fixed dt of 1e-3 (dtmax)
+    nsteps = 4000
+    assert g.step(nsteps) == 0
+    d = g.diag()
+    assert abs(d.time - 4.0) < 1e-9
+    psi = g.get("psi")[1:-1, 1, 1:-1]
+    ref = psi0[1:-1, 1, 1:-1]
+    l1 = np.sum(np.abs(psi - ref)) / psi.size
+    assert l1 < 2e-2, l1
+    m0 = np.sum(ref)
+    assert abs(np.sum(psi) - m0) / m0 < 1e-3
+
+
+@pytest.fixture(scope="module")
+def droplets_full():
+    p, f = workloads.droplets_acdi(seed=2026)
+    return p, f
+
+
+def test_full_size_divergence_and_mass(droplets_full):
+    p, f = droplets_full
+    g = C.Case(p)
+    g.set_fields(*f)
+    g.prepare()
+    m0 = g.diag().mass12
+    assert g.step(20) == 0  # icheck = 10: two divergence checks
+    d = g.diag()
+    assert d.divmax < 1e-12, d.divmax      # projection to round-off (reference abort threshold 2.2e-9)
+    drift = abs(d.mass12[0] - m0[0]) / m0[0]
+    assert drift < 1e-10, drift
+    g.close()
+
+
+def test_mass_drift_matches_oracle():
+    """The clip of psi to [0,1] (src/rk.f90:248) is not conservative: compare
+    the GPU's phase-mass change with the oracle's own on the same input."""
+    p, f = workloads.droplets((96, 96, 96), (1.0, 1.0, 1.0), False, count=16, rmin=0.05, rmax=0.09, seed=9)
+    g = C.Case(p)
+    g.set_fields(*f)
+    g.prepare()
+    o = O.Case(p)
+    for nm, a in zip(("u", "v", "w", "p", "psi"), f):
+        o.set(nm, a)
+    o.prepare()
+    mg0, mo0 = g.diag().mass12[0], o.diag().mass12[0]
+    assert g.step(20) == 0 and o.step(20) == 0
+    dg = g.diag().mass12[0] - mg0
+    do = o.diag().mass12[0] - mo0
+    assert abs(dg - do) <= 1e-12 * mo0 + 1e-3 * abs(do)
+
+
+def test_abort_on_nan_input():
+    p = _vortex_params(32, 1.0e-3)
+    p.is_solve_ns = 1
+    psi = init.init2fl(p, "bub2", np.array([[0.5, 0.0, 0.5, 0.2]]))
+    u, v, w, pr = init.initflow(p, "zer")
+    u[10, 1, 10] = np.nan
+    g = C.Case(p)
+    g.set_fields(u, v, w, pr, psi)
+    rc = g.step(60)  # icheck = 50
+    assert rc in (4, 5)  # CANSFZ_ERR_NAN or _DIVERGENCE, as the reference aborts
+    d = g.diag()
+    assert d.istep == 50  # the steps after the aborting one did nothing
+    assert g.step(1) == rc
+
+
+def test_abort_on_fixed_dt_above_limit():
+    p = _vortex_params(32, 1.0e-3)
+    p.is_solve_ns = 1
+    p.dt_f = 10.0
+    p.icheck = 5
+    psi = init.init2fl(p, "bub2", np.array([[0.5, 0.0, 0.5, 0.2]]))
+    u, v, w, pr = init.initflow(p, "zer")
+    g = C.Case(p)
+    g.set_fields(u, v, w, pr, psi)
+    rc = g.step(10)
+    assert rc == 6  # CANSFZ_ERR_DT
+    assert g.diag().istep == 5
