@@ -72,6 +72,8 @@ SIGNATURES = {
     "cansfz_set_inivel": (I, [V, ct.c_char_p]),
     "cansfz_kernels_per_step": (I, [V, ct.POINTER(I)]),
     "cansfz_profile_stages": (I, [V, I, PD, I, ct.POINTER(I), ct.c_char_p, I]),
+    "cansfz_solver_refined": (I, [V, V, V, I]),
+    "cansfz_poisson_residual": (I, [V, V, V, V]),
 }
 
 _lib = None

@@ -108,6 +108,9 @@ struct LinePlan {
   const double2* tw;    // exp(-2 pi i q / m), q = 0..m-1
   const double2* tw2;   // exp(-2 pi i k / n), k = 0..n/2 (real-transform post twiddle)
   const double2* twc;   // exp(-i pi k / (2n)), k = 0..n (DCT/DST twiddle)
+  const float2* twf;    // the same three tables rounded to FP32 (mixed form)
+  const float2* tw2f;
+  const float2* twcf;
 };
 
 struct PoissonPlan {
@@ -120,6 +123,9 @@ struct PoissonPlan {
   int zper;              // periodic z: Sherman-Morrison variant
   double* work;          // nx*ny*nz spectral buffer
   double* work2;         // second buffer (periodic z, DCT remaps)
+  float* workf;          // FP32 spectral buffers of the mixed form
+  float* work2f;
+  int zsing;             // z operator singular (no Dirichlet wall): pin the (0,0) mode in FP32
 };
 
 // ---------------------------------------------------------------------------
@@ -218,6 +224,12 @@ void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
 void poisson_set_attributes();
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                     double* p, const StageMark* mk = nullptr);
+// mixed form: FP32 spectral solve (dst = S(src) or dst += S(src)) and the
+// FP64 residual res = rhs - L(phi) of the refinement
+void launch_poisson_f32(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                        const double* src, double* dst, bool add, const StageMark* mk = nullptr);
+void launch_residual(const Launch& L, const Geo& g, const DevScalars* sc, const double* rhs,
+                     const double* phi, double* res);
 void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& pl,
                               const Phys& ph, const DevScalars* sc, const double* u,
                               const double* v, const double* w, const double* rhsb_planes,

@@ -95,6 +95,11 @@ struct cansfz_ctx {
   double* rhsbx = nullptr; double* rhsby = nullptr; double* rhsbz = nullptr;
   bool rhsb_zero = true;
   double* d_work = nullptr;
+  // mixed form: FP64 right-hand side and refinement residual (halo layout)
+  double* rhs64 = nullptr;
+  double* res64 = nullptr;
+  bool mixed = false;
+  int sweeps = 2;
   // reductions, scalars
   double* partial = nullptr;
   DevScalars* sc = nullptr;       // the step scalars (device)
@@ -364,6 +369,21 @@ int setup_solver(cansfz_ctx* c) {
     lps[d]->twc = (const double2*)(D + off_twc[d]);
   }
   c->rhsbx = D + off_rx; c->rhsby = D + off_ry; c->rhsbz = D + off_rz;
+  // FP32 copies of the twiddle tables (mixed form)
+  {
+    std::vector<float> hf(host.size());
+    for (size_t q = 0; q < host.size(); ++q) hf[q] = (float)host[q];
+    float* F = nullptr;
+    rc = dalloc(c, &F, hf.size() + 4);
+    if (rc) return rc;
+    CK(cudaMemcpy(F, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    for (int d = 0; d < 2; ++d) {
+      lps[d]->twf = (const float2*)(F + off_tw[d]);
+      lps[d]->tw2f = (const float2*)(F + off_tw2[d]);
+      lps[d]->twcf = (const float2*)(F + off_twc[d]);
+    }
+  }
+  c->pl.zsing = (P.cbcpre[2][0] != 'D' && P.cbcpre[2][1] != 'D') ? 1 : 0;
   c->pl.normfft = 1. / normfft;
   c->pl.zper = is_pp(P.cbcpre[2]) ? 1 : 0;
   const size_t nint = (size_t)nx * ny * nz;
@@ -372,6 +392,15 @@ int setup_solver(cansfz_ctx* c) {
   if (c->pl.zper) {
     rc = dalloc(c, &c->pl.work2, nint);
     if (rc) return rc;
+  }
+  if (P.form == CANSFZ_FORM_MIXED) {
+    if (!c->rhsb_zero) return CANSFZ_ERR_UNSUPPORTED;  // refinement assumes homogeneous pressure BCs
+    rc = dalloc(c, &c->pl.workf, nint);
+    if (rc) return rc;
+    if (c->pl.zper) {
+      rc = dalloc(c, &c->pl.work2f, nint);
+      if (rc) return rc;
+    }
   }
   return CANSFZ_OK;
 }
@@ -488,7 +517,18 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw");
     // fillps + updt_rhs_b + solver
-    if (c->rhsb_zero) {
+    if (c->mixed) {
+      // FP32 spectral solve + FP64-residual refinement sweeps
+      launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->rhs64);
+      MARK("fillps");
+      launch_poisson_f32(L, g, c->pl, sc, c->rhs64, c->phip, false, mk);
+      for (int sw = 0; sw < c->sweeps; ++sw) {
+        run_bcp(c, 0, c->phip, sc);
+        launch_residual(L, g, sc, c->rhs64, c->phip, c->res64);
+        MARK("residual");
+        launch_poisson_f32(L, g, c->pl, sc, c->res64, c->phip, true, mk);
+      }
+    } else if (c->rhsb_zero) {
       launch_poisson_fused_rhs(L, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip, mk);
     } else {
       launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->phip);
@@ -640,6 +680,12 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   for (double** f : {&c->hpsi, &c->hu, &c->hv, &c->hw, &c->tu, &c->tv, &c->tw_, &c->tpsi})
     if ((rc = dalloc(c, f, I))) return fail(rc);
   if ((rc = setup_solver(c))) return fail(rc);
+  c->mixed = P.form == CANSFZ_FORM_MIXED;
+  c->sweeps = P.refine_sweeps < 0 ? 0 : (P.refine_sweeps > 8 ? 8 : P.refine_sweeps);
+  if (c->mixed) {
+    if ((rc = dalloc(c, &c->rhs64, H))) return fail(rc);
+    if ((rc = dalloc(c, &c->res64, H))) return fail(rc);
+  }
   // reductions: partial sums of one launch over the interior blocks
   const int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
   const size_t nblk = (size_t)((nx + bx - 1) / bx) * ny * nz;
@@ -1183,4 +1229,39 @@ int cansfz_profile_stages(cansfz_ctx* c, int nsteps, double* ms, int maxstages, 
   return sync_status(c);
 }
 
+
+// Mixed-form Poisson solve on its own: p = S32(rhs), then `sweeps` times
+// p += S32(rhs - L(p)) with the FP64 residual of the 7-point operator.
+// rhs and p are halo-layout device fields; p's ghosts are left filled.
+int cansfz_solver_refined(cansfz_ctx* c, const double* rhs, double* p, int sweeps) {
+  if (!c || !rhs || !p || sweeps < 0 || sweeps > 16) return CANSFZ_ERR_ARG;
+  if (!c->rhsb_zero) return CANSFZ_ERR_UNSUPPORTED;
+  const size_t nint = (size_t)c->g.tsize(), H = (size_t)c->g.hsize();
+  int rc;
+  if (!c->pl.workf && (rc = dalloc(c, &c->pl.workf, nint))) return rc;
+  if (c->pl.zper && !c->pl.work2f && (rc = dalloc(c, &c->pl.work2f, nint))) return rc;
+  if (!c->res64 && (rc = dalloc(c, &c->res64, H))) return rc;
+  DevScalars h{};
+  if ((rc = call_scalars(c, h))) return rc;
+  launch_poisson_f32(c->L, c->g, c->pl, c->sc_call, rhs, p, false);
+  for (int sw = 0; sw < sweeps; ++sw) {
+    run_bcp(c, 0, p, nullptr);
+    launch_residual(c->L, c->g, c->sc_call, rhs, p, c->res64);
+    launch_poisson_f32(c->L, c->g, c->pl, c->sc_call, c->res64, p, true);
+  }
+  run_bcp(c, 0, p, nullptr);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+// FP64 residual res = rhs - L(p) of the 7-point operator (p's ghosts filled here)
+int cansfz_poisson_residual(cansfz_ctx* c, const double* rhs, double* p, double* res) {
+  if (!c || !rhs || !p || !res) return CANSFZ_ERR_ARG;
+  DevScalars h{};
+  if (int rc = call_scalars(c, h)) return rc;
+  run_bcp(c, 0, p, nullptr);
+  launch_residual(c->L, c->g, c->sc_call, rhs, p, res);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
 }  // extern "C"

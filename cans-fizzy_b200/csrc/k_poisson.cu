@@ -1,15 +1,15 @@
 // Constant-coefficient Poisson solve of solver_gpu (src/solver_gpu.f90:31-163)
-// on one GPU, 1x1 pencil, FP64.  No transposes: the x lines are contiguous
-// rows, the y lines are read as column tiles of TL consecutive x positions,
-// and the z tridiagonal systems are solved one column per thread.
+// on one GPU, 1x1 pencil.  No transposes: the x lines are contiguous rows,
+// the y lines are read as column tiles of TL consecutive x positions, and the
+// z tridiagonal systems are solved one column per thread.
 //
 //   x: real transform of each row    (R2HC packed / DCT-II / DST-II)
 //   y: real transform of each column (same kinds, per BC)
 //   z: Thomas per (x,y) mode with b + lambda_x + lambda_y (gaussel_gpu,
 //      src/solver_gpu.f90:165-230), Sherman-Morrison for periodic z
 //      (gaussel_periodic_gpu, :232-370)
-//   y, x: inverse transforms; x inverse scales by normfft and writes the
-//      interior of the halo-layout output.
+//   y, x: inverse transforms; x inverse scales by normfft and writes (or,
+//      for a refinement correction, adds to) the interior of a halo field.
 //
 // Line transforms: a complex FFT of length m = n/2 (the real sequence packed
 // as z_j = x_2j + i x_2j+1), Stockham auto-sort, radix 4/2/3 (generic radix
@@ -18,48 +18,72 @@
 // periodic kind stores the spectrum as (r0, r_{n/2}, r1, i1, r2, i2, ...);
 // the eigenvalues are permuted to that order on the host.  The cosine and
 // sine kinds follow Makhoul's reordering (as src/fft.f90:320-658 does).
+//
+// Every transform kernel is a template on the precision T of the spectral
+// data: T = double is the drop-in FP64 solve; T = float is the spectral
+// solve of the mixed form, whose accuracy an FP64 residual refinement wins
+// back (launch_poisson_mixed).
 #include "cansfz_internal.cuh"
 
 namespace cansfz {
 
 #define HALTED(sc) ((sc) != nullptr && (sc)->halted)
 
+template <typename T> struct CT;
+template <> struct CT<double> { using t = double2; };
+template <> struct CT<float> { using t = float2; };
+template <typename T> using cx = typename CT<T>::t;
+
+template <typename T> __device__ __forceinline__ cx<T> mk(T a, T b) { cx<T> r; r.x = a; r.y = b; return r; }
+template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T> __device__ __forceinline__ cx<T> cadd(cx<T> a, cx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ cx<T> csub(cx<T> a, cx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ cx<T> cconj(cx<T> a) { return mk<T>(a.x, -a.y); }
+template <typename T> __device__ __forceinline__ cx<T> mul_i(cx<T> a) { return mk<T>(-a.y, a.x); }  // i*a
+
+// twiddle tables in the transform precision
+template <typename T> __device__ __forceinline__ cx<T> TW(const LinePlan& pl, int q);
+template <> __device__ __forceinline__ double2 TW<double>(const LinePlan& pl, int q) { return __ldg(&pl.tw[q]); }
+template <> __device__ __forceinline__ float2 TW<float>(const LinePlan& pl, int q) { return __ldg(&pl.twf[q]); }
+template <typename T> __device__ __forceinline__ cx<T> TW2(const LinePlan& pl, int q);
+template <> __device__ __forceinline__ double2 TW2<double>(const LinePlan& pl, int q) { return __ldg(&pl.tw2[q]); }
+template <> __device__ __forceinline__ float2 TW2<float>(const LinePlan& pl, int q) { return __ldg(&pl.tw2f[q]); }
+template <typename T> __device__ __forceinline__ cx<T> TWC(const LinePlan& pl, int q);
+template <> __device__ __forceinline__ double2 TWC<double>(const LinePlan& pl, int q) { return __ldg(&pl.twc[q]); }
+template <> __device__ __forceinline__ float2 TWC<float>(const LinePlan& pl, int q) { return __ldg(&pl.twcf[q]); }
+
+template <typename T>
 struct Bufs {
-  double* re[2];
-  double* im[2];
+  T* re[2];
+  T* im[2];
   int LP;  // line pitch in shared memory (odd: conflict-free strided access)
 };
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ double2 mul_i(double2 a) { return make_double2(-a.y, a.x); }  // i*a
-
-__device__ __forceinline__ double2 ld2(const Bufs& B, int b, int pos, int line) {
+template <typename T> __device__ __forceinline__ cx<T> ld2(const Bufs<T>& B, int b, int pos, int line) {
   const int q = pos * B.LP + line;
-  return make_double2(B.re[b][q], B.im[b][q]);
+  return mk<T>(B.re[b][q], B.im[b][q]);
 }
-__device__ __forceinline__ void st2(const Bufs& B, int b, int pos, int line, double2 v) {
+template <typename T> __device__ __forceinline__ void st2(const Bufs<T>& B, int b, int pos, int line, cx<T> v) {
   const int q = pos * B.LP + line;
   B.re[b][q] = v.x;
   B.im[b][q] = v.y;
 }
 // raw real position s of a line stored as complex pairs (s even: re, odd: im)
-__device__ __forceinline__ double ldr(const Bufs& B, int b, int s, int line) {
+template <typename T> __device__ __forceinline__ T ldr(const Bufs<T>& B, int b, int s, int line) {
   const int q = (s >> 1) * B.LP + line;
   return (s & 1) ? B.im[b][q] : B.re[b][q];
 }
-__device__ __forceinline__ void str(const Bufs& B, int b, int s, int line, double v) {
+template <typename T> __device__ __forceinline__ void str(const Bufs<T>& B, int b, int s, int line, T v) {
   const int q = (s >> 1) * B.LP + line;
   if (s & 1) B.im[b][q] = v; else B.re[b][q] = v;
 }
 
 // complex FFT (sign -1 forward, +1 backward) of length pl.m on L lines held
 // in buffer `in`; returns the buffer index holding the result.
-__device__ int fft_lines(const LinePlan& pl, const Bufs& B, int in, int L, int sign) {
+template <typename T>
+__device__ int fft_lines(const LinePlan& pl, const Bufs<T>& B, int in, int L, int sign) {
   const int m = pl.m;
   int len = m, s = 1, cur = in;
   for (int st = 0; st < pl.nst; ++st) {
@@ -71,46 +95,46 @@ __device__ int fft_lines(const LinePlan& pl, const Bufs& B, int in, int L, int s
     for (int it = threadIdx.x; it < L * nb; it += blockDim.x) {
       const int line = it % L, b = it / L;
       const int p = b / s, q = b - p * s;
-      auto put = [&](int u, double2 y) {
+      auto put = [&](int u, cx<T> y) {
         if (u > 0 && p > 0) {
-          double2 wp = __ldg(&pl.tw[(p * u * tstep) % m]);
-          if (sign > 0) wp = cconj(wp);
-          y = cmul(y, wp);
+          cx<T> wp = TW<T>(pl, (p * u * tstep) % m);
+          if (sign > 0) wp = cconj<T>(wp);
+          y = cmul<T>(y, wp);
         }
-        st2(B, nxt, q + s * (r * p + u), line, y);
+        st2<T>(B, nxt, q + s * (r * p + u), line, y);
       };
       if (r == 2) {
-        const double2 a0 = ld2(B, cur, q + s * p, line), a1 = ld2(B, cur, q + s * (p + mm), line);
-        put(0, cadd(a0, a1));
-        put(1, csub(a0, a1));
+        const cx<T> a0 = ld2<T>(B, cur, q + s * p, line), a1 = ld2<T>(B, cur, q + s * (p + mm), line);
+        put(0, cadd<T>(a0, a1));
+        put(1, csub<T>(a0, a1));
       } else if (r == 4) {
-        const double2 a0 = ld2(B, cur, q + s * p, line), a1 = ld2(B, cur, q + s * (p + mm), line);
-        const double2 a2 = ld2(B, cur, q + s * (p + 2 * mm), line), a3 = ld2(B, cur, q + s * (p + 3 * mm), line);
-        const double2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+        const cx<T> a0 = ld2<T>(B, cur, q + s * p, line), a1 = ld2<T>(B, cur, q + s * (p + mm), line);
+        const cx<T> a2 = ld2<T>(B, cur, q + s * (p + 2 * mm), line), a3 = ld2<T>(B, cur, q + s * (p + 3 * mm), line);
+        const cx<T> t0 = cadd<T>(a0, a2), t1 = csub<T>(a0, a2), t2 = cadd<T>(a1, a3), t3 = csub<T>(a1, a3);
         // W4 = exp(sign * i pi / 2) = sign * i
-        const double2 it3 = sign < 0 ? make_double2(t3.y, -t3.x) : make_double2(-t3.y, t3.x);  // W4 * t3
-        put(0, cadd(t0, t2));
-        put(1, cadd(t1, it3));
-        put(2, csub(t0, t2));
-        put(3, csub(t1, it3));
+        const cx<T> it3 = sign < 0 ? mk<T>(t3.y, -t3.x) : mk<T>(-t3.y, t3.x);  // W4 * t3
+        put(0, cadd<T>(t0, t2));
+        put(1, cadd<T>(t1, it3));
+        put(2, csub<T>(t0, t2));
+        put(3, csub<T>(t1, it3));
       } else if (r == 3) {
-        const double2 a0 = ld2(B, cur, q + s * p, line), a1 = ld2(B, cur, q + s * (p + mm), line);
-        const double2 a2 = ld2(B, cur, q + s * (p + 2 * mm), line);
-        const double2 t1 = cadd(a1, a2), t2 = csub(a1, a2);
-        const double c3 = 0.86602540378443864676 * (double)(-sign);  // -sign*sqrt(3)/2
-        const double2 base = make_double2(a0.x - 0.5 * t1.x, a0.y - 0.5 * t1.y);
-        const double2 rot = make_double2(c3 * t2.y, -c3 * t2.x);  // -i * c3 * t2
-        put(0, cadd(a0, t1));
-        put(1, cadd(base, rot));
-        put(2, csub(base, rot));
+        const cx<T> a0 = ld2<T>(B, cur, q + s * p, line), a1 = ld2<T>(B, cur, q + s * (p + mm), line);
+        const cx<T> a2 = ld2<T>(B, cur, q + s * (p + 2 * mm), line);
+        const cx<T> t1 = cadd<T>(a1, a2), t2 = csub<T>(a1, a2);
+        const T c3 = (T)0.86602540378443864676 * (T)(-sign);  // -sign*sqrt(3)/2
+        const cx<T> base = mk<T>(a0.x - (T)0.5 * t1.x, a0.y - (T)0.5 * t1.y);
+        const cx<T> rot = mk<T>(c3 * t2.y, -c3 * t2.x);  // -i * c3 * t2
+        put(0, cadd<T>(a0, t1));
+        put(1, cadd<T>(base, rot));
+        put(2, csub<T>(base, rot));
       } else {
         // generic radix (5, 7): direct r-point DFT with the twiddle table
         for (int u = 0; u < r; ++u) {
-          double2 acc = make_double2(0., 0.);
+          cx<T> acc = mk<T>(0, 0);
           for (int v = 0; v < r; ++v) {
-            double2 wv = __ldg(&pl.tw[((v * u) % r) * (m / r)]);
-            if (sign > 0) wv = cconj(wv);
-            acc = cadd(acc, cmul(ld2(B, cur, q + s * (p + v * mm), line), wv));
+            cx<T> wv = TW<T>(pl, ((v * u) % r) * (m / r));
+            if (sign > 0) wv = cconj<T>(wv);
+            acc = cadd<T>(acc, cmul<T>(ld2<T>(B, cur, q + s * (p + v * mm), line), wv));
           }
           put(u, acc);
         }
@@ -125,31 +149,34 @@ __device__ int fft_lines(const LinePlan& pl, const Bufs& B, int in, int L, int s
 }
 
 // post-processing of a forward real transform: X_k, k = 0..m, from Z
-__device__ __forceinline__ double2 real_fwd_X(const LinePlan& pl, const Bufs& B, int zb, int k, int line) {
+template <typename T>
+__device__ __forceinline__ cx<T> real_fwd_X(const LinePlan& pl, const Bufs<T>& B, int zb, int k, int line) {
   const int m = pl.m;
-  const double2 zk = ld2(B, zb, k % m, line);
-  const double2 zc = cconj(ld2(B, zb, (m - k) % m, line));
-  const double2 w = __ldg(&pl.tw2[k]);
-  const double2 sum = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-  const double2 dif = csub(zk, zc);
-  const double2 wd = cmul(w, dif);
+  const cx<T> zk = ld2<T>(B, zb, k % m, line);
+  const cx<T> zc = cconj<T>(ld2<T>(B, zb, (m - k) % m, line));
+  const cx<T> w = TW2<T>(pl, k);
+  const cx<T> sum = mk<T>((T)0.5 * (zk.x + zc.x), (T)0.5 * (zk.y + zc.y));
+  const cx<T> dif = csub<T>(zk, zc);
+  const cx<T> wd = cmul<T>(w, dif);
   // -i/2 * wd = (0.5*wd.y, -0.5*wd.x)
-  return make_double2(sum.x + 0.5 * wd.y, sum.y - 0.5 * wd.x);
+  return mk<T>(sum.x + (T)0.5 * wd.y, sum.y - (T)0.5 * wd.x);
 }
 
 // Z_k = (X_k + conj X_{m-k}) + i (X_k - conj X_{m-k}) conj(W^k), k = 0..m-1
-__device__ __forceinline__ double2 real_bwd_Z(const LinePlan& pl, double2 xk, double2 xmk, int k) {
-  const double2 xc = cconj(xmk);
-  const double2 w = cconj(__ldg(&pl.tw2[k]));
-  return cadd(cadd(xk, xc), mul_i(cmul(csub(xk, xc), w)));
+template <typename T>
+__device__ __forceinline__ cx<T> real_bwd_Z(const LinePlan& pl, cx<T> xk, cx<T> xmk, int k) {
+  const cx<T> xc = cconj<T>(xmk);
+  const cx<T> w = cconj<T>(TW2<T>(pl, k));
+  return cadd<T>(cadd<T>(xk, xc), mul_i<T>(cmul<T>(csub<T>(xk, xc), w)));
 }
 
 // packed spectrum of the periodic kind: complex index k -> X_k with
 // X_0 = (r0, 0), X_m = (r_m, 0) both held in complex slot 0
-__device__ __forceinline__ double2 packed_X(const Bufs& B, int b, int k, int m, int line) {
-  if (k == 0) return make_double2(B.re[b][line], 0.);
-  if (k == m) return make_double2(B.im[b][line], 0.);
-  return ld2(B, b, k, line);
+template <typename T>
+__device__ __forceinline__ cx<T> packed_X(const Bufs<T>& B, int b, int k, int m, int line) {
+  if (k == 0) return mk<T>(B.re[b][line], 0);
+  if (k == m) return mk<T>(B.im[b][line], 0);
+  return ld2<T>(B, b, k, line);
 }
 
 // ---------------------------------------------------------------------------
@@ -157,16 +184,16 @@ __device__ __forceinline__ double2 packed_X(const Bufs& B, int b, int k, int m, 
 // ---------------------------------------------------------------------------
 // forward: input real line in buffer 0 as pairs (x_2j, x_2j+1) (after the
 // kind's input reordering); output real line written through `out(line, s, v)`
-template <bool LF, typename OUT>
-__device__ void line_forward(const LinePlan& pl, const Bufs& B, int L, OUT out) {
+template <typename T, bool LF, typename OUT>
+__device__ void line_forward(const LinePlan& pl, const Bufs<T>& B, int L, OUT out) {
   const int m = pl.m, n = pl.n;
-  const int zb = fft_lines(pl, B, 0, L, -1);
+  const int zb = fft_lines<T>(pl, B, 0, L, -1);
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * m; it += blockDim.x) {
       const int line = LF ? it % L : it / m, k = LF ? it / L : it - line * m;
-      const double2 X = real_fwd_X(pl, B, zb, k, line);
+      const cx<T> X = real_fwd_X<T>(pl, B, zb, k, line);
       if (k == 0) {
-        const double2 Xm = real_fwd_X(pl, B, zb, m, line);
+        const cx<T> Xm = real_fwd_X<T>(pl, B, zb, m, line);
         out(line, 0, X.x);
         out(line, 1, Xm.x);
       } else {
@@ -178,13 +205,13 @@ __device__ void line_forward(const LinePlan& pl, const Bufs& B, int L, OUT out) 
     const bool dst = pl.kind == 2;
     for (int it = threadIdx.x; it < L * (m + 1); it += blockDim.x) {
       const int line = LF ? it % L : it / (m + 1), k = LF ? it / L : it - line * (m + 1);
-      const double2 V = real_fwd_X(pl, B, zb, k, line);
-      const double2 wk = __ldg(&pl.twc[k]);
-      const double yk = 2. * (wk.x * V.x - wk.y * V.y);
+      const cx<T> V = real_fwd_X<T>(pl, B, zb, k, line);
+      const cx<T> wk = TWC<T>(pl, k);
+      const T yk = (T)2 * (wk.x * V.x - wk.y * V.y);
       if (k < n) out(line, dst ? n - 1 - k : k, yk);
       if (k > 0 && k < m) {
-        const double2 wn = __ldg(&pl.twc[n - k]);
-        const double ynk = 2. * (wn.x * V.x + wn.y * V.y);  // Re(w_{n-k} conj(V_k))
+        const cx<T> wn = TWC<T>(pl, n - k);
+        const T ynk = (T)2 * (wn.x * V.x + wn.y * V.y);  // Re(w_{n-k} conj(V_k))
         out(line, dst ? k - 1 : n - k, ynk);
       }
     }
@@ -193,44 +220,44 @@ __device__ void line_forward(const LinePlan& pl, const Bufs& B, int L, OUT out) 
 
 // backward: input real line (packed spectrum or natural DCT/DST coefficients)
 // in buffer 1 as pairs; output real line through `out(line, i, v)`
-template <bool LF, typename OUT>
-__device__ void line_backward(const LinePlan& pl, const Bufs& B, int L, OUT out) {
+template <typename T, bool LF, typename OUT>
+__device__ void line_backward(const LinePlan& pl, const Bufs<T>& B, int L, OUT out) {
   const int m = pl.m, n = pl.n;
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * m; it += blockDim.x) {
       const int line = it % L, k = it / L;
-      st2(B, 0, k, line, real_bwd_Z(pl, packed_X(B, 1, k, m, line), packed_X(B, 1, m - k, m, line), k));
+      st2<T>(B, 0, k, line,
+             real_bwd_Z<T>(pl, packed_X<T>(B, 1, k, m, line), packed_X<T>(B, 1, m - k, m, line), k));
     }
   } else {
     const bool dst = pl.kind == 2;
     // X_k of the DCT-III (for the sine kind: the reversed input)
-    auto X = [&](int k, int line) -> double {
-      if (k >= n) return 0.;
-      return ldr(B, 1, dst ? n - 1 - k : k, line);
+    auto X = [&](int k, int line) -> T {
+      if (k >= n) return (T)0;
+      return ldr<T>(B, 1, dst ? n - 1 - k : k, line);
     };
-    auto V = [&](int k, int line) -> double2 {  // e^{i pi k/(2n)} (X_k - i X_{n-k})
-      const double2 w = cconj(__ldg(&pl.twc[k]));
-      const double2 a = make_double2(X(k, line), -X(n - k, line));
-      return cmul(w, a);
+    auto V = [&](int k, int line) -> cx<T> {  // e^{i pi k/(2n)} (X_k - i X_{n-k})
+      const cx<T> w = cconj<T>(TWC<T>(pl, k));
+      return cmul<T>(w, mk<T>(X(k, line), -X(n - k, line)));
     };
     for (int it = threadIdx.x; it < L * m; it += blockDim.x) {
       const int line = it % L, k = it / L;
-      st2(B, 0, k, line, real_bwd_Z(pl, V(k, line), V(m - k, line), k));
+      st2<T>(B, 0, k, line, real_bwd_Z<T>(pl, V(k, line), V(m - k, line), k));
     }
   }
   __syncthreads();
-  const int zb = fft_lines(pl, B, 0, L, +1);
+  const int zb = fft_lines<T>(pl, B, 0, L, +1);
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
       const int line = LF ? it % L : it / n, i = LF ? it / L : it - line * n;
-      out(line, i, ldr(B, zb, i, line));
+      out(line, i, ldr<T>(B, zb, i, line));
     }
   } else {
     const bool dst = pl.kind == 2;
     for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
       const int line = LF ? it % L : it / n, i = LF ? it / L : it - line * n;
       const int pos = (i & 1) ? n - 1 - (i >> 1) : (i >> 1);
-      double v = ldr(B, zb, pos, line);
+      T v = ldr<T>(B, zb, pos, line);
       if (dst && (i & 1)) v = -v;
       out(line, i, v);
     }
@@ -243,8 +270,9 @@ __device__ __forceinline__ int fwd_pos(int kind, int n, int i) {
   return (i & 1) ? n - 1 - (i >> 1) : (i >> 1);
 }
 
-__device__ __forceinline__ Bufs smem_bufs(double* sm, int m, int L) {
-  Bufs B;
+template <typename T>
+__device__ __forceinline__ Bufs<T> smem_bufs(T* sm, int m, int L) {
+  Bufs<T> B;
   B.LP = L | 1;
   const int sz = m * B.LP;
   B.re[0] = sm;
@@ -256,18 +284,19 @@ __device__ __forceinline__ Bufs smem_bufs(double* sm, int m, int L) {
 
 // ---------------------------------------------------------------------------
 // x transforms.  Lines = rows (j,k), L per CTA.
-// Forward input: the interior of a halo-layout field, or (FUSED) the
-// fillps right-hand side rho0*div(u)/dt computed on the fly
-// (src/fillps.f90:39-50) plus the updt_rhs_b planes.
+// Forward input: the interior of a halo-layout FP64 field, or (FUSED) the
+// fillps right-hand side rho0*div(u)/dt computed on the fly in FP64
+// (src/fillps.f90:39-50).
 // ---------------------------------------------------------------------------
-template <bool FUSED>
+template <typename T, bool FUSED>
 __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
     const double* __restrict__ src, const double* __restrict__ u, const double* __restrict__ v,
-    const double* __restrict__ w, Phys ph, double* __restrict__ work, int L) {
+    const double* __restrict__ w, Phys ph, T* __restrict__ work, int L) {
   if (HALTED(sc)) return;
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const int n = pl.n, m = pl.m;
-  const Bufs B = smem_bufs(sm, m < 1 ? 1 : m, L);
+  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int nlines = g.ny * g.nz;
   const int l0 = blockIdx.x * L;
   const double dti = FUSED ? sc->dti : 0.;
@@ -286,73 +315,77 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const Dev
         x = __ldg(src + c);
       }
     }
-    double xv = x;
+    T xv = (T)x;
     if (pl.kind == 2 && (i & 1)) xv = -xv;  // sine kind: negate odd samples
-    str(B, 0, fwd_pos(pl.kind, n, i), line, xv);
+    str<T>(B, 0, fwd_pos(pl.kind, n, i), line, xv);
   }
   __syncthreads();
-  line_forward<false>(pl, B, L, [&](int line, int s, double val) {
+  line_forward<T, false>(pl, B, L, [&](int line, int s, T val) {
     const int gl = l0 + line;
     if (gl < nlines) work[(size_t)gl * n + s] = val;
   });
 }
 
+// ADD: dst += normfft * x (refinement correction) instead of dst = normfft * x
+template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
-    const double* __restrict__ work, double normfft, double* __restrict__ dst, int L) {
+    const T* __restrict__ work, double normfft, double* __restrict__ dst, int L) {
   if (HALTED(sc)) return;
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const int n = pl.n, m = pl.m;
-  const Bufs B = smem_bufs(sm, m < 1 ? 1 : m, L);
+  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int nlines = g.ny * g.nz;
   const int l0 = blockIdx.x * L;
   for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
     const int line = it / n, s = it - line * n;
     const int gl = l0 + line;
-    str(B, 1, s, line, gl < nlines ? __ldg(work + (size_t)gl * n + s) : 0.);
+    str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
   }
   __syncthreads();
-  line_backward<false>(pl, B, L, [&](int line, int i, double val) {
+  line_backward<T, false>(pl, B, L, [&](int line, int i, T val) {
     const int gl = l0 + line;
     if (gl < nlines) {
       const int j = gl % g.ny + 1, k = gl / g.ny + 1;
-      dst[g.h(i + 1, j, k)] = val * normfft;
+      const int c = g.h(i + 1, j, k);
+      if (ADD) dst[c] = dst[c] + (double)val * normfft;
+      else dst[c] = (double)val * normfft;
     }
   });
 }
 
 // ---------------------------------------------------------------------------
-// y transforms, in place on the spectral buffer.  Lines = TL consecutive x
+// y transforms, in place on the spectral buffer.  Lines = L consecutive x
 // positions of one z plane; the tile is read and written row by row.
 // ---------------------------------------------------------------------------
-template <int DIR>
+template <typename T, int DIR>
 __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
-                                               double* __restrict__ work, int L) {
+                                               T* __restrict__ work, int L) {
   if (HALTED(sc)) return;
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const int n = pl.n, m = pl.m, nx = g.nx;
-  const Bufs B = smem_bufs(sm, m < 1 ? 1 : m, L);
+  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int i0 = blockIdx.x * L, k = blockIdx.y;
-  double* plane = work + (size_t)k * nx * n;
-  const int buf = DIR > 0 ? 0 : 1;
+  T* plane = work + (size_t)k * nx * n;
   for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
     const int line = it % L, j = it / L;
     const int i = i0 + line;
-    double x = i < nx ? plane[(size_t)j * nx + i] : 0.;
+    T x = i < nx ? plane[(size_t)j * nx + i] : (T)0;
     if (DIR > 0) {
       if (pl.kind == 2 && (j & 1)) x = -x;
-      str(B, 0, fwd_pos(pl.kind, n, j), line, x);
+      str<T>(B, 0, fwd_pos(pl.kind, n, j), line, x);
     } else {
-      str(B, 1, j, line, x);
+      str<T>(B, 1, j, line, x);
     }
   }
   __syncthreads();
-  (void)buf;
-  auto out = [&](int line, int j, double val) {
+  auto out = [&](int line, int j, T val) {
     const int i = i0 + line;
     if (i < nx) plane[(size_t)j * nx + i] = val;
   };
-  if (DIR > 0) line_forward<true>(pl, B, L, out);
-  else line_backward<true>(pl, B, L, out);
+  if (DIR > 0) line_forward<T, true>(pl, B, L, out);
+  else line_backward<T, true>(pl, B, L, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -360,37 +393,57 @@ __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScal
 // 151-177 / src/solver_gpu.f90:179-203).  One column per thread; the forward
 // sweep writes p' in place and keeps d only at chunk ends (shared memory);
 // the backward sweep recomputes d per chunk from those checkpoints with the
-// same operations, so it equals the stored one bit for bit.  The pivots use
-// round-to-nearest intrinsics (no FMA contraction), as the reference's CPU
-// build evaluates them.
+// same operations, so it equals the stored one bit for bit.  In FP64 the
+// pivots use round-to-nearest intrinsics (no FMA contraction), as the
+// reference's CPU build evaluates them.  In FP32 the eps shift vanishes, so
+// the singular (0,0) column of an all-Neumann/periodic problem pins its last
+// unknown to zero instead (any constant solves it).
 // ---------------------------------------------------------------------------
 #define ZCH 16
 
-__device__ __forceinline__ double piv_inv(double bl, double lam, double al, double dprev) {
-  // 1./(b(l)+lambda - a(l)*d(l-1) + eps)
-  return __ddiv_rn(1.0, __dadd_rn(__dsub_rn(__dadd_rn(bl, lam), __dmul_rn(al, dprev)), CANSFZ_EPS));
+template <typename T> struct Rn;
+template <> struct Rn<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <> struct Rn<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+
+// 1./(b(l)+lambda - a(l)*d(l-1) + eps); `pin`: singular column, last row
+template <typename T>
+__device__ __forceinline__ T piv_inv(int l, int n, T bl, T lam, T al, T dprev, bool pin) {
+  typedef Rn<T> R;
+  if (pin && l == n - 1) return (T)0;
+  if (l == 0) return R::div((T)1, R::add(R::add(bl, lam), (T)CANSFZ_EPS));
+  return R::div((T)1, R::add(R::sub(R::add(bl, lam), R::mul(al, dprev)), (T)CANSFZ_EPS));
 }
 
+template <typename T>
 __device__ void thomas_column(int n, const double* __restrict__ a, const double* __restrict__ b,
-                              const double* __restrict__ c, double lam, double* __restrict__ col,
-                              size_t st, double* __restrict__ dchk, int tpitch) {
+                              const double* __restrict__ c, T lam, T* __restrict__ col, size_t st,
+                              T* __restrict__ dchk, int tpitch, bool pin) {
+  typedef Rn<T> R;
   // forward elimination
-  double dprev = 0., pprev = 0.;
+  T dprev = 0, pprev = 0;
   const int nch = (n + ZCH - 1) / ZCH;
   for (int ch = 0; ch < nch; ++ch) {
     const int k0 = ch * ZCH;
-    double pv[ZCH];
+    T pv[ZCH];
 #pragma unroll
-    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : 0.;
+    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : (T)0;
 #pragma unroll
     for (int q = 0; q < ZCH; ++q) {
       const int l = k0 + q;
       if (l < n) {
-        double z;
-        if (l == 0) z = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(b[0], lam), CANSFZ_EPS));
-        else z = piv_inv(b[l], lam, a[l], dprev);
-        const double d = __dmul_rn(c[l], z);
-        const double pn = (l == 0) ? __dmul_rn(pv[q], z) : __dmul_rn(__dsub_rn(pv[q], __dmul_rn(a[l], pprev)), z);
+        const T z = piv_inv<T>(l, n, (T)b[l], lam, (T)a[l], dprev, pin);
+        const T d = R::mul((T)c[l], z);
+        const T pn = (l == 0) ? R::mul(pv[q], z) : R::mul(R::sub(pv[q], R::mul((T)a[l], pprev)), z);
         dprev = d;
         pprev = pn;
         pv[q] = pn;
@@ -402,31 +455,26 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
     dchk[ch * tpitch] = dprev;  // d at the last element of chunk ch
   }
   // backward substitution, chunk by chunk from the top
-  double pnext = 0.;
+  T pnext = 0;
   for (int ch = nch - 1; ch >= 0; --ch) {
     const int k0 = ch * ZCH;
-    double dd[ZCH], pv[ZCH];
-    double dp = ch > 0 ? dchk[(ch - 1) * tpitch] : 0.;
+    T dd[ZCH], pv[ZCH];
+    T dp = ch > 0 ? dchk[(ch - 1) * tpitch] : (T)0;
 #pragma unroll
     for (int q = 0; q < ZCH; ++q) {
       const int l = k0 + q;
-      double d = 0.;
-      if (l < n) {
-        double z;
-        if (l == 0) z = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(b[0], lam), CANSFZ_EPS));
-        else z = piv_inv(b[l], lam, a[l], dp);
-        d = __dmul_rn(c[l], z);
-      }
+      T d = 0;
+      if (l < n) d = R::mul((T)c[l], piv_inv<T>(l, n, (T)b[l], lam, (T)a[l], dp, pin));
       dd[q] = d;
       dp = d;
     }
 #pragma unroll
-    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : 0.;
+    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : (T)0;
 #pragma unroll
     for (int q = ZCH - 1; q >= 0; --q) {
       const int l = k0 + q;
       if (l < n) {
-        if (l < n - 1) pv[q] = __dsub_rn(pv[q], __dmul_rn(dd[q], pnext));
+        if (l < n - 1) pv[q] = R::sub(pv[q], R::mul(dd[q], pnext));
         pnext = pv[q];
       }
     }
@@ -436,41 +484,70 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
   }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(128) k_zsolve(int ncol, int nz, const double* __restrict__ lam,
     const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
-    const DevScalars* __restrict__ sc, double* __restrict__ work) {
+    const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
   if (HALTED(sc)) return;
-  extern __shared__ double dchk[];  // [nch][blockDim]
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* dchk = reinterpret_cast<T*>(smraw);  // [nch][blockDim]
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
-  thomas_column(nz, a, b, c, __ldg(lam + col), work + col, (size_t)ncol, dchk + threadIdx.x, blockDim.x);
+  const double lm = __ldg(lam + col);
+  const bool pin = (sizeof(T) == 4) && zsing && lm == 0.;
+  thomas_column<T>(nz, a, b, c, (T)lm, work + col, (size_t)ncol, dchk + threadIdx.x, blockDim.x, pin);
 }
 
 // periodic z: gaussel_periodic (src/solver.f90:107-149)
+template <typename T>
 __global__ void __launch_bounds__(128) k_zsolve_periodic(int ncol, int nz, const double* __restrict__ lam,
     const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
-    const DevScalars* __restrict__ sc, double* __restrict__ work, double* __restrict__ work2) {
+    const DevScalars* __restrict__ sc, T* __restrict__ work, T* __restrict__ work2) {
   if (HALTED(sc)) return;
-  extern __shared__ double dchk[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* dchk = reinterpret_cast<T*>(smraw);
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   const int n = nz;
-  const double lm = __ldg(lam + col);
-  double* p = work + col;
-  double* p2 = work2 + col;
+  const double lmd = __ldg(lam + col);
+  const T lm = (T)lmd;
+  T* p = work + col;
+  T* p2 = work2 + col;
   const size_t st = (size_t)ncol;
   // p1 = solution of the (n-1) system with the RHS, in place
-  thomas_column(n - 1, a, b, c, lm, p, st, dchk + threadIdx.x, blockDim.x);
+  thomas_column<T>(n - 1, a, b, c, lm, p, st, dchk + threadIdx.x, blockDim.x, false);
   // p2 = solution with the spike RHS
-  for (int k = 0; k < n - 1; ++k) p2[(size_t)k * st] = 0.;
-  p2[0] = -a[0];
-  p2[(size_t)(n - 2) * st] = -c[n - 2];
-  thomas_column(n - 1, a, b, c, lm, p2, st, dchk + threadIdx.x, blockDim.x);
-  const double bbn = b[n - 1] + lm;
-  const double pn = (p[(size_t)(n - 1) * st] - c[n - 1] * p[0] - a[n - 1] * p[(size_t)(n - 2) * st]) /
-                    (bbn + c[n - 1] * p2[0] + a[n - 1] * p2[(size_t)(n - 2) * st] + CANSFZ_EPS);
+  for (int k = 0; k < n - 1; ++k) p2[(size_t)k * st] = 0;
+  p2[0] = (T)-a[0];
+  p2[(size_t)(n - 2) * st] = (T)-c[n - 2];
+  thomas_column<T>(n - 1, a, b, c, lm, p2, st, dchk + threadIdx.x, blockDim.x, false);
+  const T bbn = (T)b[n - 1] + lm;
+  const T den = bbn + (T)c[n - 1] * p2[0] + (T)a[n - 1] * p2[(size_t)(n - 2) * st] + (T)CANSFZ_EPS;
+  T pn = (p[(size_t)(n - 1) * st] - (T)c[n - 1] * p[0] - (T)a[n - 1] * p[(size_t)(n - 2) * st]) / den;
+  if (sizeof(T) == 4 && lmd == 0.) pn = 0;  // FP32: pin the singular mode
   p[(size_t)(n - 1) * st] = pn;
   for (int k = 0; k < n - 1; ++k) p[(size_t)k * st] = p[(size_t)k * st] + p2[(size_t)k * st] * pn;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 residual of the discrete operator the spectral solve inverts: the
+// 7-point Laplacian with the BC ghosts of cbcpre (chk_poisson,
+// src/debug.f90:100-106).  res = rhs - L(phi) on the interior; phi's ghost
+// layer must be filled (boundp) before.
+// ---------------------------------------------------------------------------
+__global__ void k_residual(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ rhs,
+                           const double* __restrict__ phi, double* __restrict__ res) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > g.nx) return;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  const int c = g.h(i, j, k);
+  const double pc = __ldg(phi + c);
+  const double lap = (__ldg(phi + c + 1) - 2. * pc + __ldg(phi + c - 1)) * (g.dxi * g.dxi) +
+                     (__ldg(phi + c + g.sx) - 2. * pc + __ldg(phi + c - g.sx)) * (g.dyi * g.dyi) +
+                     ((__ldg(phi + c + g.sxy) - pc) * g.dzci[k] - (pc - __ldg(phi + c - g.sxy)) * g.dzci[k - 1]) *
+                         g.dzfi[k];
+  res[c] = __ldg(rhs + c) - lap;
 }
 
 // ---------------------------------------------------------------------------
@@ -479,76 +556,99 @@ __global__ void __launch_bounds__(128) k_zsolve_periodic(int ncol, int nz, const
 // opt the transform kernels into > 48 KB of dynamic shared memory (once)
 void poisson_set_attributes() {
   const int lim = 100 * 1024;
-  cudaFuncSetAttribute(k_fft_x_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fft_x_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fft_x_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fft_y<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fft_y<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+#define ATTR(k) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)
+  ATTR((k_fft_x_fwd<double, true>));
+  ATTR((k_fft_x_fwd<double, false>));
+  ATTR((k_fft_x_fwd<float, true>));
+  ATTR((k_fft_x_fwd<float, false>));
+  ATTR((k_fft_x_bwd<double, false>));
+  ATTR((k_fft_x_bwd<double, true>));
+  ATTR((k_fft_x_bwd<float, false>));
+  ATTR((k_fft_x_bwd<float, true>));
+  ATTR((k_fft_y<double, 1>));
+  ATTR((k_fft_y<double, -1>));
+  ATTR((k_fft_y<float, 1>));
+  ATTR((k_fft_y<float, -1>));
+#undef ATTR
 }
 
+template <typename T>
 static int lines_per_cta(int m, int maxL) {
-  // keep 4*m*LP doubles within ~96 KB
+  // keep the 4*m*LP elements of shared memory within ~96 KB
   int L = maxL;
-  while (L > 1 && 4 * (size_t)m * (L | 1) * 8 > 96 * 1024) L >>= 1;
+  while (L > 1 && 4 * (size_t)m * (L | 1) * sizeof(T) > 96 * 1024) L >>= 1;
   return L;
 }
 
+template <typename T> static T* wbuf(const PoissonPlan& pl);
+template <> double* wbuf<double>(const PoissonPlan& pl) { return pl.work; }
+template <> float* wbuf<float>(const PoissonPlan& pl) { return pl.workf; }
+template <typename T> static T* wbuf2(const PoissonPlan& pl);
+template <> double* wbuf2<double>(const PoissonPlan& pl) { return pl.work2; }
+template <> float* wbuf2<float>(const PoissonPlan& pl) { return pl.work2f; }
+
+template <typename T>
 static void x_forward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                       const double* src, const double* u, const double* v, const double* w, const Phys* ph,
                       bool fused) {
   const int m = pl.px.m < 1 ? 1 : pl.px.m;
-  const int L = lines_per_cta(m, pl.px.n >= 128 ? 8 : 32);
-  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(double);
+  const int L = lines_per_cta<T>(m, pl.px.n >= 128 ? 8 : 32);
+  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
   const dim3 grid((nlines + L - 1) / L);
   Phys pz{};
   if (fused)
-    k_fft_x_fwd<true><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, nullptr, u, v, w, *ph, pl.work, L);
+    k_fft_x_fwd<T, true><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, nullptr, u, v, w, *ph, wbuf<T>(pl), L);
   else
-    k_fft_x_fwd<false><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, src, nullptr, nullptr, nullptr, pz, pl.work, L);
+    k_fft_x_fwd<T, false><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, src, nullptr, nullptr, nullptr, pz,
+                                                      wbuf<T>(pl), L);
 }
 
+template <typename T>
 static void y_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
   const int m = pl.py.m < 1 ? 1 : pl.py.m;
-  const int L = lines_per_cta(m, 16);
-  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(double);
+  const int L = lines_per_cta<T>(m, 16);
+  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const dim3 grid((g.nx + L - 1) / L, g.nz);
-  if (dir > 0) k_fft_y<1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, pl.work, L);
-  else k_fft_y<-1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, pl.work, L);
+  if (dir > 0) k_fft_y<T, 1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
+  else k_fft_y<T, -1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
 }
 
+template <typename T>
 static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
   const int tb = 128;
   const int nch = (g.nz + ZCH - 1) / ZCH;
-  const size_t smem = (size_t)nch * tb * sizeof(double);
+  const size_t smem = (size_t)nch * tb * sizeof(T);
   if (pl.zper)
-    k_zsolve_periodic<<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc, pl.work,
-                                                                  pl.work2);
+    k_zsolve_periodic<T><<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc,
+                                                                     wbuf<T>(pl), wbuf2<T>(pl));
   else
-    k_zsolve<<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc, pl.work);
+    k_zsolve<T><<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl),
+                                                            pl.zsing);
 }
 
+template <typename T, bool ADD>
 static void x_backward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* dst) {
   const int m = pl.px.m < 1 ? 1 : pl.px.m;
-  const int L = lines_per_cta(m, pl.px.n >= 128 ? 8 : 32);
-  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(double);
+  const int L = lines_per_cta<T>(m, pl.px.n >= 128 ? 8 : 32);
+  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
-  k_fft_x_bwd<<<(nlines + L - 1) / L, 256, smem, Lc.st>>>(g, pl.px, sc, pl.work, pl.normfft, dst, L);
+  k_fft_x_bwd<T, ADD><<<(nlines + L - 1) / L, 256, smem, Lc.st>>>(g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L);
 }
 
 // solver_gpu on the interior of the halo-layout field p (in place)
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* p,
                     const StageMark* mk) {
-  x_forward(L, g, pl, sc, p, nullptr, nullptr, nullptr, nullptr, false);
+  x_forward<double>(L, g, pl, sc, p, nullptr, nullptr, nullptr, nullptr, false);
   if (mk) mk->mark("poisson_x_fwd");
-  y_pass(L, g, pl, sc, +1);
+  y_pass<double>(L, g, pl, sc, +1);
   if (mk) mk->mark("poisson_y_fwd");
-  z_pass(L, g, pl, sc);
+  z_pass<double>(L, g, pl, sc);
   if (mk) mk->mark("poisson_z_solve");
-  y_pass(L, g, pl, sc, -1);
+  y_pass<double>(L, g, pl, sc, -1);
   if (mk) mk->mark("poisson_y_bwd");
-  x_backward(L, g, pl, sc, p);
+  x_backward<double, false>(L, g, pl, sc, p);
   if (mk) mk->mark("poisson_x_bwd");
 }
 
@@ -558,16 +658,34 @@ void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& 
                               const DevScalars* sc, const double* u, const double* v, const double* w,
                               const double* rhsb_planes, double* phi, const StageMark* mk) {
   (void)rhsb_planes;
-  x_forward(L, g, pl, sc, nullptr, u, v, w, &ph, true);
+  x_forward<double>(L, g, pl, sc, nullptr, u, v, w, &ph, true);
   if (mk) mk->mark("poisson_x_fwd_fillps");
-  y_pass(L, g, pl, sc, +1);
+  y_pass<double>(L, g, pl, sc, +1);
   if (mk) mk->mark("poisson_y_fwd");
-  z_pass(L, g, pl, sc);
+  z_pass<double>(L, g, pl, sc);
   if (mk) mk->mark("poisson_z_solve");
-  y_pass(L, g, pl, sc, -1);
+  y_pass<double>(L, g, pl, sc, -1);
   if (mk) mk->mark("poisson_y_bwd");
-  x_backward(L, g, pl, sc, phi);
+  x_backward<double, false>(L, g, pl, sc, phi);
   if (mk) mk->mark("poisson_x_bwd");
+}
+
+// FP32 spectral solve of the mixed form: dst = S(src), or dst += S(src) (add)
+void launch_poisson_f32(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                        const double* src, double* dst, bool add, const StageMark* mk) {
+  x_forward<float>(L, g, pl, sc, src, nullptr, nullptr, nullptr, nullptr, false);
+  y_pass<float>(L, g, pl, sc, +1);
+  z_pass<float>(L, g, pl, sc);
+  y_pass<float>(L, g, pl, sc, -1);
+  if (add) x_backward<float, true>(L, g, pl, sc, dst);
+  else x_backward<float, false>(L, g, pl, sc, dst);
+  if (mk) mk->mark(add ? "poisson_f32_correction" : "poisson_f32");
+}
+
+void launch_residual(const Launch& L, const Geo& g, const DevScalars* sc, const double* rhs, const double* phi,
+                     double* res) {
+  const int bx = g.nx >= 128 ? 128 : (g.nx >= 64 ? 64 : 32);
+  k_residual<<<dim3((g.nx + bx - 1) / bx, g.ny, g.nz), bx, 0, L.st>>>(g, sc, rhs, phi, res);
 }
 
 }  // namespace cansfz

@@ -255,6 +255,15 @@ int cansfz_kernels_per_step(cansfz_ctx* ctx, int* count);
 int cansfz_profile_stages(cansfz_ctx* ctx, int nsteps, double* ms, int maxstages,
                           int* nstages, char* names, int cap);
 
+/* ---- mixed form (no reference counterpart) ------------------------------
+ * FP32 spectral solve of the same discrete operator as cansfz_solver, then
+ * `sweeps` refinement sweeps p += S32(rhs - L(p)) with the FP64 residual of
+ * the 7-point Laplacian.  rhs and p: halo-layout device fields (p's ghost
+ * layer is filled on return).  Homogeneous pressure BCs only.             */
+int cansfz_solver_refined(cansfz_ctx* ctx, const double* rhs, double* p, int sweeps);
+/* FP64 residual res = rhs - L(p) of that operator (p's ghosts are filled). */
+int cansfz_poisson_residual(cansfz_ctx* ctx, const double* rhs, double* p, double* res);
+
 #ifdef __cplusplus
 }
 #endif

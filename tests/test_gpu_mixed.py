@@ -1,0 +1,83 @@
+"""The mixed-precision form against the FP64 drop-in and the oracle.
+
+* Poisson only (the 256^3 configuration at a reduced size): FP32 spectral
+  solve plus 0-3 FP64-residual refinement sweeps vs the FP64 solve; the
+  error must fall with each sweep and reach FP64 level by the third.
+* Whole steps: the mixed form (FP32 transforms + 2 sweeps) vs the FP64
+  oracle, error within the 1e-6 relative bound stated for that form.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cansfz import case as C
+from cansfz import init, namelist, params, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _poisson_pair(n=64, seed=2026, cbc="PPPPNN"):
+    p, rhs = workloads.poisson_rhs(n, seed)
+    if cbc != "PPPPNN":
+        p.cbcpre = cbc.encode()
+    return p, rhs
+
+
+@pytest.mark.parametrize("cbc", ["PPPPNN", "NNPPNN", "PPPPPP"])
+def test_refinement_converges(cbc):
+    p, rhs = _poisson_pair(64, 2026, cbc)
+    g = C.Case(p)
+    ref = g.field(rhs)
+    g.call("solver", ref)
+    a64 = ref.get()[1:-1, 1:-1, 1:-1]
+    a64 = a64 - a64.mean()
+    errs = []
+    res_norms = []
+    for sweeps in range(4):
+        src = g.field(rhs)
+        out = g.field()
+        g.call("solver_refined", src, out, sweeps)
+        b = out.get()[1:-1, 1:-1, 1:-1]
+        b = b - b.mean()
+        errs.append(np.abs(b - a64).max() / np.abs(a64).max())
+        r = g.field()
+        g.call("poisson_residual", src, out, r)
+        rr = r.get()[1:-1, 1:-1, 1:-1]
+        res_norms.append(np.abs(rr).max() / np.abs(rhs).max())
+    assert errs[0] < 1e-4, errs
+    assert errs[1] < errs[0] * 1e-2, errs
+    assert errs[2] < 1e-11 or errs[2] < errs[1] * 1e-2, errs
+    assert res_norms[3] < 1e-11, res_norms
+
+
+def _step_params(n=32, mixed=True, sweeps=2):
+    p, f = workloads.droplets((n, n, n), (1.0, 1.0, 1.0), False, count=6, rmin=0.1, rmax=0.15, seed=3)
+    if mixed:
+        p.form = 1
+        p.refine_sweeps = sweeps
+    return p, f
+
+
+def test_mixed_step_error_vs_oracle():
+    p, f = _step_params(32, True, 2)
+    g = C.Case(p)
+    g.set_fields(*f)
+    g.prepare()
+    p64 = p.copy()
+    p64.form = 0
+    o = O.Case(p64)
+    for nm, a in zip(("u", "v", "w", "p", "psi"), f):
+        o.set(nm, a)
+    o.prepare()
+    assert g.step(10) == 0 and o.step(10) == 0
+    for nm in ("u", "v", "w", "psi"):
+        a, b = g.get(nm), o.get(nm)
+        e = np.abs(a - b).max() / np.abs(b).max()
+        assert e < 1e-6, (nm, e)
+    pa, pb = g.get("p")[1:-1, 1:-1, 1:-1], o.get("p")[1:-1, 1:-1, 1:-1]
+    pa, pb = pa - pa.mean(), pb - pb.mean()
+    assert np.abs(pa - pb).max() / np.abs(pb).max() < 1e-6
+    d = g.diag()
+    assert d.divmax < 1e-10

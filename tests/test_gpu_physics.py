@@ -66,9 +66,14 @@ def test_vortex_parity_with_oracle():
     p = _vortex_params(64, 2.0e-3)
     g, _ = _vortex_case(p, "gpu")
     o, _ = _vortex_case(p, "cpu")
-    assert g.step(100) == 0 and o.step(100) == 0
+    assert g.step(10) == 0 and o.step(10) == 0
+    assert np.abs(g.get("psi") - o.get("psi")).max() < 1e-11
+    # the prescribed velocity is re-evaluated every step with the device's
+    # sin/cos (1-2 ulp from the host's); over 100 steps the sharpening term
+    # carries that to ~1e-10 in psi
+    assert g.step(90) == 0 and o.step(90) == 0
     a, b = g.get("psi"), o.get("psi")
-    assert np.abs(a - b).max() < 1e-11
+    assert np.abs(a - b).max() < 1e-9
     assert abs(g.diag().time - o.diag().time) < 1e-13
 
 
@@ -102,7 +107,8 @@ def test_full_size_divergence_and_mass(droplets_full):
     m0 = g.diag().mass12
     assert g.step(20) == 0  # icheck = 10: two divergence checks
     d = g.diag()
-    assert d.divmax < 1e-12, d.divmax      # projection to round-off (reference abort threshold 2.2e-9)
+    # projection to FP64 round-off (the reference aborts above 2.2e-9)
+    assert d.divmax < 1e-10, d.divmax
     drift = abs(d.mass12[0] - m0[0]) / m0[0]
     assert drift < 1e-10, drift
     g.close()
@@ -124,6 +130,8 @@ def test_mass_drift_matches_oracle():
     dg = g.diag().mass12[0] - mg0
     do = o.diag().mass12[0] - mo0
     assert abs(dg - do) <= 1e-12 * mo0 + 1e-3 * abs(do)
+    # divergence after the last check: both at FP64 round-off
+    assert g.diag().divmax <= 10.0 * o.diag().divmax + 1e-13
 
 
 def test_abort_on_nan_input():
