@@ -63,6 +63,9 @@ def parse_args():
     ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", type=int, default=256, help="cube size of the droplet workload (profiling runs)")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--sweeps", type=int, default=2, help="refinement sweeps of the mixed form")
     return ap.parse_args()
 
 
@@ -192,7 +195,13 @@ def gpu_arm(args):
     from cansfz import workloads as W
 
     rank, world, local = dist_setup(args.gpus)
-    p, fields = W.droplets_acdi(seed=2026)
+    if args.grid == 256:
+        p, fields = W.droplets_acdi(seed=2026)
+    else:
+        p, fields = W.droplets((args.grid,) * 3, (1.0, 1.0, 1.0), False, seed=2026)
+    if args.form == "mixed":
+        p.form = 1
+        p.refine_sweeps = args.sweeps
     nx, ny, nz = p.n
     cells = nx * ny * nz
     case = C.Case(p)
@@ -250,8 +259,10 @@ def gpu_arm(args):
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": WORKLOAD, "grid": [nx, ny, nz], "form": "fp64 (drop-in)",
+        "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64 state / f32 transforms", "data": DATA,
+        "config": {"workload": WORKLOAD if args.grid == 256 else f"droplets_acdi at {args.grid}^3 (profiling size)",
+                   "grid": [nx, ny, nz],
+                   "form": "fp64 (drop-in)" if args.form == "fp64" else f"mixed (FP32 transforms + {args.sweeps} sweeps)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (each FP64 field 137 MB > 126 MB)",
                    "final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},

@@ -57,7 +57,7 @@ struct DevScalars {
 // ---------------------------------------------------------------------------
 struct Phys {
   double rho12[2], mu12[2];
-  double rho0;
+  double rho0, irho0;          // rho0 = min(rho12) and its reciprocal
   double sigma, surf_factor;   // sigma or sigma*2/(rho1+rho2) (Brackbill)
   double bforce[3], gacc[3];
   double gam_factor, gam_min;
@@ -199,9 +199,9 @@ void launch_copy(const Launch& L, size_t n, const double* src, double* dst);
 void launch_fill(const Launch& L, size_t n, double val, double* dst);
 
 // reductions: results land in DevScalars
-void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
+void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                   const double* u, const double* v, const double* w, bool apply_floor);
-void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
+void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                   const double* u, const double* v, const double* w, bool only_on_check);
 void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial,
                    const double* u, const double* v, const double* w, bool only_on_check);

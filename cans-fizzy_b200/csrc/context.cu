@@ -548,9 +548,9 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     MARK("bc_p");
   }
   launch_step_end(L, c->ph, sc);
-  if (c->ph.acdi) launch_gamma(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
+  if (c->ph.acdi) launch_gamma(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
   MARK("gamma");
-  launch_chkdt(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], true);
+  launch_chkdt(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
   launch_chkdiv(L, g, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
   MARK("chkdt_chkdiv");
 #undef MARK
@@ -647,6 +647,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   Phys& ph = c->ph;
   for (int q = 0; q < 2; ++q) { ph.rho12[q] = P.rho12[q]; ph.mu12[q] = P.mu12[q]; }
   ph.rho0 = std::min(P.rho12[0], P.rho12[1]);
+  ph.irho0 = 1. / ph.rho0;
   ph.sigma = P.sigma;
   ph.brackbill = P.brackbill ? 1 : 0;
   ph.surf_factor = ph.brackbill ? P.sigma * 2. / (P.rho12[0] + P.rho12[1]) : P.sigma;
@@ -792,8 +793,8 @@ int cansfz_prepare(cansfz_ctx* c) {
   run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
              bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
          sc);
-  if (c->ph.acdi) launch_gamma(L, c->g, c->ph, sc, c->u[a], c->v[a], c->w[a], true);
-  launch_chkdt(L, c->g, c->ph, sc, c->u[a], c->v[a], c->w[a], false);
+  if (c->ph.acdi) launch_gamma(L, c->g, c->ph, sc, c->partial, c->u[a], c->v[a], c->w[a], true);
+  launch_chkdt(L, c->g, c->ph, sc, c->partial, c->u[a], c->v[a], c->w[a], false);
   // dto = dt (src/main.f90:409)
   if (int rc = sync_status(c)) return rc;
   c->sc_host->dto = c->sc_host->dt;
@@ -945,7 +946,7 @@ int cansfz_acdi_set_gamma(cansfz_ctx* c, double gam_factor, const double* u, con
   if (int rc = call_scalars(c, h)) return rc;
   Phys ph = c->ph;
   ph.gam_factor = gam_factor;
-  launch_gamma(c->L, c->g, ph, c->sc_call, u, v, w, false);
+  launch_gamma(c->L, c->g, ph, c->sc_call, c->partial, u, v, w, false);
   DevScalars r{};
   CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -1077,7 +1078,7 @@ int cansfz_chkdt(cansfz_ctx* c, const double* u, const double* v, const double* 
   DevScalars h{};
   h.gam = gam; h.seps = seps;
   if (int rc = call_scalars(c, h)) return rc;
-  launch_chkdt(c->L, c->g, c->ph, c->sc_call, u, v, w, false);
+  launch_chkdt(c->L, c->g, c->ph, c->sc_call, c->partial, u, v, w, false);
   DevScalars r{};
   CK(cudaMemcpyAsync(&r, c->sc_call, sizeof(r), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));

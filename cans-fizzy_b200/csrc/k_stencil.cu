@@ -86,12 +86,13 @@ __global__ void __launch_bounds__(128) k_acdi_transport(Geo g, const DevScalars*
   if (SDF) {
     const double phi_ccc = LD(phi, c);
     const double qg = 0.25 * gam;
-    sharpxm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - 1)) / seps))) * rn_01);
-    sharpxp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + 1) + phi_ccc) / seps))) * rn_11);
-    sharpym = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sx)) / seps))) * rn_02);
-    sharpyp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sx) + phi_ccc) / seps))) * rn_12);
-    sharpzm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sxy)) / seps))) * rn_03);
-    sharpzp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sxy) + phi_ccc) / seps))) * rn_13);
+    const double is = 1. / seps;  // (0.25*(a+b))/seps as (0.25*(a+b))*(1/seps)
+    sharpxm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - 1)) * is))) * rn_01);
+    sharpxp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + 1) + phi_ccc) * is))) * rn_11);
+    sharpym = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sx)) * is))) * rn_02);
+    sharpyp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sx) + phi_ccc) * is))) * rn_12);
+    sharpzm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sxy)) * is))) * rn_03);
+    sharpzp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sxy) + phi_ccc) * is))) * rn_13);
   } else {
     const double psi_xm = 0.5 * (psi_ccc + psi_mcc), psi_xp = 0.5 * (psi_pcc + psi_ccc);
     const double psi_ym = 0.5 * (psi_ccc + psi_cmc), psi_yp = 0.5 * (psi_cpc + psi_ccc);
@@ -329,15 +330,17 @@ __global__ void __launch_bounds__(128) k_youngs(Geo g, const DevScalars* __restr
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const double norm = sqrt(sq(mx[q]) + sq(my[q]) + sq(mz[q])) + CANSFZ_EPS;
-    mx[q] = mx[q] / norm; my[q] = my[q] / norm; mz[q] = mz[q] / norm;
+    const double inv = 1. / norm;  // one FP64 division instead of three (within 1 ulp of x/norm)
+    mx[q] = mx[q] * inv; my[q] = my[q] * inv; mz[q] = mz[q] * inv;
   }
   const double norm_x = .125 * (mx[0] + mx[1] + mx[2] + mx[3] + mx[4] + mx[5] + mx[6] + mx[7]);
   const double norm_y = .125 * (my[0] + my[1] + my[2] + my[3] + my[4] + my[5] + my[6] + my[7]);
   const double norm_z = .125 * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
   const double norm = sqrt(sq(norm_x) + sq(norm_y) + sq(norm_z)) + CANSFZ_EPS;
-  normx[c] = norm_x / norm;
-  normy[c] = norm_y / norm;
-  normz[c] = norm_z / norm;
+  const double inv = 1. / norm;
+  normx[c] = norm_x * inv;
+  normy[c] = norm_y * inv;
+  normz[c] = norm_z * inv;
   kappa[c] = -(0.25 * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
                0.25 * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
                0.25 * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * g.dzfi[k]);
@@ -513,9 +516,9 @@ __device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, doub
   dvdt_aux = dvdt_aux + skappayp * (c_cpc - c_ccc) * dyi;
   dwdt_aux = dwdt_aux + skappazp * (c_ccp - c_ccc) * dzci_c;
   const double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
-  dudt_aux = dudt_aux - (dpdx_e + rhoxp / ph.rho0 * (dpdx - dpdx_e));
-  dvdt_aux = dvdt_aux - (dpdy_e + rhoyp / ph.rho0 * (dpdy - dpdy_e));
-  dwdt_aux = dwdt_aux - (dpdz_e + rhozp / ph.rho0 * (dpdz - dpdz_e));
+  dudt_aux = dudt_aux - (dpdx_e + rhoxp * ph.irho0 * (dpdx - dpdx_e));
+  dvdt_aux = dvdt_aux - (dpdy_e + rhoyp * ph.irho0 * (dpdy - dpdy_e));
+  dwdt_aux = dwdt_aux - (dpdz_e + rhozp * ph.irho0 * (dpdz - dpdz_e));
   return {dudt_aux, dvdt_aux, dwdt_aux};
 }
 
@@ -640,14 +643,16 @@ __global__ void __launch_bounds__(128) k_momentum_fused(Geo g, Phys ph, const De
   const bool first = sc->first_rk;
   const double Ruo = first ? r.du : duo[t], Rvo = first ? r.dv : dvo[t], Rwo = first ? r.dw : dwo[t];
   const double f1 = sc->f1, f2 = sc->f2, f12 = sc->f12;
-  double un = LD(u, c) * rhox_n / rhox_p + (f1 * r.du + f2 * Ruo) / rhox_p;
-  double vn = LD(v, c) * rhoy_n / rhoy_p + (f1 * r.dv + f2 * Rvo) / rhoy_p;
-  double wn = LD(w, c) * rhoz_n / rhoz_p + (f1 * r.dw + f2 * Rwo) / rhoz_p;
+  // one reciprocal per face density instead of four divisions
+  const double irx = 1. / rhox_p, iry = 1. / rhoy_p, irz = 1. / rhoz_p;
+  double un = LD(u, c) * rhox_n * irx + (f1 * r.du + f2 * Ruo) * irx;
+  double vn = LD(v, c) * rhoy_n * iry + (f1 * r.dv + f2 * Rvo) * iry;
+  double wn = LD(w, c) * rhoz_n * irz + (f1 * r.dw + f2 * Rwo) * irz;
   duo[t] = r.du; dvo[t] = r.dv; dwo[t] = r.dw;
   const AdOut s = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, p, po);
-  uo[c] = un + f12 * s.du / rhox_p;
-  vo[c] = vn + f12 * s.dv / rhoy_p;
-  wo[c] = wn + f12 * s.dw / rhoz_p;
+  uo[c] = un + f12 * s.du * irx;
+  vo[c] = vn + f12 * s.dv * iry;
+  wo[c] = wn + f12 * s.dw * irz;
 }
 
 void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
@@ -783,8 +788,8 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, doub
 }
 
 // acdi_set_gamma, src/acdi.f90:32-62: max over the interior of |u_c|^2
-__global__ void k_gamma_max(Geo g, DevScalars* __restrict__ sc, const double* __restrict__ u,
-                            const double* __restrict__ v, const double* __restrict__ w) {
+__global__ void k_gamma_max(Geo g, DevScalars* __restrict__ sc, double* __restrict__ part,
+                            const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w) {
   if (HALTED(sc)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y + 1, k = blockIdx.z + 1;
@@ -797,26 +802,34 @@ __global__ void k_gamma_max(Geo g, DevScalars* __restrict__ sc, const double* __
     vel = uc * uc + vc * vc + wc * wc;
   }
   vel = block_max(vel);
-  if (threadIdx.x == 0) atomic_max_nonneg(&sc->max_bits[0], vel);
+  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = vel;
 }
-__global__ void k_gamma_final(Phys ph, DevScalars* __restrict__ sc, int apply_floor) {
+// maximum of n non-negative partials, one block
+__device__ __forceinline__ double reduce_max_partials(int n, const double* __restrict__ part) {
+  double m = 0.;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, part[q]);
+  return block_max(m);
+}
+__global__ void k_gamma_final(Phys ph, DevScalars* __restrict__ sc, int n, const double* __restrict__ part,
+                              int apply_floor) {
   if (HALTED(sc)) return;
-  const double velmax = __longlong_as_double((long long)sc->max_bits[0]);
+  const double velmax = reduce_max_partials(n, part);
+  if (threadIdx.x != 0) return;
   double gam = sqrt(velmax) * ph.gam_factor;
   if (apply_floor) gam = fmax(gam, ph.gam_min);
   sc->gam = gam;
-  sc->max_bits[0] = 0ull;
 }
-void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, const double* u, const double* v,
-                  const double* w, bool apply_floor) {
+void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, const double* u,
+                  const double* v, const double* w, bool apply_floor) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_gamma_max<<<gr, b, 0, L.st>>>(g, sc, u, v, w);
-  k_gamma_final<<<1, 1, 0, L.st>>>(ph, sc, apply_floor ? 1 : 0);
+  k_gamma_max<<<gr, b, 0, L.st>>>(g, sc, partial, u, v, w);
+  k_gamma_final<<<1, 1024, 0, L.st>>>(ph, sc, (int)(gr.x * gr.y * gr.z), partial, apply_floor ? 1 : 0);
 }
 
 // chkdt, src/chkdt.f90:15-94
-__global__ void k_chkdt_max(Geo g, DevScalars* __restrict__ sc, int only_on_check, const double* __restrict__ u,
-                            const double* __restrict__ v, const double* __restrict__ w) {
+__global__ void k_chkdt_max(Geo g, DevScalars* __restrict__ sc, int only_on_check, double* __restrict__ part,
+                            const double* __restrict__ u, const double* __restrict__ v,
+                            const double* __restrict__ w) {
   if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y + 1, k = blockIdx.z + 1;
@@ -839,13 +852,14 @@ __global__ void k_chkdt_max(Geo g, DevScalars* __restrict__ sc, int only_on_chec
     dti = fmax(dtix, fmax(dtiy, dtiz));
   }
   dti = block_max(dti);
-  if (threadIdx.x == 0) atomic_max_nonneg(&sc->max_bits[1], dti);
+  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = dti;
 }
 // completes chkdt and the dt update of src/main.f90:530-551
-__global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int in_loop) {
+__global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int in_loop, int n,
+                              const double* __restrict__ part) {
   if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
-  double dti = __longlong_as_double((long long)sc->max_bits[1]);
-  sc->max_bits[1] = 0ull;
+  double dti = reduce_max_partials(n, part);
+  if (threadIdx.x != 0) return;
   double dtipsi;
   if (ph.acdi) {
     dtipsi = sc->gam * sc->seps / (ph.dlmin * ph.dlmin);
@@ -875,11 +889,12 @@ __global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_
   sc->dti = 1. / dt;
   if (in_loop && dtmax < ph.small) sc->status = CANSFZ_ERR_DT;
 }
-void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, const double* u, const double* v,
-                  const double* w, bool only_on_check) {
+void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, const double* u,
+                  const double* v, const double* w, bool only_on_check) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_chkdt_max<<<gr, b, 0, L.st>>>(g, sc, only_on_check ? 1 : 0, u, v, w);
-  k_chkdt_final<<<1, 1, 0, L.st>>>(ph, sc, only_on_check ? 1 : 0, only_on_check ? 1 : 0);
+  const int oc = only_on_check ? 1 : 0;
+  k_chkdt_max<<<gr, b, 0, L.st>>>(g, sc, oc, partial, u, v, w);
+  k_chkdt_final<<<1, 1024, 0, L.st>>>(ph, sc, oc, oc, (int)(gr.x * gr.y * gr.z), partial);
 }
 
 // chkdiv, src/chkdiv.f90:15-49: per-block partial sums, max via atomics
@@ -898,8 +913,10 @@ __global__ void k_chkdiv_part(Geo g, DevScalars* __restrict__ sc, int only_on_ch
   const double m = block_max(fabs(div));
   const double s = block_sum(div);
   if (threadIdx.x == 0) {
-    atomic_max_nonneg(&sc->max_bits[2], m);
-    part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    part[bid] = s;
+    part[nb + bid] = m;
   }
 }
 __global__ void k_sum_partials(int n, const double* __restrict__ part, double* __restrict__ out,
@@ -910,10 +927,12 @@ __global__ void k_sum_partials(int n, const double* __restrict__ part, double* _
   s = block_sum(s);
   if (threadIdx.x == 0) *out = s;
 }
-__global__ void k_chkdiv_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check) {
+__global__ void k_chkdiv_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int n,
+                               const double* __restrict__ part) {
   if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
-  sc->divmax = __longlong_as_double((long long)sc->max_bits[2]);
-  sc->max_bits[2] = 0ull;
+  const double m = reduce_max_partials(n, part + n);
+  if (threadIdx.x != 0) return;
+  sc->divmax = m;
   // src/main.f90:552-561, after the dt checks (an earlier dt abort is kept)
   if (only_on_check && sc->status == CANSFZ_OK) {
     if (isnan(sc->divtot)) sc->status = CANSFZ_ERR_NAN;
@@ -928,7 +947,7 @@ void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partia
   k_sum_partials<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, &sc->divtot, sc, oc);
   Phys ph{};
   ph.small = CANSFZ_EPS * 1.0e7;
-  k_chkdiv_final<<<1, 1, 0, L.st>>>(ph, sc, oc);
+  k_chkdiv_final<<<1, 1024, 0, L.st>>>(ph, sc, oc, (int)(gr.x * gr.y * gr.z), partial);
 }
 
 // bulk_mean_12_stag, src/utils.f90:68-136
