@@ -264,6 +264,23 @@ int cansfz_solver_refined(cansfz_ctx* ctx, const double* rhs, double* p, int swe
 /* FP64 residual res = rhs - L(p) of that operator (p's ghosts are filled). */
 int cansfz_poisson_residual(cansfz_ctx* ctx, const double* rhs, double* p, double* res);
 
+/* ---- allocation-free Poisson solve (no reference counterpart) ---------
+ * solver_gpu for callers that may not allocate device memory while they
+ * run: the spectral work buffer and the twiddle tables are static device
+ * arrays of this library (16 MiB + 64 KiB on every GPU that loads it), so
+ * no cudaMalloc or cudaFree runs.  Limits: nx*ny*nz <= 128^3 cells, nx and
+ * ny even and <= 1024, x/y pressure BCs PP, NN or DD, z not periodic;
+ * beyond them the call returns CANSFZ_ERR_ARG or CANSFZ_ERR_UNSUPPORTED
+ * and launches nothing.  n: interior sizes; cbc: cbcpre(0:1,1:3); normfft,
+ * lambdaxy (nx*ny, packed spectral order), a, b, c (nz): initsolver's
+ * outputs as cansfz_solver uses them (device pointers); p: halo-layout
+ * device field, right-hand side in, solution out (interior).  The first
+ * call on a device (with that device current) does the set-up; make it
+ * before any stream capture.  Calls share the static arrays, so calls
+ * whose kernels overlap on the GPU race.                                 */
+int cansfz_solver_static(const int n[3], const char cbc[3][2], double normfft, const double* lambdaxy,
+                         const double* a, const double* b, const double* c, double* p, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
