@@ -35,6 +35,9 @@ DATA = "synthetic (seeded generator, numpy default_rng(2026)); no dataset"
 
 # Algorithmic bytes per cell of each stage of the FP64 step (8 B per access of
 # the persistent state a stage must read or write once; neighbours reused).
+# Algorithmic bytes per cell of each profiled stage (one read of every input
+# point, one write of every output point; halo and neighbour re-reads are
+# not counted).  FP64 drop-in:
 STAGE_BYTES = {
     # psi, phi, u, v, w, normx/y/z, history (r) + psi_new, history, fx, fy, fz (w)
     "phase_transport": 8 * (9 + 5),
@@ -49,7 +52,20 @@ STAGE_BYTES = {
     "poisson_x_bwd": 8 * 2,
     "correc": 8 * (1 + 6),
     "updatep": 8 * 3,
-    "gamma": 8 * 3,
+    "gamma_chkdt_chkdiv": 8 * 3,
+}
+# mixed form: state u, v, w, p, psi FP64; phi, normals, kappa, fluxes, histories
+# and the spectral work buffer FP32
+STAGE_BYTES_MIXED = {
+    "phase_transport": 8 * 5 + 4 * 5 + 8 + 4 * 4,
+    "cmpt_phi": 8 + 4,
+    "youngs": 4 * (1 + 4),
+    "momentum": 8 * 7 + 4 * 7 + 4 * 3 + 8 * 3,
+    "fillps": 8 * 4,
+    "poisson_f32": (8 + 4) + 4 * 2 * 3 + (4 + 8),
+    "correc": 8 * (1 + 6),
+    "updatep": 8 * 3,
+    "gamma_chkdt_chkdiv": 8 * 3,
 }
 B_ALG_STEP = 232  # bytes per cell-step: 19 state accesses + 10 Poisson-pass accesses (FP64)
 
@@ -66,6 +82,10 @@ def parse_args():
     ap.add_argument("--grid", type=int, default=256, help="cube size of the droplet workload (profiling runs)")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--sweeps", type=int, default=2, help="refinement sweeps of the mixed form")
+    ap.add_argument("--ensemble-steps", type=int, default=100,
+                    help="steps per case of the batched-ensemble measurement (0: skip)")
+    ap.add_argument("--accuracy-steps", type=int, default=50,
+                    help="mixed form: steps of the error check against the FP64 form (0: skip)")
     return ap.parse_args()
 
 
@@ -186,6 +206,108 @@ def cpu_run(p, fields, budget_s: float, warmup: int = 1, max_steps: int = 1000):
     return cells * n / dt, n, threads, dt
 
 
+def mixed_accuracy(p, fields, nsteps):
+    """Relative errors of the mixed form against the FP64 form (itself pinned to
+    the oracle) after `nsteps` steps from the same state: max|a-b|/max|b| for
+    u, v, w, psi and mean-free p; phase-mass drift and max divergence of both."""
+    import numpy as np
+
+    from cansfz import case as C
+
+    res = {}
+    runs = {}
+    for form in (0, 1):
+        q = p.copy()
+        q.form = form
+        c = C.Case(q)
+        c.set_fields(*fields)
+        c.prepare()
+        m0 = c.diag().mass12[0]
+        rc = c.step(nsteps)
+        if rc != 0:
+            raise RuntimeError(f"accuracy run (form {form}) failed with status {rc}")
+        d = c.diag()
+        runs[form] = {nm: c.get(nm) for nm in ("u", "v", "w", "p", "psi")}
+        res["fp64" if form == 0 else "mixed"] = {"mass_drift_rel": abs(d.mass12[0] - m0) / m0, "divmax": d.divmax}
+        c.close()
+    err = {}
+    for nm in ("u", "v", "w", "psi", "p"):
+        a, b = runs[1][nm][1:-1, 1:-1, 1:-1], runs[0][nm][1:-1, 1:-1, 1:-1]
+        if nm == "p":
+            a, b = a - a.mean(), b - b.mean()
+        err[nm] = float(np.abs(a - b).max() / np.abs(b).max())
+    res["steps"] = nsteps
+    res["rel_err_max"] = err
+    return res
+
+
+def ensemble_bench(nsteps, warmup, form):
+    """The batched-ensemble configuration: 64 independent rising-bubble cases,
+    `nsteps` steps each, run (a) one case at a time (each case's own graph,
+    cansfz_step) and (b) batched (cansfz_ensemble_step: one graph launch per
+    step for all cases), from the same initial states.  cases/s = completed
+    case-runs per second, wall clock around synchronised work."""
+    import torch
+
+    from cansfz import case as C
+    from cansfz import workloads as W
+
+    specs = W.ensemble_cases(seed=4)
+
+    def build():
+        cs = []
+        for p, f in specs:
+            q = p.copy()
+            q.form = form
+            c = C.Case(q, own_stream=True)
+            c.set_fields(*f)
+            c.prepare()
+            cs.append(c)
+        return cs
+
+    seq = build()
+    for c in seq:  # warm-up: graph capture and first steps
+        if c.step(warmup) != 0:
+            raise RuntimeError("ensemble warm-up failed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for c in seq:
+        rc = c.step(nsteps)
+        if rc != 0:
+            raise RuntimeError(f"sequential ensemble case failed with status {rc}")
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    seq_state = [c.get("psi") for c in seq[:4]]
+    for c in seq:
+        c.close()
+    bat = build()
+    ens = C.Ensemble(bat)
+    rc, _ = ens.step(warmup)
+    if rc != 0:
+        raise RuntimeError("batched ensemble warm-up failed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc, sts = ens.step(nsteps)
+    torch.cuda.synchronize()
+    t_bat = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"batched ensemble failed with statuses {sts}")
+    # the batched run computes exactly what the one-at-a-time run computes
+    same = all(float(abs(a - c.get("psi")).max()) == 0.0 for a, c in zip(seq_state, bat[:4]))
+    ens.close()
+    cells = sum(int(p.n[0] * p.n[1] * p.n[2]) for p, _ in specs)
+    for c in bat:
+        c.close()
+    n = len(specs)
+    return {"cases": n, "steps_per_case": nsteps, "warmup": warmup, "form": "fp64" if form == 0 else "mixed",
+            "cells_total": cells,
+            "cases_per_s_batched": n / t_bat, "cases_per_s_sequential": n / t_seq,
+            "speedup": t_seq / t_bat, "cell_steps_per_s_batched": cells * nsteps / t_bat,
+            "batched_equals_sequential": bool(same),
+            "what": "64 rising-bubble cases (seed 4; 32 2-D 64x128..256x512, 32 3-D 32^3..96x96x192); "
+                    "wall clock around synchronised work"}
+
+
 def gpu_arm(args):
     import numpy as np
     import torch
@@ -244,25 +366,29 @@ def gpu_arm(args):
     stage_names = names.value.decode().split(",")
     stage_ms = {nm: buf[q] / nprof for q, nm in enumerate(stage_names)}
     tot = sum(stage_ms.values())
-    heavy = [s for s in stage_ms if s in STAGE_BYTES]
+    table = STAGE_BYTES if args.form == "fp64" else STAGE_BYTES_MIXED
+    heavy = [s for s in stage_ms if s in table]
     dom = max(heavy, key=lambda s: stage_ms[s])
     peak, peak_kind = measured_peaks()
-    bytes_launch = STAGE_BYTES[dom] * cells
+    bytes_launch = table[dom] * cells
     achieved = bytes_launch / (stage_ms[dom] * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        if dom in tj:
-            traffic = tj[dom]["bytes_per_cell"] * cells
+        key = dom if args.form == "fp64" else dom + ":mixed"
+        if key in tj:
+            traffic = tj[key]["bytes_per_cell"] * cells
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64 state / f32 transforms", "data": DATA,
+        "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64 state / f32 stencils+transforms",
+        "data": DATA,
         "config": {"workload": WORKLOAD if args.grid == 256 else f"droplets_acdi at {args.grid}^3 (profiling size)",
                    "grid": [nx, ny, nz],
-                   "form": "fp64 (drop-in)" if args.form == "fp64" else f"mixed (FP32 transforms + {args.sweeps} sweeps)",
+                   "form": "fp64 (drop-in)" if args.form == "fp64" else
+                           f"mixed (FP32 stencils and transforms, FP64 state, {args.sweeps} refinement sweeps)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (each FP64 field 137 MB > 126 MB)",
                    "final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
@@ -275,6 +401,12 @@ def gpu_arm(args):
         "gpu_launches": int(kps.value) * args.steps,
         "clocks": clocks,
     }
+    # ---- batched ensemble of independent small cases
+    if world == 1 and args.ensemble_steps > 0:
+        out["ensemble"] = ensemble_bench(args.ensemble_steps, 3, 0 if args.form == "fp64" else 1)
+    # ---- mixed form: error against the FP64 form after the same steps from the same state
+    if args.form == "mixed" and args.accuracy_steps > 0:
+        out["accuracy_vs_fp64"] = mixed_accuracy(p, fields, args.accuracy_steps)
     # ---- end to end through the C ABI with pinned host buffers
     if not args.no_e2e:
         hshape = tuple(x + 2 for x in p.n)

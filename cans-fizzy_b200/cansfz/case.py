@@ -44,7 +44,11 @@ class DeviceField:
 
 
 class Case:
-    def __init__(self, params: Params, device: str = "cuda"):
+    """own_stream: the context creates its own CUDA stream instead of using
+    torch's current one (cases of an Ensemble need one each; fields then go
+    through host arrays, which every entry synchronises)."""
+
+    def __init__(self, params: Params, device: str = "cuda", own_stream: bool = False):
         if not torch.cuda.is_available():
             raise RuntimeError("cansfz needs a CUDA device (B200, sm_100a); there is no CPU fallback")
         self.lib = _L.load()
@@ -52,10 +56,10 @@ class Case:
         self.n = params.n
         self.hshape = tuple(x + 2 for x in self.n)
         self.device = device
-        self.stream = torch.cuda.current_stream()
+        self.stream = None if own_stream else torch.cuda.current_stream()
         h = ct.c_void_p()
-        _L.check(self.lib.cansfz_create(ct.byref(self.params), ct.c_void_p(self.stream.cuda_stream), ct.byref(h)),
-                 "cansfz_create")
+        st = ct.c_void_p(None if own_stream else self.stream.cuda_stream)
+        _L.check(self.lib.cansfz_create(ct.byref(self.params), st, ct.byref(h)), "cansfz_create")
         self.h = h
 
     def close(self):
@@ -142,3 +146,32 @@ class Case:
         _L.check(rc, "cansfz_" + name)
         torch.cuda.synchronize()
         return rc
+
+
+class Ensemble:
+    """Independent cases advanced together: one CUDA graph launch per step
+    holds every case's step as a parallel branch (cansfz_ensemble_*)."""
+
+    def __init__(self, cases):
+        self.lib = _L.load()
+        self.cases = list(cases)
+        arr = (ct.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
+        h = ct.c_void_p()
+        _L.check(self.lib.cansfz_ensemble_create(arr, len(self.cases), None, ct.byref(h)), "cansfz_ensemble_create")
+        self.h = h
+
+    def step(self, nsteps: int = 1):
+        st = (ct.c_int * len(self.cases))()
+        rc = self.lib.cansfz_ensemble_step(self.h, int(nsteps), st)
+        return rc, list(st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cansfz_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -12,6 +12,11 @@ numpy.random.default_rng(seed).
                     droplets = dense phase), rho 1000/1, mu 100/1, sigma 1,
                     g = 1, random divergence-free u0 (|k| <= 4, rms 0.1), ACDI.
   droplets_thinc    512x512x256, box 2x2x1, same physics, THINC/QQ.
+  ensemble_cases    64 rising-bubble cases (seed 4): 32 2-D (ny = 2, periodic
+                    y) with (nx, nz) from 64x128 to 256x512 and 32 3-D from
+                    32^3 to 96x96x192, sizes 2^a 3^b multiples of 16; rho
+                    ratio in {10,100,1000}, mu ratio in {10,100}, sigma in
+                    [1,30], bubble diameter in [0.25,0.5] of the box width.
   shear_stretched   512x256x256, gtype 1, gr 1.5, Poiseuille mean 1 with the
                     laminar pressure gradient, 1% seeded perturbation, 200
                     droplets R ~ U[0.04,0.08], rho ratio 10, mu ratio 1,
@@ -110,3 +115,34 @@ BUILDERS = {
     "droplets_thinc": droplets_thinc,
     "shear_stretched": shear_stretched,
 }
+
+
+def _bubble_case(nx, ny, nz, lx, ly, lz, rho_ratio, mu_ratio, sigma, diam, two_d):
+    p = _walls_z(nx, ny, nz, (lx, ly, lz), (1000.0, 1000.0 / rho_ratio), (10.0, 10.0 / mu_ratio), sigma,
+                 (0.0, 0.0, -0.98))
+    if two_d:
+        psi = init.init2fl(p, "bub2", np.array([[0.5 * lx, 0.0, 0.5 * lz, 0.5 * diam]]))
+    else:
+        psi = init.init2fl(p, "bub3", np.array([[0.5 * lx, 0.5 * ly, 0.5 * lz, 0.5 * diam]]))
+    u, v, w, pr = init.initflow(p, "zer")
+    return p, (u, v, w, pr, psi)
+
+
+def ensemble_cases(seed=4, count2d=32, count3d=32):
+    """The batched-ensemble configuration: a list of (params, fields)."""
+    rng = np.random.default_rng(seed)
+    sizes2d = [64, 96, 128, 192, 256]      # nx; nz = 2 nx (box 1 x 2)
+    sizes3d = [32, 48, 64, 96]             # nx = ny; nz = 2 nx (box 1 x 1 x 2)
+    out = []
+    for q in range(count2d + count3d):
+        two_d = q < count2d
+        n = int(rng.choice(sizes2d if two_d else sizes3d))
+        rho_ratio = float(rng.choice([10.0, 100.0, 1000.0]))
+        mu_ratio = float(rng.choice([10.0, 100.0]))
+        sigma = float(rng.uniform(1.0, 30.0))
+        diam = float(rng.uniform(0.25, 0.5))
+        if two_d:
+            out.append(_bubble_case(n, 2, 2 * n, 1.0, 2.0 / n, 2.0, rho_ratio, mu_ratio, sigma, diam, True))
+        else:
+            out.append(_bubble_case(n, n, 2 * n, 1.0, 1.0, 2.0, rho_ratio, mu_ratio, sigma, diam, False))
+    return out

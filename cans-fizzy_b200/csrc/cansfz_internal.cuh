@@ -85,7 +85,8 @@ struct BcFace {
   double sgn;
 };
 struct BcField {
-  double* p;
+  void* p;               // double*, or float* when f32 (intermediates of the mixed form)
+  int f32;
   BcFace face[3][2];     // [idir][ibound]
   int halo_periodic[3];  // y/z periodic self-exchange (updthalo)
 };
@@ -197,12 +198,22 @@ void launch_updatep_interior(const Launch& L, const Geo& g, const DevScalars* sc
 void launch_updatep_full(const Launch& L, const Geo& g, const double* pp, double* p);
 void launch_copy(const Launch& L, size_t n, const double* src, double* dst);
 void launch_fill(const Launch& L, size_t n, double val, double* dst);
+void launch_fill(const Launch& L, size_t n, float val, float* dst);
+void launch_widen(const Launch& L, size_t n, const float* src, double* dst);
+void launch_cmpt_phi_f32(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
+                         float* phi, bool narrow_only);
+template <typename TI>
+void launch_thinc_step_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
+                         const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
+                         const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz);
 
 // reductions: results land in DevScalars
 void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                   const double* u, const double* v, const double* w, bool apply_floor);
 void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                   const double* u, const double* v, const double* w, bool only_on_check);
+void launch_step_reductions(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
+                            const double* u, const double* v, const double* w);
 void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial,
                    const double* u, const double* v, const double* w, bool only_on_check);
 void launch_bulk_mean(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
@@ -222,6 +233,21 @@ void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
 
 // k_poisson.cu
 void poisson_set_attributes();
+
+// z-marching tile kernels (k_tiles.cu), TI = double (drop-in) or float (mixed form)
+template <typename TI>
+void launch_youngs_t(const Launch& L, const Geo& g, const DevScalars* sc, const TI* phi, TI* nx, TI* ny, TI* nz,
+                     TI* kappa);
+template <typename TI>
+void launch_acdi_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, bool upd, const double* u,
+                   const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
+                   const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz);
+template <typename TI>
+void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
+                       const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
+                       const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
+                       TI* dvo, TI* dwo, double* uo, double* vo, double* wo);
+void tiles_set_attributes();
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                     double* p, const StageMark* mk = nullptr);
 // mixed form: FP32 spectral solve (dst = S(src) or dst += S(src)) and the

@@ -100,6 +100,10 @@ struct cansfz_ctx {
   double* res64 = nullptr;
   bool mixed = false;
   int sweeps = 2;
+  // mixed form: FP32 intermediates of the phase-field and momentum stages
+  float *phif = nullptr, *kappaf = nullptr, *nxf = nullptr, *nyf = nullptr, *nzf = nullptr;
+  float *fxf = nullptr, *fyf = nullptr, *fzf = nullptr;                     // halo layout
+  float *hpsif = nullptr, *huf = nullptr, *hvf = nullptr, *hwf = nullptr;   // AB2 histories (interior)
   // reductions, scalars
   double* partial = nullptr;
   DevScalars* sc = nullptr;       // the step scalars (device)
@@ -157,14 +161,24 @@ BcField bc_scalar(const cansfz_ctx* c, const char cbc[3][2], const double bc[3][
   return F;
 }
 
-// bounduvw, src/bound.f90:15-79: the three velocity components
-void bc_vel(const cansfz_ctx* c, bool is_correc, double* u, double* v, double* w, BcField out[3]) {
+BcField bc_scalar(const cansfz_ctx* c, const char cbc[3][2], const double bc[3][2], float* p) {
+  BcField F = bc_scalar(c, cbc, bc, (double*)nullptr);
+  F.p = p;
+  F.f32 = 1;
+  return F;
+}
+
+// bounduvw, src/bound.f90:15-79: the three velocity components (or the three
+// phase fluxes, which take the velocity's boundary rules)
+template <typename E>
+void bc_vel(const cansfz_ctx* c, bool is_correc, E* u, E* v, E* w, BcField out[3]) {
   const cansfz_params& P = c->P;
-  double* fld[3] = {u, v, w};
+  E* fld[3] = {u, v, w};
   for (int ivel = 0; ivel < 3; ++ivel) {
     BcField& F = out[ivel];
     F = BcField{};
     F.p = fld[ivel];
+    F.f32 = sizeof(E) == sizeof(float);
     for (int d = 0; d < 3; ++d) F.halo_periodic[d] = c->halo_periodic[d];
     for (int d = 0; d < 3; ++d) {
       const bool normal = (ivel == d);
@@ -458,6 +472,19 @@ __global__ void k_prescribed_vel(Geo g, const DevScalars* __restrict__ sc, int w
   p[c] = 0.;
 }
 
+// phi, Youngs normals and curvature and their ghost fills in FP32 (mixed form)
+void normals_f32(cansfz_ctx* c, const double* psi, const DevScalars* sc, const StageMark* mk = nullptr) {
+  const cansfz_params& P = c->P;
+  launch_cmpt_phi_f32(c->L, c->g, sc, c->ph.acdi != 0, psi, c->phif, c->ph.sdf == 0);
+  if (mk) mk->mark("cmpt_phi");
+  launch_youngs_t<float>(c->L, c->g, sc, c->phif, c->nxf, c->nyf, c->nzf, c->kappaf);
+  if (mk) mk->mark("youngs");
+  run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappaf), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nxf),
+             bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->nyf), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nzf)},
+         sc);
+  if (mk) mk->mark("bc_normals");
+}
+
 // ---------------------------------------------------------------------------
 // one time step (src/main.f90:422-529) on the current parity `c->cur`
 // ---------------------------------------------------------------------------
@@ -471,7 +498,21 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
   launch_step_begin(L, sc, P.icheck);
   MARK("step_begin");
   // phase field: rk_2fl + boundary fills + phi + normals/curvature
-  if (P.is_track_interface) {
+  if (P.is_track_interface && c->mixed) {
+    const bool sdf = c->ph.sdf != 0;
+    if (c->ph.acdi)
+      launch_acdi_t<float>(L, g, sc, sdf, true, c->u[a], c->v[a], c->w[a], c->nxf, c->nyf, c->nzf, c->phif,
+                           c->psi[a], c->psi[b], c->hpsif, c->fxf, c->fyf, c->fzf);
+    else
+      launch_thinc_step_t<float>(L, g, sc, sdf, c->u[a], c->v[a], c->w[a], c->nxf, c->nyf, c->nzf, c->phif,
+                                 c->psi[a], c->psi[b], c->hpsif, c->fxf, c->fyf, c->fzf);
+    MARK("phase_transport");
+    BcField F[3];
+    bc_vel(c, false, c->fxf, c->fyf, c->fzf, F);
+    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc);
+    MARK("bc_phase");
+    normals_f32(c, c->psi[b], sc, mk);
+  } else if (P.is_track_interface) {
     if (c->ph.acdi)
       launch_acdi_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
                        c->psi[a], c->psi[b], c->hpsi, c->fx, c->fy, c->fz);
@@ -493,9 +534,13 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     MARK("bc_normals");
   } else {
     launch_copy(L, (size_t)g.hsize(), c->psi[a], c->psi[b]);
-    launch_fill(L, (size_t)g.hsize(), 0., c->fx);
-    launch_fill(L, (size_t)g.hsize(), 0., c->fy);
-    launch_fill(L, (size_t)g.hsize(), 0., c->fz);
+    if (c->mixed) {
+      for (float* f : {c->fxf, c->fyf, c->fzf}) launch_fill(L, (size_t)g.hsize(), 0.f, f);
+    } else {
+      launch_fill(L, (size_t)g.hsize(), 0., c->fx);
+      launch_fill(L, (size_t)g.hsize(), 0., c->fy);
+      launch_fill(L, (size_t)g.hsize(), 0., c->fz);
+    }
   }
   if (!P.is_solve_ns) {
     const std::string iv(c->inivel);
@@ -511,8 +556,13 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
       if (std::fabs(P.gacc[d]) > 0. && is_pp(P.cbcpre[d]))
         launch_bulk_mean(L, g, c->ph, sc, c->partial, d + 1, c->d_grid + (d == 2 ? 5 : 4) * (g.nz + 2), c->psi[b]);
     // rk: the whole momentum update in one pass
-    launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy, c->fz,
-                          c->p[a], c->p[b], c->kappa, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
+    if (c->mixed)
+      launch_momentum_t<float>(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fxf, c->fyf,
+                               c->fzf, c->p[a], c->p[b], c->kappaf, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
+                               c->w[b]);
+    else
+      launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy,
+                            c->fz, c->p[a], c->p[b], c->kappa, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
     MARK("momentum");
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw");
@@ -548,11 +598,9 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     MARK("bc_p");
   }
   launch_step_end(L, c->ph, sc);
-  if (c->ph.acdi) launch_gamma(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
-  MARK("gamma");
-  launch_chkdt(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
-  launch_chkdiv(L, g, sc, c->partial, c->u[b], c->v[b], c->w[b], true);
-  MARK("chkdt_chkdiv");
+  // acdi_set_gamma, and on icheck steps chkdt + chkdiv, in one pass
+  launch_step_reductions(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b]);
+  MARK("gamma_chkdt_chkdiv");
 #undef MARK
 }
 
@@ -605,6 +653,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   cudaDeviceGetAttribute(&c->L.nsm, cudaDevAttrMultiProcessorCount, dev);
   c->L.st = c->st;
   poisson_set_attributes();
+  tiles_set_attributes();
   for (int d = 0; d < 3; ++d) c->n[d] = P.ng[d];
   const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
   for (int d = 0; d < 3; ++d) {
@@ -686,11 +735,17 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   if (c->mixed) {
     if ((rc = dalloc(c, &c->rhs64, H))) return fail(rc);
     if ((rc = dalloc(c, &c->res64, H))) return fail(rc);
+    for (float** f : {&c->phif, &c->kappaf, &c->nxf, &c->nyf, &c->nzf, &c->fxf, &c->fyf, &c->fzf})
+      if ((rc = dalloc(c, f, H))) return fail(rc);
+    for (float** f : {&c->hpsif, &c->huf, &c->hvf, &c->hwf})
+      if ((rc = dalloc(c, f, I))) return fail(rc);
   }
   // reductions: partial sums of one launch over the interior blocks
   const int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
   const size_t nblk = (size_t)((nx + bx - 1) / bx) * ny * nz;
-  if ((rc = dalloc(c, &c->partial, 2 * nblk + 64))) return fail(rc);
+  // ... and four per block of the fused end-of-step reduction (8 blocks per SM at most)
+  const size_t nred = 4 * (size_t)(c->L.nsm > 0 ? c->L.nsm : 148) * 8;
+  if ((rc = dalloc(c, &c->partial, std::max(2 * nblk, nred) + 64))) return fail(rc);
   if ((rc = dalloc(c, &c->sc, 1))) return fail(rc);
   if ((rc = dalloc(c, &c->sc_call, 1))) return fail(rc);
   if (cudaMallocHost(&c->sc_host, sizeof(DevScalars)) != cudaSuccess) return fail(CANSFZ_ERR_NOMEM);
@@ -771,6 +826,26 @@ int cansfz_get_aux(cansfz_ctx* c, const char* name, double* out, int on_device) 
   else if (s == "dvdtrko") { src = c->hv; n = c->g.tsize(); }
   else if (s == "dwdtrko") { src = c->hw; n = c->g.tsize(); }
   else return CANSFZ_ERR_ARG;
+  if (c->mixed) {  // FP32 intermediates, widened into scratch for the caller
+    const float* f = nullptr;
+    double* tmp = c->res64;
+    if (s == "phi") f = c->phif;
+    else if (s == "kappa") f = c->kappaf;
+    else if (s == "normx") f = c->nxf;
+    else if (s == "normy") f = c->nyf;
+    else if (s == "normz") f = c->nzf;
+    else if (s == "psiflx_x") f = c->fxf;
+    else if (s == "psiflx_y") f = c->fyf;
+    else if (s == "psiflx_z") f = c->fzf;
+    else if (s == "dpsidtrko") f = c->hpsif;
+    else if (s == "dudtrko") f = c->huf;
+    else if (s == "dvdtrko") f = c->hvf;
+    else if (s == "dwdtrko") f = c->hwf;
+    if (f) {
+      launch_widen(c->L, n, f, tmp);
+      src = tmp;
+    }
+  }
   CK(cudaMemcpyAsync(out, src, n * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -788,11 +863,15 @@ int cansfz_prepare(cansfz_ctx* c) {
   run_bcp(c, 0, c->p[a], sc);
   launch_copy(L, (size_t)c->g.hsize(), c->p[a], c->p[a ^ 1]);  // po = pn = p
   run_bcp(c, 1, c->psi[a], sc);
-  if (c->ph.sdf) launch_cmpt_phi(L, c->g, sc, c->ph.acdi != 0, c->psi[a], c->phi);
-  launch_youngs(L, c->g, sc, c->ph.sdf ? c->phi : c->psi[a], c->nx, c->ny, c->nz, c->kappa);
-  run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
-             bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
-         sc);
+  if (c->mixed) {
+    normals_f32(c, c->psi[a], sc);
+  } else {
+    if (c->ph.sdf) launch_cmpt_phi(L, c->g, sc, c->ph.acdi != 0, c->psi[a], c->phi);
+    launch_youngs(L, c->g, sc, c->ph.sdf ? c->phi : c->psi[a], c->nx, c->ny, c->nz, c->kappa);
+    run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
+               bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
+           sc);
+  }
   if (c->ph.acdi) launch_gamma(L, c->g, c->ph, sc, c->partial, c->u[a], c->v[a], c->w[a], true);
   launch_chkdt(L, c->g, c->ph, sc, c->partial, c->u[a], c->v[a], c->w[a], false);
   // dto = dt (src/main.f90:409)
@@ -802,6 +881,114 @@ int cansfz_prepare(cansfz_ctx* c) {
   CK(cudaStreamSynchronize(c->st));
   c->prepared = true;
   return CANSFZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: independent cases (any sizes, any parameters) advance
+// together.  One CUDA graph per step parity holds every case's whole step as
+// a parallel branch (fork/join capture over the cases' own streams), so one
+// graph launch advances all cases by a step and the GPU overlaps the small
+// cases' kernels instead of running them one case at a time.
+// ---------------------------------------------------------------------------
+struct cansfz_ensemble {
+  std::vector<cansfz_ctx*> cases;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int cur = 0;
+};
+
+int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, cansfz_ensemble** out) {
+  if (!cases || ncases <= 0 || !out) return CANSFZ_ERR_ARG;
+  *out = nullptr;
+  for (int q = 0; q < ncases; ++q) {
+    if (!cases[q]) return CANSFZ_ERR_ARG;
+    if (!cases[q]->prepared) {
+      if (int rc = cansfz_prepare(cases[q])) return rc;
+    }
+    if (cases[q]->cur != cases[0]->cur) return CANSFZ_ERR_ARG;  // all cases at the same buffer parity
+  }
+  auto* e = new cansfz_ensemble();
+  e->cases.assign(cases, cases + ncases);
+  e->cur = cases[0]->cur;
+  bool ok = true;
+  if (stream) e->st = (cudaStream_t)stream;
+  else ok = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+  e->join.resize(ncases, nullptr);
+  for (int q = 0; ok && q < ncases; ++q)
+    ok = cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cansfz_ensemble_destroy(e);
+    return CANSFZ_ERR_CUDA;
+  }
+  *out = e;
+  return CANSFZ_OK;
+}
+
+int cansfz_ensemble_destroy(cansfz_ensemble* e) {
+  if (!e) return CANSFZ_ERR_ARG;
+  for (int q = 0; q < 2; ++q)
+    if (e->gexec[q]) cudaGraphExecDestroy(e->gexec[q]);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  // the stream is the caller's when one was given; a created one is released
+  bool own = true;
+  for (cansfz_ctx* c : e->cases)
+    if (c && c->st == e->st) own = false;
+  if (own && e->st) cudaStreamDestroy(e->st);
+  delete e;
+  return CANSFZ_OK;
+}
+
+// status_out (optional, ncases entries): each case's status after the steps
+int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
+  if (!e || nsteps < 0) return CANSFZ_ERR_ARG;
+  const int n = (int)e->cases.size();
+  std::vector<long long> istep0(n);
+  for (int q = 0; q < n; ++q) {
+    cansfz_ctx* c = e->cases[q];
+    if (c->last_status != CANSFZ_OK) return c->last_status;  // an aborted case stops the ensemble
+    if (c->cur != e->cur) return CANSFZ_ERR_ARG;  // a case was stepped on its own in between
+    if (int rc = sync_status(c)) return rc;
+    istep0[q] = c->sc_host->istep;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int par = e->cur;
+    if (!e->gexec[par]) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+      CK(cudaEventRecord(e->fork, e->st));
+      for (int q = 0; q < n; ++q) {
+        cansfz_ctx* c = e->cases[q];
+        CK(cudaStreamWaitEvent(c->st, e->fork, 0));
+        enqueue_step(c);
+        CK(cudaEventRecord(e->join[q], c->st));
+        CK(cudaStreamWaitEvent(e->st, e->join[q], 0));
+      }
+      CK(cudaStreamEndCapture(e->st, &graph));
+      CK(cudaGraphInstantiate(&e->gexec[par], graph, 0));
+      cudaGraphDestroy(graph);
+    }
+    CK(cudaGraphLaunch(e->gexec[par], e->st));
+    e->cur ^= 1;
+    for (cansfz_ctx* c : e->cases) c->cur ^= 1;
+  }
+  CK(cudaStreamSynchronize(e->st));
+  int worst = CANSFZ_OK;
+  for (int q = 0; q < n; ++q) {
+    cansfz_ctx* c = e->cases[q];
+    if (int rc = sync_status(c)) return rc;
+    // a case that aborted skipped its later steps: its parity follows the executed count
+    const long long done = c->sc_host->istep - istep0[q];
+    if ((long long)nsteps != done) c->cur ^= (int)((nsteps - done) & 1);
+    c->last_status = c->sc_host->status;
+    if (status_out) status_out[q] = c->last_status;
+    if (c->last_status != CANSFZ_OK && worst == CANSFZ_OK) worst = c->last_status;
+  }
+  return worst;
 }
 
 int cansfz_step(cansfz_ctx* c, int nsteps) {

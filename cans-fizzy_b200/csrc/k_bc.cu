@@ -15,8 +15,8 @@ enum { ST_PER = 0, ST_X = 1, ST_Y = 2, ST_Z = 3 };
 
 // set_bc for one line along idir through the plane point: q(m) addresses the
 // element at index m (0..n+1) of that line.
-template <typename Q>
-__device__ __forceinline__ void set_bc_line(const BcFace& f, int ib, int n, double* __restrict__ p, Q q) {
+template <typename E, typename Q>
+__device__ __forceinline__ void set_bc_line(const BcFace& f, int ib, int n, E* __restrict__ p, Q q) {
   if (f.type == BC_NONE) return;
   if (f.type == BC_P) {
     // p(0) = p(n); p(n+1) = p(1)
@@ -24,26 +24,21 @@ __device__ __forceinline__ void set_bc_line(const BcFace& f, int ib, int n, doub
     p[q(n + 1)] = p[q(1)];
     return;
   }
+  const E factor = (E)f.factor, sgn = (E)f.sgn;
   if (f.centered) {
-    if (ib == 0) p[q(0)] = f.factor + f.sgn * p[q(1)];
-    else p[q(n + 1)] = f.factor + f.sgn * p[q(n)];
+    if (ib == 0) p[q(0)] = factor + sgn * p[q(1)];
+    else p[q(n + 1)] = factor + sgn * p[q(n)];
   } else if (f.type == BC_D) {
-    if (ib == 0) p[q(0)] = f.factor;
-    else { p[q(n + 1)] = p[q(n - 1)]; p[q(n)] = f.factor; }
+    if (ib == 0) p[q(0)] = factor;
+    else { p[q(n + 1)] = p[q(n - 1)]; p[q(n)] = factor; }
   } else {  // non-centered N
-    if (ib == 0) p[q(0)] = 1. * f.factor + p[q(1)];
-    else { p[q(n + 1)] = p[q(n)]; p[q(n)] = 1. * f.factor + p[q(n - 1)]; }
+    if (ib == 0) p[q(0)] = E(1.) * factor + p[q(1)];
+    else { p[q(n + 1)] = p[q(n)]; p[q(n)] = E(1.) * factor + p[q(n - 1)]; }
   }
 }
 
-template <int STAGE>
-__global__ void k_bc_stage(Geo g, BcGroup grp, const DevScalars* __restrict__ sc) {
-  if (sc != nullptr && sc->halted) return;
-  const int fi = blockIdx.y;
-  if (fi >= grp.nf) return;
-  const BcField& F = grp.f[fi];
-  double* __restrict__ p = F.p;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+template <int STAGE, typename E>
+__device__ __forceinline__ void bc_stage_point(const Geo& g, const BcField& F, E* __restrict__ p, int q) {
   const int NX = g.nx + 2, NY = g.ny + 2, NZ = g.nz + 2;
   if (STAGE == ST_PER) {
     const bool py = F.halo_periodic[1], pz = F.halo_periodic[2];
@@ -83,6 +78,17 @@ __global__ void k_bc_stage(Geo g, BcGroup grp, const DevScalars* __restrict__ sc
     set_bc_line(F.face[2][0], 0, g.nz, p, at);
     set_bc_line(F.face[2][1], 1, g.nz, p, at);
   }
+}
+
+template <int STAGE>
+__global__ void k_bc_stage(Geo g, BcGroup grp, const DevScalars* __restrict__ sc) {
+  if (sc != nullptr && sc->halted) return;
+  const int fi = blockIdx.y;
+  if (fi >= grp.nf) return;
+  const BcField& F = grp.f[fi];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (F.f32) bc_stage_point<STAGE, float>(g, F, static_cast<float*>(F.p), q);
+  else bc_stage_point<STAGE, double>(g, F, static_cast<double*>(F.p), q);
 }
 
 void launch_bc_group(const Launch& L, const Geo& g, const BcGroup& grp, const DevScalars* sc) {

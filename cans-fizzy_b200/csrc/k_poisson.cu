@@ -82,12 +82,27 @@ template <typename T> __device__ __forceinline__ void str(const Bufs<T>& B, int 
 
 // complex FFT (sign -1 forward, +1 backward) of length pl.m on L lines held
 // in buffer `in`; returns the buffer index holding the result.
+// MC > 0: the complex length is the compile-time power of two MC (radix-4
+// stages, then one radix-2 stage when log2(MC) is odd -- the plan the host
+// derives for such lengths) and LC the compile-time lines per CTA, so every
+// index division below folds into shifts and masks.
+template <int MC>
+struct Pow2Plan {
+  static constexpr int lg = MC <= 1 ? 0 : 1 + Pow2Plan<(MC >> 1)>::lg;
+  static constexpr int n4 = lg / 2;
+  static constexpr int nst = n4 + (lg & 1);
+  static __device__ __forceinline__ constexpr int radix(int st) { return st < n4 ? 4 : 2; }
+};
+template <>
+struct Pow2Plan<0> {
+  static constexpr int lg = 0, n4 = 0, nst = 0;
+  static __device__ __forceinline__ constexpr int radix(int) { return 1; }
+};
+
+// one Stockham stage of radix r on L lines: buffer cur -> cur^1
 template <typename T>
-__device__ int fft_lines(const LinePlan& pl, const Bufs<T>& B, int in, int L, int sign) {
-  const int m = pl.m;
-  int len = m, s = 1, cur = in;
-  for (int st = 0; st < pl.nst; ++st) {
-    const int r = pl.radix[st];
+__device__ __forceinline__ void fft_stage(const LinePlan& pl, const Bufs<T>& B, int cur, int L, int sign, int m,
+                                          int r, int len, int s) {
     const int mm = len / r;
     const int tstep = m / len;  // exp(-2 pi i p u / len) = tw[p*u*tstep]
     const int nb = m / r;       // butterflies per line (= mm * s)
@@ -140,18 +155,41 @@ __device__ int fft_lines(const LinePlan& pl, const Bufs<T>& B, int in, int L, in
         }
       }
     }
-    __syncthreads();
-    cur = nxt;
-    len = mm;
-    s *= r;
+}
+
+template <typename T, int MC, int LC>
+__device__ int fft_lines(const LinePlan& pl, const Bufs<T>& B, int in, int Lrt, int sign) {
+  const int L = LC ? LC : Lrt;
+  int cur = in;
+  if constexpr (MC > 0) {
+    int len = MC, s = 1;
+#pragma unroll
+    for (int st = 0; st < Pow2Plan<MC>::nst; ++st) {
+      const int r = Pow2Plan<MC>::radix(st);
+      fft_stage<T>(pl, B, cur, L, sign, MC, r, len, s);
+      __syncthreads();
+      cur ^= 1;
+      len /= r;
+      s *= r;
+    }
+  } else {
+    const int m = pl.m;
+    int len = m, s = 1;
+    for (int st = 0; st < pl.nst; ++st) {
+      const int r = pl.radix[st];
+      fft_stage<T>(pl, B, cur, L, sign, m, r, len, s);
+      __syncthreads();
+      cur ^= 1;
+      len /= r;
+      s *= r;
+    }
   }
   return cur;
 }
 
 // post-processing of a forward real transform: X_k, k = 0..m, from Z
 template <typename T>
-__device__ __forceinline__ cx<T> real_fwd_X(const LinePlan& pl, const Bufs<T>& B, int zb, int k, int line) {
-  const int m = pl.m;
+__device__ __forceinline__ cx<T> real_fwd_X(const LinePlan& pl, const Bufs<T>& B, int zb, int k, int line, int m) {
   const cx<T> zk = ld2<T>(B, zb, k % m, line);
   const cx<T> zc = cconj<T>(ld2<T>(B, zb, (m - k) % m, line));
   const cx<T> w = TW2<T>(pl, k);
@@ -184,16 +222,17 @@ __device__ __forceinline__ cx<T> packed_X(const Bufs<T>& B, int b, int k, int m,
 // ---------------------------------------------------------------------------
 // forward: input real line in buffer 0 as pairs (x_2j, x_2j+1) (after the
 // kind's input reordering); output real line written through `out(line, s, v)`
-template <typename T, bool LF, typename OUT>
-__device__ void line_forward(const LinePlan& pl, const Bufs<T>& B, int L, OUT out) {
-  const int m = pl.m, n = pl.n;
-  const int zb = fft_lines<T>(pl, B, 0, L, -1);
+template <typename T, bool LF, int MC, int LC, typename OUT>
+__device__ void line_forward(const LinePlan& pl, const Bufs<T>& B, int Lrt, OUT out) {
+  const int m = MC ? MC : pl.m, n = MC ? 2 * MC : pl.n;
+  const int L = LC ? LC : Lrt;
+  const int zb = fft_lines<T, MC, LC>(pl, B, 0, L, -1);
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * m; it += blockDim.x) {
       const int line = LF ? it % L : it / m, k = LF ? it / L : it - line * m;
-      const cx<T> X = real_fwd_X<T>(pl, B, zb, k, line);
+      const cx<T> X = real_fwd_X<T>(pl, B, zb, k, line, m);
       if (k == 0) {
-        const cx<T> Xm = real_fwd_X<T>(pl, B, zb, m, line);
+        const cx<T> Xm = real_fwd_X<T>(pl, B, zb, m, line, m);
         out(line, 0, X.x);
         out(line, 1, Xm.x);
       } else {
@@ -205,7 +244,7 @@ __device__ void line_forward(const LinePlan& pl, const Bufs<T>& B, int L, OUT ou
     const bool dst = pl.kind == 2;
     for (int it = threadIdx.x; it < L * (m + 1); it += blockDim.x) {
       const int line = LF ? it % L : it / (m + 1), k = LF ? it / L : it - line * (m + 1);
-      const cx<T> V = real_fwd_X<T>(pl, B, zb, k, line);
+      const cx<T> V = real_fwd_X<T>(pl, B, zb, k, line, m);
       const cx<T> wk = TWC<T>(pl, k);
       const T yk = (T)2 * (wk.x * V.x - wk.y * V.y);
       if (k < n) out(line, dst ? n - 1 - k : k, yk);
@@ -220,9 +259,10 @@ __device__ void line_forward(const LinePlan& pl, const Bufs<T>& B, int L, OUT ou
 
 // backward: input real line (packed spectrum or natural DCT/DST coefficients)
 // in buffer 1 as pairs; output real line through `out(line, i, v)`
-template <typename T, bool LF, typename OUT>
-__device__ void line_backward(const LinePlan& pl, const Bufs<T>& B, int L, OUT out) {
-  const int m = pl.m, n = pl.n;
+template <typename T, bool LF, int MC, int LC, typename OUT>
+__device__ void line_backward(const LinePlan& pl, const Bufs<T>& B, int Lrt, OUT out) {
+  const int m = MC ? MC : pl.m, n = MC ? 2 * MC : pl.n;
+  const int L = LC ? LC : Lrt;
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * m; it += blockDim.x) {
       const int line = it % L, k = it / L;
@@ -246,7 +286,7 @@ __device__ void line_backward(const LinePlan& pl, const Bufs<T>& B, int L, OUT o
     }
   }
   __syncthreads();
-  const int zb = fft_lines<T>(pl, B, 0, L, +1);
+  const int zb = fft_lines<T, MC, LC>(pl, B, 0, L, +1);
   if (pl.kind == 0) {
     for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
       const int line = LF ? it % L : it / n, i = LF ? it / L : it - line * n;
@@ -288,14 +328,15 @@ __device__ __forceinline__ Bufs<T> smem_bufs(T* sm, int m, int L) {
 // fillps right-hand side rho0*div(u)/dt computed on the fly in FP64
 // (src/fillps.f90:39-50).
 // ---------------------------------------------------------------------------
-template <typename T, bool FUSED>
+template <typename T, bool FUSED, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
     const double* __restrict__ src, const double* __restrict__ u, const double* __restrict__ v,
-    const double* __restrict__ w, Phys ph, T* __restrict__ work, int L) {
+    const double* __restrict__ w, Phys ph, T* __restrict__ work, int Lrt) {
   if (HALTED(sc)) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
-  const int n = pl.n, m = pl.m;
+  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
+  const int L = LC ? LC : Lrt;
   const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int nlines = g.ny * g.nz;
   const int l0 = blockIdx.x * L;
@@ -320,20 +361,21 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const Dev
     str<T>(B, 0, fwd_pos(pl.kind, n, i), line, xv);
   }
   __syncthreads();
-  line_forward<T, false>(pl, B, L, [&](int line, int s, T val) {
+  line_forward<T, false, MC, LC>(pl, B, L, [&](int line, int s, T val) {
     const int gl = l0 + line;
     if (gl < nlines) work[(size_t)gl * n + s] = val;
   });
 }
 
 // ADD: dst += normfft * x (refinement correction) instead of dst = normfft * x
-template <typename T, bool ADD>
+template <typename T, bool ADD, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
-    const T* __restrict__ work, double normfft, double* __restrict__ dst, int L) {
+    const T* __restrict__ work, double normfft, double* __restrict__ dst, int Lrt) {
   if (HALTED(sc)) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
-  const int n = pl.n, m = pl.m;
+  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
+  const int L = LC ? LC : Lrt;
   const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int nlines = g.ny * g.nz;
   const int l0 = blockIdx.x * L;
@@ -343,7 +385,7 @@ __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const Dev
     str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
   }
   __syncthreads();
-  line_backward<T, false>(pl, B, L, [&](int line, int i, T val) {
+  line_backward<T, false, MC, LC>(pl, B, L, [&](int line, int i, T val) {
     const int gl = l0 + line;
     if (gl < nlines) {
       const int j = gl % g.ny + 1, k = gl / g.ny + 1;
@@ -358,13 +400,14 @@ __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const Dev
 // y transforms, in place on the spectral buffer.  Lines = L consecutive x
 // positions of one z plane; the tile is read and written row by row.
 // ---------------------------------------------------------------------------
-template <typename T, int DIR>
+template <typename T, int DIR, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
-                                               T* __restrict__ work, int L) {
+                                               T* __restrict__ work, int Lrt) {
   if (HALTED(sc)) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
-  const int n = pl.n, m = pl.m, nx = g.nx;
+  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m, nx = g.nx;
+  const int L = LC ? LC : Lrt;
   const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
   const int i0 = blockIdx.x * L, k = blockIdx.y;
   T* plane = work + (size_t)k * nx * n;
@@ -384,8 +427,8 @@ __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScal
     const int i = i0 + line;
     if (i < nx) plane[(size_t)j * nx + i] = val;
   };
-  if (DIR > 0) line_forward<T, true>(pl, B, L, out);
-  else line_backward<T, true>(pl, B, L, out);
+  if (DIR > 0) line_forward<T, true, MC, LC>(pl, B, L, out);
+  else line_backward<T, true, MC, LC>(pl, B, L, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -406,13 +449,14 @@ template <> struct Rn<double> {
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  // 1/x correctly rounded: the same value as the division 1./x
+  static __device__ __forceinline__ double rcp(double b) { return __drcp_rn(b); }
 };
 template <> struct Rn<float> {
   static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
   static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float rcp(float b) { return __frcp_rn(b); }
 };
 
 // 1./(b(l)+lambda - a(l)*d(l-1) + eps); `pin`: singular column, last row
@@ -420,8 +464,8 @@ template <typename T>
 __device__ __forceinline__ T piv_inv(int l, int n, T bl, T lam, T al, T dprev, bool pin) {
   typedef Rn<T> R;
   if (pin && l == n - 1) return (T)0;
-  if (l == 0) return R::div((T)1, R::add(R::add(bl, lam), (T)CANSFZ_EPS));
-  return R::div((T)1, R::add(R::sub(R::add(bl, lam), R::mul(al, dprev)), (T)CANSFZ_EPS));
+  if (l == 0) return R::rcp(R::add(R::add(bl, lam), (T)CANSFZ_EPS));
+  return R::rcp(R::add(R::sub(R::add(bl, lam), R::mul(al, dprev)), (T)CANSFZ_EPS));
 }
 
 template <typename T>
@@ -553,31 +597,41 @@ __global__ void k_residual(Geo g, const DevScalars* __restrict__ sc, const doubl
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-// opt the transform kernels into > 48 KB of dynamic shared memory (once)
-void poisson_set_attributes() {
+// lines per CTA: keep the 4*m*LP elements of shared memory within ~96 KB
+constexpr int lines_per_cta(int m, int maxL, int tsize) {
+  int L = maxL;
+  while (L > 1 && 4LL * m * (L | 1) * tsize > 96 * 1024) L >>= 1;
+  return L;
+}
+constexpr int x_maxL(int m) { return 2 * m >= 128 ? 8 : 32; }
+constexpr int y_maxL() { return 16; }
+template <typename T, int MC>
+constexpr int xL() { return MC ? lines_per_cta(MC, x_maxL(MC), sizeof(T)) : 0; }
+template <typename T, int MC>
+constexpr int yL() { return MC ? lines_per_cta(MC, y_maxL(), sizeof(T)) : 0; }
+
+// the compile-time complex lengths (real lines of 64, 128, 256 and 512
+// points); other lengths take the runtime-length kernels
+#define CANSFZ_FOR_LENGTHS(X) X(32) X(64) X(128) X(256)
+
+template <typename T, int MC>
+static void set_attr_len() {
   const int lim = 100 * 1024;
-#define ATTR(k) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)
-  ATTR((k_fft_x_fwd<double, true>));
-  ATTR((k_fft_x_fwd<double, false>));
-  ATTR((k_fft_x_fwd<float, true>));
-  ATTR((k_fft_x_fwd<float, false>));
-  ATTR((k_fft_x_bwd<double, false>));
-  ATTR((k_fft_x_bwd<double, true>));
-  ATTR((k_fft_x_bwd<float, false>));
-  ATTR((k_fft_x_bwd<float, true>));
-  ATTR((k_fft_y<double, 1>));
-  ATTR((k_fft_y<double, -1>));
-  ATTR((k_fft_y<float, 1>));
-  ATTR((k_fft_y<float, -1>));
-#undef ATTR
+  cudaFuncSetAttribute(k_fft_x_fwd<T, true, MC, xL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_x_fwd<T, false, MC, xL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_x_bwd<T, false, MC, xL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_x_bwd<T, true, MC, xL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_y<T, 1, MC, yL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_y<T, -1, MC, yL<T, MC>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
-template <typename T>
-static int lines_per_cta(int m, int maxL) {
-  // keep the 4*m*LP elements of shared memory within ~96 KB
-  int L = maxL;
-  while (L > 1 && 4 * (size_t)m * (L | 1) * sizeof(T) > 96 * 1024) L >>= 1;
-  return L;
+// opt the transform kernels into > 48 KB of dynamic shared memory (once)
+void poisson_set_attributes() {
+  set_attr_len<double, 0>();
+  set_attr_len<float, 0>();
+#define X(M) set_attr_len<double, M>(); set_attr_len<float, M>();
+  CANSFZ_FOR_LENGTHS(X)
+#undef X
 }
 
 template <typename T> static T* wbuf(const PoissonPlan& pl);
@@ -587,31 +641,54 @@ template <typename T> static T* wbuf2(const PoissonPlan& pl);
 template <> double* wbuf2<double>(const PoissonPlan& pl) { return pl.work2; }
 template <> float* wbuf2<float>(const PoissonPlan& pl) { return pl.work2f; }
 
-template <typename T>
-static void x_forward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
-                      const double* src, const double* u, const double* v, const double* w, const Phys* ph,
-                      bool fused) {
+template <typename T, int MC>
+static void x_forward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                          const double* src, const double* u, const double* v, const double* w, const Phys* ph,
+                          bool fused) {
   const int m = pl.px.m < 1 ? 1 : pl.px.m;
-  const int L = lines_per_cta<T>(m, pl.px.n >= 128 ? 8 : 32);
+  const int L = MC ? xL<T, MC>() : lines_per_cta(m, x_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
   const dim3 grid((nlines + L - 1) / L);
   Phys pz{};
   if (fused)
-    k_fft_x_fwd<T, true><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, nullptr, u, v, w, *ph, wbuf<T>(pl), L);
+    k_fft_x_fwd<T, true, MC, xL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, nullptr, u, v, w, *ph,
+                                                                       wbuf<T>(pl), L);
   else
-    k_fft_x_fwd<T, false><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, src, nullptr, nullptr, nullptr, pz,
-                                                      wbuf<T>(pl), L);
+    k_fft_x_fwd<T, false, MC, xL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, src, nullptr, nullptr,
+                                                                        nullptr, pz, wbuf<T>(pl), L);
+}
+
+template <typename T>
+static void x_forward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                      const double* src, const double* u, const double* v, const double* w, const Phys* ph,
+                      bool fused) {
+  switch (pl.px.m) {
+#define X(M) case M: x_forward_len<T, M>(Lc, g, pl, sc, src, u, v, w, ph, fused); return;
+    CANSFZ_FOR_LENGTHS(X)
+#undef X
+    default: x_forward_len<T, 0>(Lc, g, pl, sc, src, u, v, w, ph, fused);
+  }
+}
+
+template <typename T, int MC>
+static void y_pass_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
+  const int m = pl.py.m < 1 ? 1 : pl.py.m;
+  const int L = MC ? yL<T, MC>() : lines_per_cta(m, y_maxL(), sizeof(T));
+  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
+  const dim3 grid((g.nx + L - 1) / L, g.nz);
+  if (dir > 0) k_fft_y<T, 1, MC, yL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
+  else k_fft_y<T, -1, MC, yL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
 }
 
 template <typename T>
 static void y_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
-  const int m = pl.py.m < 1 ? 1 : pl.py.m;
-  const int L = lines_per_cta<T>(m, 16);
-  const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
-  const dim3 grid((g.nx + L - 1) / L, g.nz);
-  if (dir > 0) k_fft_y<T, 1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
-  else k_fft_y<T, -1><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
+  switch (pl.py.m) {
+#define X(M) case M: y_pass_len<T, M>(Lc, g, pl, sc, dir); return;
+    CANSFZ_FOR_LENGTHS(X)
+#undef X
+    default: y_pass_len<T, 0>(Lc, g, pl, sc, dir);
+  }
 }
 
 template <typename T>
@@ -628,13 +705,25 @@ static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const 
                                                             pl.zsing);
 }
 
-template <typename T, bool ADD>
-static void x_backward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* dst) {
+template <typename T, bool ADD, int MC>
+static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
+                           double* dst) {
   const int m = pl.px.m < 1 ? 1 : pl.px.m;
-  const int L = lines_per_cta<T>(m, pl.px.n >= 128 ? 8 : 32);
+  const int L = MC ? xL<T, MC>() : lines_per_cta(m, x_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
-  k_fft_x_bwd<T, ADD><<<(nlines + L - 1) / L, 256, smem, Lc.st>>>(g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L);
+  k_fft_x_bwd<T, ADD, MC, xL<T, MC>()><<<(nlines + L - 1) / L, 256, smem, Lc.st>>>(g, pl.px, sc, wbuf<T>(pl),
+                                                                                   pl.normfft, dst, L);
+}
+
+template <typename T, bool ADD>
+static void x_backward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, double* dst) {
+  switch (pl.px.m) {
+#define X(M) case M: x_backward_len<T, ADD, M>(Lc, g, pl, sc, dst); return;
+    CANSFZ_FOR_LENGTHS(X)
+#undef X
+    default: x_backward_len<T, ADD, 0>(Lc, g, pl, sc, dst);
+  }
 }
 
 // solver_gpu on the interior of the halo-layout field p (in place)

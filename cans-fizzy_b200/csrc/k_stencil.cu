@@ -28,162 +28,60 @@ __device__ __forceinline__ double sq(double x) { return x * x; }
 #define LD(p, q) __ldg((p) + (q))
 
 // ---------------------------------------------------------------------------
-// acdi_transport_pf, src/acdi.f90:64-225
+// acdi_transport_pf, src/acdi.f90:64-225: the z-marching tile kernel of
+// k_tiles.cu (face fluxes computed once per face)
 // ---------------------------------------------------------------------------
-// UPD: rk_2fl fused in (src/rk.f90:234-248): psi_out = clip(psi + f1*d + f2*d_old),
-// the history slot `dpsidt` holds d_old on entry and d on exit.
-template <bool SDF, bool UPD>
-__global__ void __launch_bounds__(128) k_acdi_transport(Geo g, const DevScalars* __restrict__ sc,
-    const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
-    const double* __restrict__ nx_, const double* __restrict__ ny_, const double* __restrict__ nz_,
-    const double* __restrict__ phi, const double* __restrict__ psi, double* __restrict__ dpsidt,
-    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ psi_out) {
-  if (HALTED(sc)) return;
-  INTERIOR_IJK(g)
-  const double gam = sc->gam, seps = sc->seps;
-  const double dxi = g.dxi, dyi = g.dyi;
-  const double dzfi_c = g.dzfi[k], dzci_c = g.dzci[k], dzci_m = g.dzci[k - 1];
-  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
-  const double psi_ccm = LD(psi, c - sxy), psi_cmc = LD(psi, c - sx), psi_mcc = LD(psi, c - 1),
-               psi_ccc = LD(psi, c), psi_pcc = LD(psi, c + 1), psi_cpc = LD(psi, c + sx),
-               psi_ccp = LD(psi, c + sxy);
-  const double u_mcc = LD(u, c - 1), u_ccc = LD(u, c);
-  const double v_cmc = LD(v, c - sx), v_ccc = LD(v, c);
-  const double w_ccm = LD(w, c - sxy), w_ccc = LD(w, c);
-  const double nxc = LD(nx_, c), nyc = LD(ny_, c), nzc = LD(nz_, c);
-  const int off[6] = {-1, 1, -sx, sx, -sxy, sxy};
-  double nxf[6], nyf[6], nzf[6];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    nxf[q] = 0.5 * (LD(nx_, c + off[q]) + nxc);
-    nyf[q] = 0.5 * (LD(ny_, c + off[q]) + nyc);
-    nzf[q] = 0.5 * (LD(nz_, c + off[q]) + nzc);
-  }
-  // advection
-  const double upsiim = 0.5 * (psi_mcc + psi_ccc) * u_mcc;
-  const double upsiip = 0.5 * (psi_pcc + psi_ccc) * u_ccc;
-  const double vpsijm = 0.5 * (psi_cmc + psi_ccc) * v_cmc;
-  const double vpsijp = 0.5 * (psi_cpc + psi_ccc) * v_ccc;
-  const double wpsikm = 0.5 * (psi_ccm + psi_ccc) * w_ccm;
-  const double wpsikp = 0.5 * (psi_ccp + psi_ccc) * w_ccc;
-  const double adv = dxi * (upsiip - upsiim) + dyi * (vpsijp - vpsijm) + dzfi_c * (wpsikp - wpsikm);
-  // diffusion
-  const double gs = gam * seps;
-  const double dpsidxm = gs * (psi_ccc - psi_mcc) * dxi;
-  const double dpsidxp = gs * (psi_pcc - psi_ccc) * dxi;
-  const double dpsidym = gs * (psi_ccc - psi_cmc) * dyi;
-  const double dpsidyp = gs * (psi_cpc - psi_ccc) * dyi;
-  const double dpsidzm = gs * (psi_ccc - psi_ccm) * dzci_m;
-  const double dpsidzp = gs * (psi_ccp - psi_ccc) * dzci_c;
-  // sharpening: face-normal component of the averaged normal, normalised
-  const double rn_01 = nxf[0] / (sqrt(sq(nxf[0]) + sq(nyf[0]) + sq(nzf[0])) + CANSFZ_EPS);
-  const double rn_11 = nxf[1] / (sqrt(sq(nxf[1]) + sq(nyf[1]) + sq(nzf[1])) + CANSFZ_EPS);
-  const double rn_02 = nyf[2] / (sqrt(sq(nxf[2]) + sq(nyf[2]) + sq(nzf[2])) + CANSFZ_EPS);
-  const double rn_12 = nyf[3] / (sqrt(sq(nxf[3]) + sq(nyf[3]) + sq(nzf[3])) + CANSFZ_EPS);
-  const double rn_03 = nzf[4] / (sqrt(sq(nxf[4]) + sq(nyf[4]) + sq(nzf[4])) + CANSFZ_EPS);
-  const double rn_13 = nzf[5] / (sqrt(sq(nxf[5]) + sq(nyf[5]) + sq(nzf[5])) + CANSFZ_EPS);
-  double sharpxm, sharpxp, sharpym, sharpyp, sharpzm, sharpzp;
-  if (SDF) {
-    const double phi_ccc = LD(phi, c);
-    const double qg = 0.25 * gam;
-    const double is = 1. / seps;  // (0.25*(a+b))/seps as (0.25*(a+b))*(1/seps)
-    sharpxm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - 1)) * is))) * rn_01);
-    sharpxp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + 1) + phi_ccc) * is))) * rn_11);
-    sharpym = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sx)) * is))) * rn_02);
-    sharpyp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sx) + phi_ccc) * is))) * rn_12);
-    sharpzm = qg * ((1. - sq(tanh(0.25 * (phi_ccc + LD(phi, c - sxy)) * is))) * rn_03);
-    sharpzp = qg * ((1. - sq(tanh(0.25 * (LD(phi, c + sxy) + phi_ccc) * is))) * rn_13);
-  } else {
-    const double psi_xm = 0.5 * (psi_ccc + psi_mcc), psi_xp = 0.5 * (psi_pcc + psi_ccc);
-    const double psi_ym = 0.5 * (psi_ccc + psi_cmc), psi_yp = 0.5 * (psi_cpc + psi_ccc);
-    const double psi_zm = 0.5 * (psi_ccc + psi_ccm), psi_zp = 0.5 * (psi_ccp + psi_ccc);
-    sharpxm = gam * psi_xm * (1. - psi_xm) * rn_01;
-    sharpxp = gam * psi_xp * (1. - psi_xp) * rn_11;
-    sharpym = gam * psi_ym * (1. - psi_ym) * rn_02;
-    sharpyp = gam * psi_yp * (1. - psi_yp) * rn_12;
-    sharpzm = gam * psi_zm * (1. - psi_zm) * rn_03;
-    sharpzp = gam * psi_zp * (1. - psi_zp) * rn_13;
-  }
-  const double rglrxm = dpsidxm - sharpxm, rglrxp = dpsidxp - sharpxp;
-  const double rglrym = dpsidym - sharpym, rglryp = dpsidyp - sharpyp;
-  const double rglrzm = dpsidzm - sharpzm, rglrzp = dpsidzp - sharpzp;
-  const double rglr = (rglrxp - rglrxm) * dxi + (rglryp - rglrym) * dyi + (rglrzp - rglrzm) * dzfi_c;
-  const double d = -adv + rglr;
-  if (UPD) {
-    const int t = g.t(i, j, k);
-    const double dO = sc->first_rk2fl ? d : dpsidt[t];
-    psi_out[c] = fmin(fmax(0., psi_ccc + sc->f1 * d + sc->f2 * dO), 1.);
-    dpsidt[t] = d;
-  } else {
-    dpsidt[g.t(i, j, k)] = d;
-  }
-  fx[c] = upsiip - rglrxp;
-  fy[c] = vpsijp - rglryp;
-  fz[c] = wpsikp - rglrzp;
-}
-
 void launch_acdi_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
                            const double* u, const double* v, const double* w, const double* nx,
                            const double* ny, const double* nz, const double* phi, const double* psi,
                            double* dpsidt, double* fx, double* fy, double* fz) {
-  dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  if (sdf)
-    k_acdi_transport<true, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, dpsidt, fx, fy, fz,
-                                                      nullptr);
-  else
-    k_acdi_transport<false, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, dpsidt, fx, fy, fz,
-                                                       nullptr);
+  launch_acdi_t<double>(L, g, sc, sdf, false, u, v, w, nx, ny, nz, phi, psi, nullptr, dpsidt, fx, fy, fz);
 }
 
 void launch_acdi_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
                       const double* v, const double* w, const double* nx, const double* ny, const double* nz,
                       const double* phi, const double* psi, double* psi_out, double* hist, double* fx, double* fy,
                       double* fz) {
-  dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  if (sdf)
-    k_acdi_transport<true, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz,
-                                                     psi_out);
-  else
-    k_acdi_transport<false, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz,
-                                                      psi_out);
+  launch_acdi_t<double>(L, g, sc, sdf, true, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
 }
 
 // ---------------------------------------------------------------------------
 // vof_thinc_transport_psi, src/vof_thinc_qq.f90:39-133: fluxes over faces
 // 0..n, then the flux divergence on the interior.
 // ---------------------------------------------------------------------------
-template <bool SDF>
+template <typename TI, bool SDF>
 __global__ void k_thinc_flux(Geo g, const DevScalars* __restrict__ sc,
     const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
-    const double* __restrict__ nx_, const double* __restrict__ ny_, const double* __restrict__ nz_,
-    const double* __restrict__ phi, const double* __restrict__ psi,
-    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+    const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
+    const TI* __restrict__ phi, const double* __restrict__ psi,
+    TI* __restrict__ fx, TI* __restrict__ fy, TI* __restrict__ fz) {
+  typedef TI T;  // FP64 in the drop-in, FP32 in the mixed form
   if (HALTED(sc)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0..n
   if (i > g.nx) return;
   const int j = blockIdx.y, k = blockIdx.z;
-  const double beta = sc->beta;
+  const T beta = (T)sc->beta;
   const int c = g.h(i, j, k);
-  const double vel_x = LD(u, c), vel_y = LD(v, c), vel_z = LD(w, c);
+  const T vel_x = (T)LD(u, c), vel_y = (T)LD(v, c), vel_z = (T)LD(w, c);
   int ci, cj, ck;
-  double xx, yy, zz;
-  if (vel_x > 0.) { ci = c; xx = 0.5; } else { ci = c + 1; xx = -0.5; }
-  if (vel_y > 0.) { cj = c; yy = 0.5; } else { cj = c + g.sx; yy = -0.5; }
-  if (vel_z > 0.) { ck = c; zz = 0.5; } else { ck = c + g.sxy; zz = -0.5; }
-  const double lnormx_x = LD(nx_, ci), lnormy_y = LD(ny_, cj), lnormz_z = LD(nz_, ck);
-  double d_x, d_y, d_z;
+  T xx, yy, zz;
+  if (vel_x > T(0.)) { ci = c; xx = T(0.5); } else { ci = c + 1; xx = T(-0.5); }
+  if (vel_y > T(0.)) { cj = c; yy = T(0.5); } else { cj = c + g.sx; yy = T(-0.5); }
+  if (vel_z > T(0.)) { ck = c; zz = T(0.5); } else { ck = c + g.sxy; zz = T(-0.5); }
+  const T lnormx_x = LD(nx_, ci), lnormy_y = LD(ny_, cj), lnormz_z = LD(nz_, ck);
+  T d_x, d_y, d_z;
   if (SDF) {
     d_x = LD(phi, ci); d_y = LD(phi, cj); d_z = LD(phi, ck);
   } else {
-    const double hb = -.5 / beta;
-    d_x = hb * log(1. / (LD(psi, ci) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
-    d_y = hb * log(1. / (LD(psi, cj) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
-    d_z = hb * log(1. / (LD(psi, ck) + CANSFZ_EPS) - 1. + CANSFZ_EPS);
+    const T hb = T(-.5) / beta;
+    d_x = hb * log(T(1.) / ((T)LD(psi, ci) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
+    d_y = hb * log(T(1.) / ((T)LD(psi, cj) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
+    d_z = hb * log(T(1.) / ((T)LD(psi, ck) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
   }
-  const double m2b = -2. * beta;
-  fx[c] = vel_x * (1. / (1. + exp(m2b * (lnormx_x * xx + d_x))));
-  fy[c] = vel_y * (1. / (1. + exp(m2b * (lnormy_y * yy + d_y))));
-  fz[c] = vel_z * (1. / (1. + exp(m2b * (lnormz_z * zz + d_z))));
+  const T m2b = T(-2.) * beta;
+  fx[c] = vel_x * (T(1.) / (T(1.) + exp(m2b * (lnormx_x * xx + d_x))));
+  fy[c] = vel_y * (T(1.) / (T(1.) + exp(m2b * (lnormy_y * yy + d_y))));
+  fz[c] = vel_z * (T(1.) / (T(1.) + exp(m2b * (lnormz_z * zz + d_z))));
 }
 
 __global__ void k_thinc_div(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ fx,
@@ -197,29 +95,41 @@ __global__ void k_thinc_div(Geo g, const DevScalars* __restrict__ sc, const doub
 }
 
 // flux divergence + rk_2fl update (history in place), src/vof_thinc_qq.f90:122-132, src/rk.f90:240-248
-__global__ void k_thinc_div_update(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ fx,
-                                   const double* __restrict__ fy, const double* __restrict__ fz,
-                                   const double* __restrict__ psi, double* __restrict__ hist,
+template <typename TI>
+__global__ void k_thinc_div_update(Geo g, const DevScalars* __restrict__ sc, const TI* __restrict__ fx,
+                                   const TI* __restrict__ fy, const TI* __restrict__ fz,
+                                   const double* __restrict__ psi, TI* __restrict__ hist,
                                    double* __restrict__ psi_out) {
+  typedef TI T;
   if (HALTED(sc)) return;
   INTERIOR_IJK(g)
   const int c = g.h(i, j, k), t = g.t(i, j, k);
-  const double d = -(g.dxi * (LD(fx, c) - LD(fx, c - 1)) + g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
-                     g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
-  const double dO = sc->first_rk2fl ? d : hist[t];
-  psi_out[c] = fmin(fmax(0., LD(psi, c) + sc->f1 * d + sc->f2 * dO), 1.);
+  const T d = -((T)g.dxi * (LD(fx, c) - LD(fx, c - 1)) + (T)g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
+                (T)g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
+  const T dO = sc->first_rk2fl ? d : hist[t];
+  psi_out[c] = fmin(fmax(0., LD(psi, c) + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
   hist[t] = d;
 }
+
+template <typename TI>
+void launch_thinc_step_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
+                         const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
+                         const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
+  dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
+  if (sdf) k_thinc_flux<TI, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  else k_thinc_flux<TI, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
+  k_thinc_div_update<TI><<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, psi, hist, psi_out);
+}
+template void launch_thinc_step_t<float>(const Launch&, const Geo&, const DevScalars*, bool, const double*,
+                                         const double*, const double*, const float*, const float*, const float*,
+                                         const float*, const double*, double*, float*, float*, float*, float*);
 
 void launch_thinc_step(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, const double* u,
                        const double* v, const double* w, const double* nx, const double* ny, const double* nz,
                        const double* phi, const double* psi, double* psi_out, double* hist, double* fx, double* fy,
                        double* fz) {
-  dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
-  if (sdf) k_thinc_flux<true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
-  else k_thinc_flux<false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
-  dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
-  k_thinc_div_update<<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, psi, hist, psi_out);
+  launch_thinc_step_t<double>(L, g, sc, sdf, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
 }
 
 void launch_thinc_transport(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf,
@@ -227,8 +137,8 @@ void launch_thinc_transport(const Launch& L, const Geo& g, const DevScalars* sc,
                             const double* ny, const double* nz, const double* phi, const double* psi,
                             double* dpsidt, double* fx, double* fy, double* fz) {
   dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
-  if (sdf) k_thinc_flux<true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
-  else k_thinc_flux<false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  if (sdf) k_thinc_flux<double, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  else k_thinc_flux<double, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
   dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
   k_thinc_div<<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, dpsidt);
 }
@@ -259,97 +169,49 @@ void launch_psi_update(const Launch& L, const Geo& g, const DevScalars* sc, cons
 // acdi_cmpt_phi (src/acdi.f90:227-248), vof_thinc_cmpt_phi
 // (src/vof_thinc_qq.f90:135-157): whole halo array
 // ---------------------------------------------------------------------------
-template <bool ACDI>
+template <bool ACDI, typename TO>
 __global__ void k_cmpt_phi(int n, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
-                           double* __restrict__ phi) {
+                           TO* __restrict__ phi) {
   if (HALTED(sc)) return;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const double ps = LD(psi, q);
   if (ACDI) {
-    phi[q] = sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS));
+    phi[q] = (TO)(sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS)));
   } else {
     const double pa = fmin(fmax(ps, CANSFZ_EPS), 1. - CANSFZ_EPS);
-    phi[q] = 0.5 / sc->beta * log(pa / (1. - pa));
+    phi[q] = (TO)(0.5 / sc->beta * log(pa / (1. - pa)));
   }
 }
 
 void launch_cmpt_phi(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
                      double* phi) {
   const int n = g.hsize();
-  if (acdi) k_cmpt_phi<true><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
-  else k_cmpt_phi<false><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  if (acdi) k_cmpt_phi<true, double><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  else k_cmpt_phi<false, double><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+}
+// the mixed form: phi evaluated in FP64 and stored in FP32
+// (narrow_only: Youngs without SDF normals works on psi itself, stored in FP32)
+__global__ void k_narrow(int n, const DevScalars* __restrict__ sc, const double* __restrict__ src,
+                         float* __restrict__ dst) {
+  if (HALTED(sc)) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = (float)src[q];
+}
+void launch_cmpt_phi_f32(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
+                         float* phi, bool narrow_only) {
+  const int n = g.hsize();
+  if (narrow_only) k_narrow<<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  else if (acdi) k_cmpt_phi<true, float><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  else k_cmpt_phi<false, float><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
 }
 
 // ---------------------------------------------------------------------------
 // cmpt_norm_curv_youngs, src/two_fluid.f90:60-175
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_youngs(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
-                                                double* __restrict__ normx, double* __restrict__ normy,
-                                                double* __restrict__ normz, double* __restrict__ kappa) {
-  if (HALTED(sc)) return;
-  INTERIOR_IJK(g)
-  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
-#define PS(a, b, cc) LD(psi, c + (a) + (b) * sx + (cc) * sxy)
-  const double psimmm = PS(-1, -1, -1), psimcm = PS(-1, 0, -1), psimpm = PS(-1, 1, -1),
-               psicmm = PS(0, -1, -1), psiccm = PS(0, 0, -1), psicpm = PS(0, 1, -1),
-               psipmm = PS(1, -1, -1), psipcm = PS(1, 0, -1), psippm = PS(1, 1, -1),
-               psimmc = PS(-1, -1, 0), psimcc = PS(-1, 0, 0), psimpc = PS(-1, 1, 0),
-               psicmc = PS(0, -1, 0), psiccc = PS(0, 0, 0), psicpc = PS(0, 1, 0),
-               psipmc = PS(1, -1, 0), psipcc = PS(1, 0, 0), psippc = PS(1, 1, 0),
-               psimmp = PS(-1, -1, 1), psimcp = PS(-1, 0, 1), psimpp = PS(-1, 1, 1),
-               psicmp = PS(0, -1, 1), psiccp = PS(0, 0, 1), psicpp = PS(0, 1, 1),
-               psipmp = PS(1, -1, 1), psipcp = PS(1, 0, 1), psippp = PS(1, 1, 1);
-#undef PS
-  const double d1 = g.dxi, d2 = g.dyi, zc = g.dzci[k], zm = g.dzci[k - 1];
-  double mx[8], my[8], mz[8];
-  mx[0] = 0.25 * ((psipcc + psippc + psipcp + psippp) - (psiccc + psicpc + psiccp + psicpp)) * d1;
-  mx[1] = 0.25 * ((psipcc + psipmc + psipcp + psipmp) - (psiccc + psicmc + psiccp + psicmp)) * d1;
-  mx[2] = 0.25 * ((psipcc + psippc + psipcm + psippm) - (psiccc + psicpc + psiccm + psicpm)) * d1;
-  mx[3] = 0.25 * ((psipcc + psipmc + psipcm + psipmm) - (psiccc + psicmc + psiccm + psicmm)) * d1;
-  mx[4] = 0.25 * ((psiccc + psicpc + psiccp + psicpp) - (psimcc + psimpc + psimcp + psimpp)) * d1;
-  mx[5] = 0.25 * ((psiccc + psicmc + psiccp + psicmp) - (psimcc + psimmc + psimcp + psimmp)) * d1;
-  mx[6] = 0.25 * ((psiccc + psicpc + psiccm + psicpm) - (psimcc + psimpc + psimcm + psimpm)) * d1;
-  mx[7] = 0.25 * ((psiccc + psicmc + psiccm + psicmm) - (psimcc + psimmc + psimcm + psimmm)) * d1;
-  my[0] = 0.25 * ((psicpc + psippc + psicpp + psippp) - (psiccc + psipcc + psiccp + psipcp)) * d2;
-  my[1] = 0.25 * ((psiccc + psipcc + psiccp + psipcp) - (psicmc + psipmc + psicmp + psipmp)) * d2;
-  my[2] = 0.25 * ((psicpc + psippc + psicpm + psippm) - (psiccc + psipcc + psiccm + psipcm)) * d2;
-  my[3] = 0.25 * ((psiccc + psipcc + psiccm + psipcm) - (psicmc + psipmc + psicmm + psipmm)) * d2;
-  my[4] = 0.25 * ((psicpc + psimpc + psicpp + psimpp) - (psiccc + psimcc + psiccp + psimcp)) * d2;
-  my[5] = 0.25 * ((psiccc + psimcc + psiccp + psimcp) - (psicmc + psimmc + psicmp + psimmp)) * d2;
-  my[6] = 0.25 * ((psicpc + psimpc + psicpm + psimpm) - (psiccc + psimcc + psiccm + psimcm)) * d2;
-  my[7] = 0.25 * ((psiccc + psimcc + psiccm + psimcm) - (psicmc + psimmc + psicmm + psimmm)) * d2;
-  mz[0] = 0.25 * ((psiccp + psipcp + psicpp + psippp) - (psiccc + psipcc + psicpc + psippc)) * zc;
-  mz[1] = 0.25 * ((psiccp + psipcp + psicmp + psipmp) - (psiccc + psipcc + psicmc + psipmc)) * zc;
-  mz[2] = 0.25 * ((psiccc + psipcc + psicpc + psippc) - (psiccm + psipcm + psicpm + psippm)) * zm;
-  mz[3] = 0.25 * ((psiccc + psipcc + psicmc + psipmc) - (psiccm + psipcm + psicmm + psipmm)) * zm;
-  mz[4] = 0.25 * ((psiccp + psimcp + psicpp + psimpp) - (psiccc + psimcc + psicpc + psimpc)) * zc;
-  mz[5] = 0.25 * ((psiccp + psimcp + psicmp + psimmp) - (psiccc + psimcc + psicmc + psimmc)) * zc;
-  mz[6] = 0.25 * ((psiccc + psimcc + psicpc + psimpc) - (psiccm + psimcm + psicpm + psimpm)) * zm;
-  mz[7] = 0.25 * ((psiccc + psimcc + psicmc + psimmc) - (psiccm + psimcm + psicmm + psimmm)) * zm;
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const double norm = sqrt(sq(mx[q]) + sq(my[q]) + sq(mz[q])) + CANSFZ_EPS;
-    const double inv = 1. / norm;  // one FP64 division instead of three (within 1 ulp of x/norm)
-    mx[q] = mx[q] * inv; my[q] = my[q] * inv; mz[q] = mz[q] * inv;
-  }
-  const double norm_x = .125 * (mx[0] + mx[1] + mx[2] + mx[3] + mx[4] + mx[5] + mx[6] + mx[7]);
-  const double norm_y = .125 * (my[0] + my[1] + my[2] + my[3] + my[4] + my[5] + my[6] + my[7]);
-  const double norm_z = .125 * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
-  const double norm = sqrt(sq(norm_x) + sq(norm_y) + sq(norm_z)) + CANSFZ_EPS;
-  const double inv = 1. / norm;
-  normx[c] = norm_x * inv;
-  normy[c] = norm_y * inv;
-  normz[c] = norm_z * inv;
-  kappa[c] = -(0.25 * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
-               0.25 * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
-               0.25 * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * g.dzfi[k]);
-}
-
 void launch_youngs(const Launch& L, const Geo& g, const DevScalars* sc, const double* psi, double* nx, double* ny,
                    double* nz, double* kappa) {
-  dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_youngs<<<gr, b, 0, L.st>>>(g, sc, psi, nx, ny, nz, kappa);
+  launch_youngs_t<double>(L, g, sc, psi, nx, ny, nz, kappa);
 }
 
 // clip_field, src/two_fluid.f90:35-58 (whole halo array)
@@ -615,54 +477,15 @@ void launch_rk_update2(const Launch& L, const Geo& g, const Phys& ph, const DevS
 }
 
 // ---------------------------------------------------------------------------
-// The whole of rk (src/rk.f90:16-131) in one pass per cell: mom_xyz_ad, the
-// first AB2 update with the density ratio, mom_xyz_oth, the second update.
-// Reads u,v,w (13-point), psi (16-point), psio, psiflx_x/y/z, p (= pn, as it
-// is when the driver calls rk), po, kappa and the AB2 history; writes the new
-// velocity into separate buffers and the new history over the old one.
+// The whole of rk (src/rk.f90:16-131) in one pass: the z-marching tile kernel
+// of k_tiles.cu (reads p for pn, as the driver calls rk with pn = p)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_momentum_fused(Geo g, Phys ph, const DevScalars* __restrict__ sc,
-    const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
-    const double* __restrict__ psi, const double* __restrict__ psio, const double* __restrict__ fx,
-    const double* __restrict__ fy, const double* __restrict__ fz, const double* __restrict__ p,
-    const double* __restrict__ po, const double* __restrict__ kappa, double* __restrict__ duo,
-    double* __restrict__ dvo, double* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo,
-    double* __restrict__ wo) {
-  if (HALTED(sc)) return;
-  INTERIOR_IJK(g)
-  const AdOut r = mom_ad_cell(g, ph, i, j, k, fx, fy, fz, u, v, w, psi);
-  const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
-  const int c = g.h(i, j, k), t = g.t(i, j, k);
-  const double po_c = LD(psio, c), ps_c = LD(psi, c);
-  const double rhox_n = rho + drho * 0.5 * (po_c + LD(psio, c + 1));
-  const double rhoy_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sx));
-  const double rhoz_n = rho + drho * 0.5 * (po_c + LD(psio, c + g.sxy));
-  const double rhox_p = rho + drho * 0.5 * (ps_c + LD(psi, c + 1));
-  const double rhoy_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sx));
-  const double rhoz_p = rho + drho * 0.5 * (ps_c + LD(psi, c + g.sxy));
-  const bool first = sc->first_rk;
-  const double Ruo = first ? r.du : duo[t], Rvo = first ? r.dv : dvo[t], Rwo = first ? r.dw : dwo[t];
-  const double f1 = sc->f1, f2 = sc->f2, f12 = sc->f12;
-  // one reciprocal per face density instead of four divisions
-  const double irx = 1. / rhox_p, iry = 1. / rhoy_p, irz = 1. / rhoz_p;
-  double un = LD(u, c) * rhox_n * irx + (f1 * r.du + f2 * Ruo) * irx;
-  double vn = LD(v, c) * rhoy_n * iry + (f1 * r.dv + f2 * Rvo) * iry;
-  double wn = LD(w, c) * rhoz_n * irz + (f1 * r.dw + f2 * Rwo) * irz;
-  duo[t] = r.du; dvo[t] = r.dv; dwo[t] = r.dw;
-  const AdOut s = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, p, po);
-  uo[c] = un + f12 * s.du * irx;
-  vo[c] = vn + f12 * s.dv * iry;
-  wo[c] = wn + f12 * s.dw * irz;
-}
-
 void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                            const double* v, const double* w, const double* psi, const double* psio,
                            const double* fx, const double* fy, const double* fz, const double* p,
                            const double* po, const double* kappa, double* duo, double* dvo, double* dwo,
                            double* uo, double* vo, double* wo) {
-  dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_momentum_fused<<<gr, b, 0, L.st>>>(g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo,
-                                       uo, vo, wo);
+  launch_momentum_t<double>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,6 +565,20 @@ __global__ void k_fillv(size_t n, double val, double* __restrict__ d) {
 void launch_fill(const Launch& L, size_t n, double val, double* dst) {
   k_fillv<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, val, dst);
 }
+__global__ void k_fillf(size_t n, float val, float* __restrict__ d) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) d[q] = val;
+}
+void launch_fill(const Launch& L, size_t n, float val, float* dst) {
+  k_fillf<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, val, dst);
+}
+__global__ void k_widen(size_t n, const float* __restrict__ s, double* __restrict__ d) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) d[q] = (double)s[q];
+}
+void launch_widen(const Launch& L, size_t n, const float* src, double* dst) {
+  k_widen<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, src, dst);
+}
 
 // ---------------------------------------------------------------------------
 // reductions.  Maxima of non-negative doubles via atomicMax on the bit
@@ -810,20 +647,43 @@ __device__ __forceinline__ double reduce_max_partials(int n, const double* __res
   for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, part[q]);
   return block_max(m);
 }
+__device__ __forceinline__ void gamma_finish(const Phys& ph, DevScalars* sc, double velmax, int apply_floor) {
+  double gam = sqrt(velmax) * ph.gam_factor;
+  if (apply_floor) gam = fmax(gam, ph.gam_min);
+  sc->gam = gam;
+}
 __global__ void k_gamma_final(Phys ph, DevScalars* __restrict__ sc, int n, const double* __restrict__ part,
                               int apply_floor) {
   if (HALTED(sc)) return;
   const double velmax = reduce_max_partials(n, part);
   if (threadIdx.x != 0) return;
-  double gam = sqrt(velmax) * ph.gam_factor;
-  if (apply_floor) gam = fmax(gam, ph.gam_min);
-  sc->gam = gam;
+  gamma_finish(ph, sc, velmax, apply_floor);
 }
 void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, const double* u,
                   const double* v, const double* w, bool apply_floor) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
   k_gamma_max<<<gr, b, 0, L.st>>>(g, sc, partial, u, v, w);
   k_gamma_final<<<1, 1024, 0, L.st>>>(ph, sc, (int)(gr.x * gr.y * gr.z), partial, apply_floor ? 1 : 0);
+}
+
+// the per-point maximum of chkdt (src/chkdt.f90:47-78)
+__device__ __forceinline__ double chkdt_cell(const Geo& g, int i, int j, int k, const double* __restrict__ u,
+                                             const double* __restrict__ v, const double* __restrict__ w) {
+  const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
+  const double dxi = 1. / g.dx, dyi = 1. / g.dy;
+  const double ux = fabs(LD(u, c));
+  const double vx = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c + 1) + LD(v, c + 1 - sx));
+  const double wx = 0.25 * fabs(LD(w, c) + LD(w, c - sxy) + LD(w, c + 1) + LD(w, c + 1 - sxy));
+  const double dtix = ux * dxi + vx * dyi + wx * g.dzfi[k];
+  const double uy = 0.25 * fabs(LD(u, c) + LD(u, c + sx) + LD(u, c - 1 + sx) + LD(u, c - 1));
+  const double vy = fabs(LD(v, c));
+  const double wy = 0.25 * fabs(LD(w, c) + LD(w, c + sx) + LD(w, c + sx - sxy) + LD(w, c - sxy));
+  const double dtiy = uy * dxi + vy * dyi + wy * g.dzfi[k];
+  const double uz = 0.25 * fabs(LD(u, c) + LD(u, c - 1) + LD(u, c - 1 + sxy) + LD(u, c + sxy));
+  const double vz = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c - sx + sxy) + LD(v, c + sxy));
+  const double wz = fabs(LD(w, c));
+  const double dtiz = uz * dxi + vz * dyi + wz * g.dzci[k];
+  return fmax(dtix, fmax(dtiy, dtiz));
 }
 
 // chkdt, src/chkdt.f90:15-94
@@ -834,32 +694,12 @@ __global__ void k_chkdt_max(Geo g, DevScalars* __restrict__ sc, int only_on_chec
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y + 1, k = blockIdx.z + 1;
   double dti = 0.;
-  if (i <= g.nx) {
-    const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
-    const double dxi = 1. / g.dx, dyi = 1. / g.dy;
-    const double ux = fabs(LD(u, c));
-    const double vx = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c + 1) + LD(v, c + 1 - sx));
-    const double wx = 0.25 * fabs(LD(w, c) + LD(w, c - sxy) + LD(w, c + 1) + LD(w, c + 1 - sxy));
-    const double dtix = ux * dxi + vx * dyi + wx * g.dzfi[k];
-    const double uy = 0.25 * fabs(LD(u, c) + LD(u, c + sx) + LD(u, c - 1 + sx) + LD(u, c - 1));
-    const double vy = fabs(LD(v, c));
-    const double wy = 0.25 * fabs(LD(w, c) + LD(w, c + sx) + LD(w, c + sx - sxy) + LD(w, c - sxy));
-    const double dtiy = uy * dxi + vy * dyi + wy * g.dzfi[k];
-    const double uz = 0.25 * fabs(LD(u, c) + LD(u, c - 1) + LD(u, c - 1 + sxy) + LD(u, c + sxy));
-    const double vz = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c - sx + sxy) + LD(v, c + sxy));
-    const double wz = fabs(LD(w, c));
-    const double dtiz = uz * dxi + vz * dyi + wz * g.dzci[k];
-    dti = fmax(dtix, fmax(dtiy, dtiz));
-  }
+  if (i <= g.nx) dti = chkdt_cell(g, i, j, k, u, v, w);
   dti = block_max(dti);
   if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = dti;
 }
-// completes chkdt and the dt update of src/main.f90:530-551
-__global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int in_loop, int n,
-                              const double* __restrict__ part) {
-  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
-  double dti = reduce_max_partials(n, part);
-  if (threadIdx.x != 0) return;
+// the dt update of src/main.f90:530-551 from the maximum of chkdt
+__device__ __forceinline__ void chkdt_finish(const Phys& ph, DevScalars* sc, double dti, int in_loop) {
   double dtipsi;
   if (ph.acdi) {
     dtipsi = sc->gam * sc->seps / (ph.dlmin * ph.dlmin);
@@ -888,6 +728,15 @@ __global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_
   sc->dt = dt;
   sc->dti = 1. / dt;
   if (in_loop && dtmax < ph.small) sc->status = CANSFZ_ERR_DT;
+}
+
+// completes chkdt and the dt update of src/main.f90:530-551
+__global__ void k_chkdt_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int in_loop, int n,
+                              const double* __restrict__ part) {
+  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+  const double dti = reduce_max_partials(n, part);
+  if (threadIdx.x != 0) return;
+  chkdt_finish(ph, sc, dti, in_loop);
 }
 void launch_chkdt(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, const double* u,
                   const double* v, const double* w, bool only_on_check) {
@@ -927,17 +776,20 @@ __global__ void k_sum_partials(int n, const double* __restrict__ part, double* _
   s = block_sum(s);
   if (threadIdx.x == 0) *out = s;
 }
+__device__ __forceinline__ void chkdiv_finish(double small, DevScalars* sc, double divmax, int only_on_check) {
+  sc->divmax = divmax;
+  // src/main.f90:552-561, after the dt checks (an earlier dt abort is kept)
+  if (only_on_check && sc->status == CANSFZ_OK) {
+    if (isnan(sc->divtot)) sc->status = CANSFZ_ERR_NAN;
+    else if (sc->divmax > small) sc->status = CANSFZ_ERR_DIVERGENCE;
+  }
+}
 __global__ void k_chkdiv_final(Phys ph, DevScalars* __restrict__ sc, int only_on_check, int n,
                                const double* __restrict__ part) {
   if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
   const double m = reduce_max_partials(n, part + n);
   if (threadIdx.x != 0) return;
-  sc->divmax = m;
-  // src/main.f90:552-561, after the dt checks (an earlier dt abort is kept)
-  if (only_on_check && sc->status == CANSFZ_OK) {
-    if (isnan(sc->divtot)) sc->status = CANSFZ_ERR_NAN;
-    else if (sc->divmax > ph.small) sc->status = CANSFZ_ERR_DIVERGENCE;
-  }
+  chkdiv_finish(ph.small, sc, m, only_on_check);
 }
 void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partial, const double* u,
                    const double* v, const double* w, bool only_on_check) {
@@ -948,6 +800,84 @@ void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partia
   Phys ph{};
   ph.small = CANSFZ_EPS * 1.0e7;
   k_chkdiv_final<<<1, 1024, 0, L.st>>>(ph, sc, oc, (int)(gr.x * gr.y * gr.z), partial);
+}
+
+// ---------------------------------------------------------------------------
+// End of a step: acdi_set_gamma every step and, on icheck steps, chkdt and
+// chkdiv -- one pass over u, v, w.  Blocks walk (j,k) rows with a grid
+// stride, threads the points of a row; four partials per block (|u_c|^2
+// max, dt^-1 max, divergence sum and |div| max), then one block finishes
+// gamma, the dt update and the divergence checks in the reference's order
+// (src/main.f90:530-561).  Maxima are order independent; the divergence sum
+// (used only for its NaN test) is summed in a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int kReduceThreads = 256;
+__global__ void __launch_bounds__(kReduceThreads) k_step_reduce(Geo g, DevScalars* __restrict__ sc, int acdi,
+                                                                double* __restrict__ part,
+                                                                const double* __restrict__ u,
+                                                                const double* __restrict__ v,
+                                                                const double* __restrict__ w) {
+  if (HALTED(sc)) return;
+  const bool chk = sc->check_now != 0;
+  if (!acdi && !chk) return;
+  double velmax = 0., dtimax = 0., divsum = 0., divmax = 0.;
+  const int nrows = g.ny * g.nz;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int j = r % g.ny + 1, k = r / g.ny + 1;
+    for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+      const int c = g.h(i, j, k);
+      if (acdi) {
+        const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
+        const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
+        const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
+        velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+      }
+      if (chk) {
+        dtimax = fmax(dtimax, chkdt_cell(g, i, j, k, u, v, w));
+        const double div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +
+                           (LD(u, c) - LD(u, c - 1)) * g.dxi;
+        divsum += div;
+        divmax = fmax(divmax, fabs(div));
+      }
+    }
+  }
+  velmax = block_max(velmax);
+  dtimax = block_max(dtimax);
+  divsum = block_sum(divsum);
+  divmax = block_max(divmax);
+  if (threadIdx.x == 0) {
+    const int nb = gridDim.x;
+    part[blockIdx.x] = velmax;
+    part[nb + blockIdx.x] = dtimax;
+    part[2 * nb + blockIdx.x] = divsum;
+    part[3 * nb + blockIdx.x] = divmax;
+  }
+}
+__global__ void k_step_reduce_final(Phys ph, DevScalars* __restrict__ sc, int nb, const double* __restrict__ part) {
+  if (HALTED(sc)) return;
+  const bool chk = sc->check_now != 0;
+  if (!ph.acdi && !chk) return;
+  const double velmax = reduce_max_partials(nb, part);
+  const double dtimax = reduce_max_partials(nb, part + nb);
+  double s = 0.;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) s += part[2 * nb + q];
+  s = block_sum(s);
+  const double divmax = reduce_max_partials(nb, part + 3 * nb);
+  if (threadIdx.x != 0) return;
+  if (ph.acdi) gamma_finish(ph, sc, velmax, 1);
+  if (chk) {
+    chkdt_finish(ph, sc, dtimax, 1);
+    sc->divtot = s;
+    chkdiv_finish(CANSFZ_EPS * 1.0e7, sc, divmax, 1);
+  }
+}
+void launch_step_reductions(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
+                            const double* u, const double* v, const double* w) {
+  const int nrows = g.ny * g.nz;
+  int nb = (L.nsm > 0 ? L.nsm : 148) * 8;
+  if (nb > nrows) nb = nrows;
+  k_step_reduce<<<nb, kReduceThreads, 0, L.st>>>(g, sc, ph.acdi, partial, u, v, w);
+  k_step_reduce_final<<<1, 1024, 0, L.st>>>(ph, sc, nb, partial);
 }
 
 // bulk_mean_12_stag, src/utils.f90:68-136

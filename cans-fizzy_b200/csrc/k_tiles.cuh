@@ -1,0 +1,49 @@
+// Shared pieces of the z-marching tile kernels (k_tiles.cu).
+//
+// A block owns TX x TY columns of cells and walks KZ levels in z.  The cell
+// planes it needs (with a one-cell halo in x and y) are staged in shared
+// memory through a three-slot ring filled by cp.async (8- or 4-byte
+// element copies, zero-filled outside the array), one plane ahead of the
+// level being computed.  Quantities shared by neighbouring cells (vertex
+// gradients of the Youngs normals, face fluxes of the transport) are then
+// computed once per vertex or face instead of once per cell that uses them.
+#pragma once
+
+#include "cansfz_internal.cuh"
+
+namespace cansfz {
+namespace tile {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int PX = TX + 2, PY = TY + 2, PXY = PX * PY;  // a plane of cells with a one-cell halo
+constexpr int NSLOT = 3;                                // ring of planes k-1, k, k+1 (k+2 in flight)
+
+__device__ __forceinline__ void cp_async(void* sdst, const double* gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async(void* sdst, const float* gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Position of plane-slot element q (0 <= q < PXY) in the halo layout; false
+// when the cell lies outside the array (beyond ghost nx+1 or ny+1).
+__device__ __forceinline__ bool plane_cell(const Geo& g, int i0, int j0, int kk, int q, int* h) {
+  const int a = q % PX, b = q / PX;
+  const int ii = i0 - 1 + a, jj = j0 - 1 + b;
+  *h = g.h(ii, jj, kk);
+  return ii <= g.nx + 1 && jj <= g.ny + 1;
+}
+
+inline dim3 grid_of(const Geo& g, int kz) {
+  return dim3((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + kz - 1) / kz);
+}
+
+}  // namespace tile
+}  // namespace cansfz

@@ -264,6 +264,23 @@ int cansfz_solver_refined(cansfz_ctx* ctx, const double* rhs, double* p, int swe
 /* FP64 residual res = rhs - L(p) of that operator (p's ghosts are filled). */
 int cansfz_poisson_residual(cansfz_ctx* ctx, const double* rhs, double* p, double* res);
 
+/* ---- batched ensemble (no reference counterpart: the reference runs one
+ * case per program) -----------------------------------------------------
+ * Groups independent, prepared contexts (any grid sizes and parameters, all
+ * at the same step parity, i.e. stepped the same number of times).  Each
+ * step is one CUDA graph launch holding every case's whole step as a
+ * parallel branch; the cases keep their own state and can be read back
+ * with cansfz_get_fields / cansfz_get_diag.  stream: origin stream of the
+ * graph launches (NULL: the ensemble creates one).  A case that aborts
+ * stops the ensemble (later calls return its status), as the reference
+ * program stops.                                                        */
+typedef struct cansfz_ensemble cansfz_ensemble;
+int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, cansfz_ensemble** out);
+/* status_out: NULL or ncases entries, each case's status after the steps;
+ * the return value is the first non-zero of them (CANSFZ_OK if none).   */
+int cansfz_ensemble_step(cansfz_ensemble* ens, int nsteps, int* status_out);
+int cansfz_ensemble_destroy(cansfz_ensemble* ens);
+
 /* ---- allocation-free Poisson solve (no reference counterpart) ---------
  * solver_gpu for callers that may not allocate device memory while they
  * run: the spectral work buffer and the twiddle tables are static device
