@@ -50,8 +50,8 @@ STAGE_BYTES = {
     "poisson_z_solve": 8 * 2,
     "poisson_y_bwd": 8 * 2,
     "poisson_x_bwd": 8 * 2,
-    "correc": 8 * (1 + 6),
-    "updatep": 8 * 3,
+    # correc: phi, u, v, w (r) + u, v, w (w); updatep: p (r) + p_new (w)
+    "correc_updatep": 8 * (1 + 6 + 2),
     "gamma_chkdt_chkdiv": 8 * 3,
 }
 # mixed form: state u, v, w, p, psi FP64; phi, normals, kappa, fluxes, histories
@@ -63,8 +63,8 @@ STAGE_BYTES_MIXED = {
     "momentum": 8 * 7 + 4 * 7 + 4 * 3 + 8 * 3,
     "fillps": 8 * 4,
     "poisson_f32": (8 + 4) + 4 * 2 * 3 + (4 + 8),
-    "correc": 8 * (1 + 6),
-    "updatep": 8 * 3,
+    # correc: phi, u, v, w (r) + u, v, w (w); updatep: p (r) + p_new (w)
+    "correc_updatep": 8 * (1 + 6 + 2),
     "gamma_chkdt_chkdiv": 8 * 3,
 }
 B_ALG_STEP = 232  # bytes per cell-step: 19 state accesses + 10 Poisson-pass accesses (FP64)
@@ -145,40 +145,22 @@ class Clocks:
 
 
 def dist_setup(n_gpus: int):
-    import torch
+    """One process per GPU under torchrun (cansfz/replicas.py); NCCL between GPU ranks."""
+    from cansfz import replicas
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return rank, world, local
+    return replicas.setup()
 
 
 def allreduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from cansfz import replicas
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(x, world)
 
 
 def barrier(world: int):
-    if world > 1:
-        import torch.distributed as dist
+    from cansfz import replicas
 
-        dist.barrier()
+    replicas.barrier(world)
 
 
 def cpu_run(p, fields, budget_s: float, warmup: int = 1, max_steps: int = 1000):
@@ -447,9 +429,9 @@ def gpu_arm(args):
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
-        import torch.distributed as dist
+        from cansfz import replicas
 
-        dist.destroy_process_group()
+        replicas.teardown(world)
 
 
 def reference_arm(args):

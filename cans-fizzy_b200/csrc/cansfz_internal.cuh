@@ -193,6 +193,8 @@ void launch_fillps(const Launch& L, const Geo& g, const Phys& ph, const DevScala
                    const double* u, const double* v, const double* w, double* p);
 void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
                    const double* p, double* u, double* v, double* w);
+void launch_correc_updatep(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
+                           double* u, double* v, double* w, const double* pp, double* pout);
 void launch_updatep_interior(const Launch& L, const Geo& g, const DevScalars* sc,
                              const double* phi, const double* pp, double* pout);
 void launch_updatep_full(const Launch& L, const Geo& g, const double* pp, double* p);

@@ -587,13 +587,12 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     }
     run_bcp(c, 0, c->phip, sc);
     MARK("bc_pcorr");
-    launch_correc(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b]);
-    MARK("correc");
+    // correc, and updatep (p_new = phi + p into the po slot, then po <- p by
+    // the parity flip), in one pass over phi
+    launch_correc_updatep(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b], c->p[a], c->p[b]);
+    MARK("correc_updatep");
     run_bcuvw(c, true, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw_correc");
-    // updatep: p_new = phi + p into the po slot, then po <- p by the parity flip
-    launch_updatep_interior(L, g, sc, c->phip, c->p[a], c->p[b]);
-    MARK("updatep");
     run_bcp(c, 0, c->p[b], sc);
     MARK("bc_p");
   }

@@ -473,14 +473,17 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
                               const double* __restrict__ c, T lam, T* __restrict__ col, size_t st,
                               T* __restrict__ dchk, int tpitch, bool pin) {
   typedef Rn<T> R;
-  // forward elimination
+  // forward elimination; the next chunk's loads are issued before this
+  // chunk's elimination so that their latency overlaps the pivot chain
   T dprev = 0, pprev = 0;
   const int nch = (n + ZCH - 1) / ZCH;
-  for (int ch = 0; ch < nch; ++ch) {
-    const int k0 = ch * ZCH;
-    T pv[ZCH];
+  T pv[ZCH], nx[ZCH];
 #pragma unroll
-    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : (T)0;
+  for (int q = 0; q < ZCH; ++q) pv[q] = (q < n) ? col[(size_t)q * st] : (T)0;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int k0 = ch * ZCH, k1 = k0 + ZCH;
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) nx[q] = (k1 + q < n) ? col[(size_t)(k1 + q) * st] : (T)0;
 #pragma unroll
     for (int q = 0; q < ZCH; ++q) {
       const int l = k0 + q;
@@ -497,12 +500,17 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
     for (int q = 0; q < ZCH; ++q)
       if (k0 + q < n) col[(size_t)(k0 + q) * st] = pv[q];
     dchk[ch * tpitch] = dprev;  // d at the last element of chunk ch
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) pv[q] = nx[q];
   }
-  // backward substitution, chunk by chunk from the top
+  // backward substitution, chunk by chunk from the top; the chunk's loads are
+  // issued before its pivots are recomputed from the checkpoint
   T pnext = 0;
   for (int ch = nch - 1; ch >= 0; --ch) {
     const int k0 = ch * ZCH;
-    T dd[ZCH], pv[ZCH];
+    T dd[ZCH];
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : (T)0;
     T dp = ch > 0 ? dchk[(ch - 1) * tpitch] : (T)0;
 #pragma unroll
     for (int q = 0; q < ZCH; ++q) {
@@ -512,8 +520,6 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
       dd[q] = d;
       dp = d;
     }
-#pragma unroll
-    for (int q = 0; q < ZCH; ++q) pv[q] = (k0 + q < n) ? col[(size_t)(k0 + q) * st] : (T)0;
 #pragma unroll
     for (int q = ZCH - 1; q >= 0; --q) {
       const int l = k0 + q;

@@ -530,6 +530,31 @@ void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScala
   k_correc<<<gr, b, 0, L.st>>>(g, ph, sc, p, u, v, w);
 }
 
+// correc (src/correc.f90:13-67) and updatep (src/updatep.f90:13-24) of the
+// step in one pass: both read the correction phi, and updatep needs none of
+// the velocity ghost fills that follow correc.  32x8 point tiles of the halo
+// array; pout = phi + pp on the interior (the new pressure into the po slot).
+__global__ void __launch_bounds__(256) k_correc_updatep(Geo g, Phys ph, const DevScalars* __restrict__ sc,
+                                                        const double* __restrict__ p, double* __restrict__ u,
+                                                        double* __restrict__ v, double* __restrict__ w,
+                                                        const double* __restrict__ pp, double* __restrict__ pout) {
+  if (HALTED(sc)) return;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+  if (i > g.nx + 1 || j > g.ny + 1) return;
+  const double dt = sc->dt, rhop = ph.rho0;
+  const int c = g.h(i, j, k);
+  const double pc = LD(p, c);
+  if (i <= g.nx) u[c] = u[c] - dt * g.dxi * (LD(p, c + 1) - pc) / rhop;
+  if (j <= g.ny) v[c] = v[c] - dt * g.dyi * (LD(p, c + g.sx) - pc) / rhop;
+  if (k <= g.nz) w[c] = w[c] - dt * g.dzci[k] * (LD(p, c + g.sxy) - pc) / rhop;
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz) pout[c] = pc + LD(pp, c);
+}
+void launch_correc_updatep(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
+                           double* u, double* v, double* w, const double* pp, double* pout) {
+  const dim3 b(32, 8), gr((g.nx + 2 + 31) / 32, (g.ny + 2 + 7) / 8, g.nz + 2);
+  k_correc_updatep<<<gr, b, 0, L.st>>>(g, ph, sc, p, u, v, w, pp, pout);
+}
+
 // updatep, src/updatep.f90:13-24
 __global__ void k_updatep_interior(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ phi,
                                    const double* __restrict__ pp, double* __restrict__ pout) {

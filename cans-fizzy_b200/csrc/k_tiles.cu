@@ -325,7 +325,7 @@ constexpr size_t mom_smem() {
 }  // namespace
 
 template <typename TI>
-__global__ void __launch_bounds__(tile::NT) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
+__global__ void __launch_bounds__(tile::NT, 3) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
     int kz, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const double* __restrict__ psi, const double* __restrict__ psio, const TI* __restrict__ fx,
     const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
@@ -412,106 +412,86 @@ __global__ void __launch_bounds__(tile::NT) k_momentum_tile(Geo g, Phys ph, cons
 #define PV(s, a, b) ((T)s_v[o##s + (a) + PX * (b)])
 #define PW(s, a, b) ((T)s_w[o##s + (a) + PX * (b)])
 #define PC(s, a, b) ((T)s_c[o##s + (a) + PX * (b)])
-#define PFX(s, a, b) (s_fx[o##s + (a) + PX * (b)])
-#define PFY(s, a, b) (s_fy[o##s + (a) + PX * (b)])
-#define PFZ(s, a, b) (s_fz[o##s + (a) + PX * (b)])
-      const T u_cmc = PU(0, 0, -1), u_mcc = PU(0, -1, 0), u_ccc = PU(0, 0, 0), u_pcc = PU(0, 1, 0),
-              u_mpc = PU(0, -1, 1), u_cpc = PU(0, 0, 1), u_mcp = PU(1, -1, 0), u_ccp = PU(1, 0, 0);
-      const T v_cmc = PV(0, 0, -1), v_pmc = PV(0, 1, -1), v_mcc = PV(0, -1, 0), v_ccc = PV(0, 0, 0),
-              v_pcc = PV(0, 1, 0), v_cpc = PV(0, 0, 1), v_cmp = PV(1, 0, -1), v_ccp = PV(1, 0, 0);
-      const T w_cmc = PW(0, 0, -1), w_mcc = PW(0, -1, 0), w_ccc = PW(0, 0, 0), w_pcc = PW(0, 1, 0),
-              w_cpc = PW(0, 0, 1), w_ccp = PW(1, 0, 0);
-      const T c_cmc = PC(0, 0, -1), c_pmc = PC(0, 1, -1), c_mcc = PC(0, -1, 0), c_ccc = PC(0, 0, 0),
-              c_pcc = PC(0, 1, 0), c_mpc = PC(0, -1, 1), c_cpc = PC(0, 0, 1), c_ppc = PC(0, 1, 1),
-              c_cmp = PC(1, 0, -1), c_mcp = PC(1, -1, 0), c_ccp = PC(1, 0, 0), c_cpp = PC(1, 0, 1),
-              c_pcp = PC(1, 1, 0);
-      const T flx_x_mcc = rho * u_mcc + drho * PFX(0, -1, 0);
-      const T flx_x_ccc = rho * u_ccc + drho * PFX(0, 0, 0);
-      const T flx_x_pcc = rho * u_pcc + drho * PFX(0, 1, 0);
-      const T flx_x_mpc = rho * u_mpc + drho * PFX(0, -1, 1);
-      const T flx_x_cpc = rho * u_cpc + drho * PFX(0, 0, 1);
-      const T flx_x_mcp = rho * u_mcp + drho * PFX(1, -1, 0);
-      const T flx_x_ccp = rho * u_ccp + drho * PFX(1, 0, 0);
-      const T flx_y_cmc = rho * v_cmc + drho * PFY(0, 0, -1);
-      const T flx_y_ccc = rho * v_ccc + drho * PFY(0, 0, 0);
-      const T flx_y_cpc = rho * v_cpc + drho * PFY(0, 0, 1);
-      const T flx_y_pmc = rho * v_pmc + drho * PFY(0, 1, -1);
-      const T flx_y_pcc = rho * v_pcc + drho * PFY(0, 1, 0);
-      const T flx_y_cmp = rho * v_cmp + drho * PFY(1, 0, -1);
-      const T flx_y_ccp = rho * v_ccp + drho * PFY(1, 0, 0);
-      const T flx_z_ccc = rho * w_ccc + drho * PFZ(0, 0, 0);
-      const T flx_z_ccp = rho * w_ccp + drho * PFZ(1, 0, 0);
-      const T flx_z_pcc = rho * w_pcc + drho * PFZ(0, 1, 0);
-      const T flx_z_cpc = rho * w_cpc + drho * PFZ(0, 0, 1);
-#undef PU
-#undef PV
-#undef PW
-#undef PC
-#undef PFX
-#undef PFY
-#undef PFZ
+#define FLX(s, a, b) (rho * PU(s, a, b) + drho * s_fx[o##s + (a) + PX * (b)])
+#define FLY(s, a, b) (rho * PV(s, a, b) + drho * s_fy[o##s + (a) + PX * (b)])
+#define FLZ(s, a, b) (rho * PW(s, a, b) + drho * s_fz[o##s + (a) + PX * (b)])
       const T dzci_c = (T)g.dzci[k], dzci_m = (T)g.dzci[k - 1], dzfi_c = (T)g.dzfi[k], dzfi_p = (T)g.dzfi[k + 1];
-      const T uuip = T(0.25) * (flx_x_pcc + flx_x_ccc) * (u_ccc + u_pcc);
-      const T uuim = T(0.25) * (flx_x_mcc + flx_x_ccc) * (u_ccc + u_mcc);
-      const T vujp = T(0.25) * (flx_y_pcc + flx_y_ccc) * (u_ccc + u_cpc);
-      const T vujm = T(0.25) * (flx_y_pmc + flx_y_cmc) * (u_ccc + u_cmc);
-      const T wukp = T(0.25) * (flx_z_pcc + flx_z_ccc) * (u_ccc + u_ccp);
-      const T wukm = T(0.25) * (flx_z_pcm + flx_z_ccm) * (u_ccc + u_ccm);
-      T dudt_aux = dxi * (-uuip + uuim) + dyi * (-vujp + vujm) + dzfi_c * (-wukp + wukm);
-      const T uvip = T(0.25) * (flx_x_ccc + flx_x_cpc) * (v_ccc + v_pcc);
-      const T uvim = T(0.25) * (flx_x_mcc + flx_x_mpc) * (v_ccc + v_mcc);
-      const T vvjp = T(0.25) * (flx_y_ccc + flx_y_cpc) * (v_ccc + v_cpc);
-      const T vvjm = T(0.25) * (flx_y_ccc + flx_y_cmc) * (v_ccc + v_cmc);
-      const T wvkp = T(0.25) * (flx_z_ccc + flx_z_cpc) * (v_ccc + v_ccp);
-      const T wvkm = T(0.25) * (flx_z_ccm + flx_z_cpm) * (v_ccc + v_ccm);
-      T dvdt_aux = dxi * (-uvip + uvim) + dyi * (-vvjp + vvjm) + dzfi_c * (-wvkp + wvkm);
-      const T uwip = T(0.25) * (flx_x_ccc + flx_x_ccp) * (w_ccc + w_pcc);
-      const T uwim = T(0.25) * (flx_x_mcc + flx_x_mcp) * (w_ccc + w_mcc);
-      const T vwjp = T(0.25) * (flx_y_ccc + flx_y_ccp) * (w_ccc + w_cpc);
-      const T vwjm = T(0.25) * (flx_y_cmc + flx_y_cmp) * (w_ccc + w_cmc);
-      const T wwkp = T(0.25) * (flx_z_ccc + flx_z_ccp) * (w_ccc + w_ccp);
-      const T wwkm = T(0.25) * (flx_z_ccc + flx_z_ccm) * (w_ccc + w_ccm);
-      T dwdt_aux = dxi * (-uwip + uwim) + dyi * (-vwjp + vwjm) + dzci_c * (-wwkp + wwkm);
+      // the three components one after another, each reading its stencil
+      // from shared memory, so that few values are live at a time
+      T dudt_aux, dvdt_aux, dwdt_aux;
       {
+        const T u_ccc = PU(0, 0, 0), u_pcc = PU(0, 1, 0), u_mcc = PU(0, -1, 0), u_cpc = PU(0, 0, 1),
+                u_cmc = PU(0, 0, -1), u_ccp = PU(1, 0, 0);
+        const T flx_x_ccc = FLX(0, 0, 0);
+        const T uuip = T(0.25) * (FLX(0, 1, 0) + flx_x_ccc) * (u_ccc + u_pcc);
+        const T uuim = T(0.25) * (FLX(0, -1, 0) + flx_x_ccc) * (u_ccc + u_mcc);
+        const T vujp = T(0.25) * (FLY(0, 1, 0) + FLY(0, 0, 0)) * (u_ccc + u_cpc);
+        const T vujm = T(0.25) * (FLY(0, 1, -1) + FLY(0, 0, -1)) * (u_ccc + u_cmc);
+        const T wukp = T(0.25) * (FLZ(0, 1, 0) + FLZ(0, 0, 0)) * (u_ccc + u_ccp);
+        const T wukm = T(0.25) * (flx_z_pcm + flx_z_ccm) * (u_ccc + u_ccm);
+        dudt_aux = dxi * (-uuip + uuim) + dyi * (-vujp + vujm) + dzfi_c * (-wukp + wukm);
+        const T c_ccc = PC(0, 0, 0), c_pcc = PC(0, 1, 0);
         const T dudxp = (u_pcc - u_ccc) * dxi, dudxm = (u_ccc - u_mcc) * dxi;
-        const T dvdxp = (v_pcc - v_ccc) * dxi, dvdxm = (v_pmc - v_cmc) * dxi;
+        const T dvdxp = (PV(0, 1, 0) - PV(0, 0, 0)) * dxi, dvdxm = (PV(0, 1, -1) - PV(0, 0, -1)) * dxi;
         const T dudyp = (u_cpc - u_ccc) * dyi, dudym = (u_ccc - u_cmc) * dyi;
         const T dudzp = (u_ccp - u_ccc) * dzci_c, dudzm = (u_ccc - u_ccm) * dzci_m;
-        const T dwdxp = (w_pcc - w_ccc) * dxi, dwdxm = (w_pcm - w_ccm) * dxi;
+        const T dwdxp = (PW(0, 1, 0) - PW(0, 0, 0)) * dxi, dwdxm = (w_pcm - w_ccm) * dxi;
         const T muxp = mu + dmu * c_pcc, muxm = mu + dmu * c_ccc;
-        const T muyp = mu + dmu * T(0.25) * (c_ccc + c_cpc + c_ppc + c_pcc);
-        const T muym = mu + dmu * T(0.25) * (c_ccc + c_cmc + c_pmc + c_pcc);
-        const T muzp = mu + dmu * T(0.25) * (c_ccc + c_pcc + c_ccp + c_pcp);
+        const T muyp = mu + dmu * T(0.25) * (c_ccc + PC(0, 0, 1) + PC(0, 1, 1) + c_pcc);
+        const T muym = mu + dmu * T(0.25) * (c_ccc + PC(0, 0, -1) + PC(0, 1, -1) + c_pcc);
+        const T muzp = mu + dmu * T(0.25) * (c_ccc + c_pcc + PC(1, 0, 0) + PC(1, 1, 0));
         const T muzm = mu + dmu * T(0.25) * (c_ccc + c_pcc + c_ccm + c_pcm);
         dudt_aux = dudt_aux + dxi * ((dudxp + dudxp) * muxp - (dudxm + dudxm) * muxm) +
                    dyi * ((dudyp + dvdxp) * muyp - (dudym + dvdxm) * muym) +
                    dzfi_c * ((dudzp + dwdxp) * muzp - (dudzm + dwdxm) * muzm);
       }
       {
+        const T v_ccc = PV(0, 0, 0), v_pcc = PV(0, 1, 0), v_mcc = PV(0, -1, 0), v_cpc = PV(0, 0, 1),
+                v_cmc = PV(0, 0, -1), v_ccp = PV(1, 0, 0);
+        const T flx_y_ccc = FLY(0, 0, 0);
+        const T uvip = T(0.25) * (FLX(0, 0, 0) + FLX(0, 0, 1)) * (v_ccc + v_pcc);
+        const T uvim = T(0.25) * (FLX(0, -1, 0) + FLX(0, -1, 1)) * (v_ccc + v_mcc);
+        const T vvjp = T(0.25) * (flx_y_ccc + FLY(0, 0, 1)) * (v_ccc + v_cpc);
+        const T vvjm = T(0.25) * (flx_y_ccc + FLY(0, 0, -1)) * (v_ccc + v_cmc);
+        const T wvkp = T(0.25) * (FLZ(0, 0, 0) + FLZ(0, 0, 1)) * (v_ccc + v_ccp);
+        const T wvkm = T(0.25) * (flx_z_ccm + flx_z_cpm) * (v_ccc + v_ccm);
+        dvdt_aux = dxi * (-uvip + uvim) + dyi * (-vvjp + vvjm) + dzfi_c * (-wvkp + wvkm);
+        const T c_ccc = PC(0, 0, 0), c_cpc = PC(0, 0, 1);
         const T dvdxp = (v_pcc - v_ccc) * dxi, dvdxm = (v_ccc - v_mcc) * dxi;
-        const T dudyp = (u_cpc - u_ccc) * dyi, dudym = (u_mpc - u_mcc) * dyi;
+        const T dudyp = (PU(0, 0, 1) - PU(0, 0, 0)) * dyi, dudym = (PU(0, -1, 1) - PU(0, -1, 0)) * dyi;
         const T dvdyp = (v_cpc - v_ccc) * dyi, dvdym = (v_ccc - v_cmc) * dyi;
         const T dvdzp = (v_ccp - v_ccc) * dzci_c, dvdzm = (v_ccc - v_ccm) * dzci_m;
-        const T dwdyp = (w_cpc - w_ccc) * dyi, dwdym = (w_cpm - w_ccm) * dyi;
-        const T muxp = mu + dmu * T(0.25) * (c_ccc + c_pcc + c_ppc + c_cpc);
-        const T muxm = mu + dmu * T(0.25) * (c_ccc + c_mcc + c_mpc + c_cpc);
+        const T dwdyp = (PW(0, 0, 1) - PW(0, 0, 0)) * dyi, dwdym = (w_cpm - w_ccm) * dyi;
+        const T muxp = mu + dmu * T(0.25) * (c_ccc + PC(0, 1, 0) + PC(0, 1, 1) + c_cpc);
+        const T muxm = mu + dmu * T(0.25) * (c_ccc + PC(0, -1, 0) + PC(0, -1, 1) + c_cpc);
         const T muyp = mu + dmu * c_cpc, muym = mu + dmu * c_ccc;
-        const T muzp = mu + dmu * T(0.25) * (c_ccc + c_cpc + c_cpp + c_ccp);
+        const T muzp = mu + dmu * T(0.25) * (c_ccc + c_cpc + PC(1, 0, 1) + PC(1, 0, 0));
         const T muzm = mu + dmu * T(0.25) * (c_ccc + c_cpc + c_cpm + c_ccm);
         dvdt_aux = dvdt_aux + dxi * ((dvdxp + dudyp) * muxp - (dvdxm + dudym) * muxm) +
                    dyi * ((dvdyp + dvdyp) * muyp - (dvdym + dvdym) * muym) +
                    dzfi_c * ((dvdzp + dwdyp) * muzp - (dvdzm + dwdym) * muzm);
       }
       {
+        const T w_ccc = PW(0, 0, 0), w_pcc = PW(0, 1, 0), w_mcc = PW(0, -1, 0), w_cpc = PW(0, 0, 1),
+                w_cmc = PW(0, 0, -1), w_ccp = PW(1, 0, 0);
+        const T flx_z_ccc = FLZ(0, 0, 0);
+        const T uwip = T(0.25) * (FLX(0, 0, 0) + FLX(1, 0, 0)) * (w_ccc + w_pcc);
+        const T uwim = T(0.25) * (FLX(0, -1, 0) + FLX(1, -1, 0)) * (w_ccc + w_mcc);
+        const T vwjp = T(0.25) * (FLY(0, 0, 0) + FLY(1, 0, 0)) * (w_ccc + w_cpc);
+        const T vwjm = T(0.25) * (FLY(0, 0, -1) + FLY(1, 0, -1)) * (w_ccc + w_cmc);
+        const T wwkp = T(0.25) * (flx_z_ccc + FLZ(1, 0, 0)) * (w_ccc + w_ccp);
+        const T wwkm = T(0.25) * (flx_z_ccc + flx_z_ccm) * (w_ccc + w_ccm);
+        dwdt_aux = dxi * (-uwip + uwim) + dyi * (-vwjp + vwjm) + dzci_c * (-wwkp + wwkm);
+        const T c_ccc = PC(0, 0, 0), c_ccp = PC(1, 0, 0);
         const T dwdxp = (w_pcc - w_ccc) * dxi, dwdxm = (w_ccc - w_mcc) * dxi;
-        const T dudzp = (u_ccp - u_ccc) * dzci_c, dudzm = (u_mcp - u_mcc) * dzci_c;
+        const T dudzp = (PU(1, 0, 0) - PU(0, 0, 0)) * dzci_c, dudzm = (PU(1, -1, 0) - PU(0, -1, 0)) * dzci_c;
         const T dwdyp = (w_cpc - w_ccc) * dyi, dwdym = (w_ccc - w_cmc) * dyi;
-        const T dvdzp = (v_ccp - v_ccc) * dzci_c, dvdzm = (v_cmp - v_cmc) * dzci_c;
+        const T dvdzp = (PV(1, 0, 0) - PV(0, 0, 0)) * dzci_c, dvdzm = (PV(1, 0, -1) - PV(0, 0, -1)) * dzci_c;
         const T dwdzp = (w_ccp - w_ccc) * dzfi_p, dwdzm = (w_ccc - w_ccm) * dzfi_c;
-        const T muxp = mu + dmu * T(0.25) * (c_ccc + c_pcc + c_ccp + c_pcp);
-        const T muxm = mu + dmu * T(0.25) * (c_ccc + c_mcc + c_ccp + c_mcp);
-        const T muyp = mu + dmu * T(0.25) * (c_ccc + c_cpc + c_ccp + c_cpp);
-        const T muym = mu + dmu * T(0.25) * (c_ccc + c_cmc + c_ccp + c_cmp);
+        const T muxp = mu + dmu * T(0.25) * (c_ccc + PC(0, 1, 0) + c_ccp + PC(1, 1, 0));
+        const T muxm = mu + dmu * T(0.25) * (c_ccc + PC(0, -1, 0) + c_ccp + PC(1, -1, 0));
+        const T muyp = mu + dmu * T(0.25) * (c_ccc + PC(0, 0, 1) + c_ccp + PC(1, 0, 1));
+        const T muym = mu + dmu * T(0.25) * (c_ccc + PC(0, 0, -1) + c_ccp + PC(1, 0, -1));
         const T muzp = mu + dmu * c_ccp, muzm = mu + dmu * c_ccc;
         dwdt_aux = dwdt_aux + dxi * ((dwdxp + dudzp) * muxp - (dwdxm + dudzm) * muxm) +
                    dyi * ((dwdyp + dvdzp) * muyp - (dwdym + dvdzm) * muym) +
@@ -572,9 +552,16 @@ __global__ void __launch_bounds__(tile::NT) k_momentum_tile(Geo g, Phys ph, cons
       vo[c] = vn + f12 * sdv * iry;
       wo[c] = wn + f12 * sdw * irz;
       // carry upwards
-      u_ccm = u_ccc; v_ccm = v_ccc; w_ccm = w_ccc; w_pcm = w_pcc; w_cpm = w_cpc;
-      c_ccm = c_ccc; c_pcm = c_pcc; c_cpm = c_cpc;
-      flx_z_ccm = flx_z_ccc; flx_z_pcm = flx_z_pcc; flx_z_cpm = flx_z_cpc;
+      u_ccm = PU(0, 0, 0); v_ccm = PV(0, 0, 0); w_ccm = PW(0, 0, 0); w_pcm = PW(0, 1, 0); w_cpm = PW(0, 0, 1);
+      c_ccm = PC(0, 0, 0); c_pcm = PC(0, 1, 0); c_cpm = PC(0, 0, 1);
+      flx_z_ccm = FLZ(0, 0, 0); flx_z_pcm = FLZ(0, 1, 0); flx_z_cpm = FLZ(0, 0, 1);
+#undef PU
+#undef PV
+#undef PW
+#undef PC
+#undef FLX
+#undef FLY
+#undef FLZ
       p_c = p_z; po_c = po_z; pso_c = pso_z; k_c = k_z;
     }
     __syncthreads();  // plane k's slot is refilled at the next level

@@ -239,14 +239,37 @@ def _check_step(g, o, tol=1e-11):
     return errs
 
 
+def _oracle_sensitivity(p, u, v, w, pr, psi, nsteps, names=("u", "v", "w")):
+    """The reference algorithm's own round-off sensitivity: the oracle rerun
+    with psi scaled by (1 - 1e-15); the largest relative change of a field."""
+    runs = []
+    for scale in (1.0, 1.0 - 1e-15):
+        o = O.Case(p)
+        for name, a in zip(("u", "v", "w", "p", "psi"), (u, v, w, pr, psi * scale)):
+            o.set(name, a)
+        o.prepare()
+        assert o.step(nsteps) == 0
+        runs.append({n: o.get(n) for n in names})
+    return max(_rel(runs[1][n], runs[0][n]) for n in names)
+
+
 def test_step_bubble_3d():
-    """10 steps of a 3-D rising bubble (periodic x,y; walls z)."""
+    """10 steps of a 3-D rising bubble (periodic x,y; walls z).
+
+    The velocity here is a small residual of the hydrostatic balance, and the
+    all-Neumann pressure's singular mode carries the constant that the
+    reference's eps-shifted pivot makes of round-off (~5e6 in this case),
+    whose rounding limits the pressure gradients.  The bar is therefore 1e-11
+    or four times the reference algorithm's own change under a 1e-15
+    perturbation of the input, whichever is larger (that change is ~1.3e-11
+    here)."""
     p = _nml(32, 32, 48, "PPPPNN", l=(1.0, 1.0, 1.5))
     psi = init.init2fl(p, "bub3", np.array([[0.5, 0.5, 0.5, 0.25]]))
     u, v, w, pr = init.initflow(p, "zer")
     g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
     assert rg == 0 and ro == 0
-    _check_step(g, o)
+    sens = _oracle_sensitivity(p, u, v, w, pr, psi, 10)
+    _check_step(g, o, tol=max(1e-11, 4.0 * sens))
 
 
 def test_step_moving_droplets_divfree():
