@@ -33,8 +33,18 @@ WORKLOAD = ("droplets_acdi: 256^3 cells, unit box, periodic x,y, no-slip z walls
             "u0 (|k|<=4, rms 0.1); AB2 step with FFT Poisson solve")
 DATA = "synthetic (seeded generator, numpy default_rng(2026)); no dataset"
 
-# Algorithmic bytes per cell of each stage of the FP64 step (8 B per access of
-# the persistent state a stage must read or write once; neighbours reused).
+# The other configurations of the benchmark matrix (--config); the default,
+# c3a, is the metric's own configuration above.
+CONFIGS = {
+    "c1": ("rising_bubble_3d", "rising bubble 64x64x128, domain 1x1x2, periodic x,y, no-slip z walls, bubble D 0.5, "
+                               "rho 1000/100, mu 10/1, sigma 24.5, g 0.98, ACDI, fluid at rest"),
+    "c3b": ("droplets_thinc", "droplets_thinc: 512x512x256 cells, box 2x2x1, 64 droplets R~U[0.03,0.06], rho 1000/1, "
+                              "mu 100/1, sigma 1, g 1, THINC/QQ (beta 1), random divergence-free u0"),
+    "c5": ("shear_stretched", "shear_stretched: 512x256x256, tanh-stretched z (gr 1.5), Poiseuille mean 1 driven by "
+                              "the laminar pressure gradient, 1% perturbation, 200 droplets R~U[0.04,0.08], "
+                              "rho 10/1, mu 1/1, sigma 0.5, ACDI"),
+}
+
 # Algorithmic bytes per cell of each profiled stage (one read of every input
 # point, one write of every output point; halo and neighbour re-reads are
 # not counted).  FP64 drop-in:
@@ -82,6 +92,8 @@ def parse_args():
     ap.add_argument("--grid", type=int, default=256, help="cube size of the droplet workload (profiling runs)")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--sweeps", type=int, default=2, help="refinement sweeps of the mixed form")
+    ap.add_argument("--config", default="c3a", choices=["c3a", "c1", "c3b", "c5", "c2"],
+                    help="benchmark-matrix configuration (c3a: the metric's 256^3 ACDI case; c2: Poisson only)")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps per case of the batched-ensemble measurement (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=50,
@@ -299,10 +311,15 @@ def gpu_arm(args):
     from cansfz import workloads as W
 
     rank, world, local = dist_setup(args.gpus)
-    if args.grid == 256:
+    workload = WORKLOAD
+    if args.config in CONFIGS:
+        builder, workload = CONFIGS[args.config]
+        p, fields = W.BUILDERS[builder]()
+    elif args.grid == 256:
         p, fields = W.droplets_acdi(seed=2026)
     else:
         p, fields = W.droplets((args.grid,) * 3, (1.0, 1.0, 1.0), False, seed=2026)
+        workload = f"droplets_acdi at {args.grid}^3 (profiling size)"
     if args.form == "mixed":
         p.form = 1
         p.refine_sweeps = args.sweeps
@@ -367,12 +384,14 @@ def gpu_arm(args):
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64 state / f32 stencils+transforms",
         "data": DATA,
-        "config": {"workload": WORKLOAD if args.grid == 256 else f"droplets_acdi at {args.grid}^3 (profiling size)",
+        "config": {"workload": workload, "config": args.config,
                    "grid": [nx, ny, nz],
                    "form": "fp64 (drop-in)" if args.form == "fp64" else
                            f"mixed (FP32 stencils and transforms, FP64 state, {args.sweeps} refinement sweeps)",
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (each FP64 field 137 MB > 126 MB)",
+                   "l2": (f"inputs larger than L2 (each FP64 field {8 * (nx + 2) * (ny + 2) * (nz + 2) / 1e6:.0f} MB"
+                          f"{' > ' if 8 * (nx + 2) * (ny + 2) * (nz + 2) > 126e6 else ' < '}126 MB; "
+                          f"{28 if args.form == 'fp64' else 20} fields resident, far above L2)"),
                    "final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -384,7 +403,7 @@ def gpu_arm(args):
         "clocks": clocks,
     }
     # ---- batched ensemble of independent small cases
-    if world == 1 and args.ensemble_steps > 0:
+    if world == 1 and args.ensemble_steps > 0 and args.config == "c3a":
         out["ensemble"] = ensemble_bench(args.ensemble_steps, 3, 0 if args.form == "fp64" else 1)
     # ---- mixed form: error against the FP64 form after the same steps from the same state
     if args.form == "mixed" and args.accuracy_steps > 0:
@@ -423,7 +442,7 @@ def gpu_arm(args):
     if world == 1 and not args.no_cpu_baseline:
         v, n, thr, dt = cpu_run(p, fields, budget_s=15.0, warmup=1, max_steps=20)
         out["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": thr, "kind": "port",
-                               "sample": f"{n} steps of the same 256^3 workload after 1 warm-up step "
+                               "sample": f"{n} steps of the same {nx}x{ny}x{nz} workload after 1 warm-up step "
                                          f"({dt:.1f} s), oracle/ C++ OpenMP restatement"}
     case.close()
     if rank == 0:
@@ -455,10 +474,71 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def poisson_arm(args):
+    """Configuration c2: the pressure solve alone at 256^3 (PPPPNN, RHS ~ N(0,1)
+    with the mean removed): the FP64 solve and the FP32 solve with 0-3 FP64
+    residual refinement sweeps; solves/s (device time of K solves, CUDA
+    events) and, per sweep count, the 7-point residual (L2, Linf, relative to
+    the RHS) and the error against the FP64 solution (mean removed)."""
+    import numpy as np
+    import torch
+
+    from cansfz import case as C
+    from cansfz import workloads as W
+
+    dist_setup(1)
+    p, rhs = W.poisson_rhs(256, 2026)
+    g = C.Case(p)
+    src = g.field(rhs)
+    k = max(args.steps // 10, 3)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(g.stream)
+        for _ in range(k):
+            fn()
+        e1.record(g.stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    ref = g.field(rhs)
+    g.call("solver", ref)
+    a64 = ref.get()[1:-1, 1:-1, 1:-1]
+    a64 = a64 - a64.mean()
+    work = g.field(rhs)
+    ms64 = timed(lambda: g.call("solver", work))
+    r = g.field()
+    out = g.field()
+    rin = rhs[1:-1, 1:-1, 1:-1]
+    res = {}
+    for sw in range(4):
+        ms = timed(lambda: g.call("solver_refined", src, out, sw))
+        b = out.get()[1:-1, 1:-1, 1:-1]
+        b = b - b.mean()
+        g.call("poisson_residual", src, out, r)
+        rr = r.get()[1:-1, 1:-1, 1:-1]
+        res[str(sw)] = {"ms_per_solve": ms, "solves_per_s": 1e3 / ms,
+                        "residual_l2_rel": float(np.linalg.norm(rr) / np.linalg.norm(rin)),
+                        "residual_linf_rel": float(np.abs(rr).max() / np.abs(rin).max()),
+                        "err_vs_fp64_rel": float(np.abs(b - a64).max() / np.abs(a64).max())}
+    print(json.dumps({"metric": "Poisson solves/s at 256^3 (PPPPNN)", "value": 1e3 / ms64, "unit": "solves/s",
+                      "n_gpus": 1, "steps": k, "warmup": 2, "ms_per_step": ms64, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+                      "config": {"workload": "poisson_256: 256^3 uniform, periodic x,y, Neumann z, RHS ~ N(0,1) "
+                                             "(seed 2026), mean removed", "config": "c2"},
+                      "fp32_refined": res}), flush=True)
+    g.close()
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.config == "c2":
+        poisson_arm(args)
     else:
         gpu_arm(args)
 
