@@ -82,22 +82,32 @@ template <typename T> __device__ __forceinline__ void str(const Bufs<T>& B, int 
 
 // complex FFT (sign -1 forward, +1 backward) of length pl.m on L lines held
 // in buffer `in`; returns the buffer index holding the result.
-// MC > 0: the complex length is the compile-time power of two MC (radix-4
-// stages, then one radix-2 stage when log2(MC) is odd -- the plan the host
-// derives for such lengths) and LC the compile-time lines per CTA, so every
-// index division below folds into shifts and masks.
-template <int MC>
-struct Pow2Plan {
-  static constexpr int lg = MC <= 1 ? 0 : 1 + Pow2Plan<(MC >> 1)>::lg;
-  static constexpr int n4 = lg / 2;
-  static constexpr int nst = n4 + (lg & 1);
-  static __device__ __forceinline__ constexpr int radix(int st) { return st < n4 ? 4 : 2; }
-};
-template <>
-struct Pow2Plan<0> {
-  static constexpr int lg = 0, n4 = 0, nst = 0;
-  static __device__ __forceinline__ constexpr int radix(int) { return 1; }
-};
+// MC > 0: the complex length is the compile-time constant MC and LC the
+// compile-time lines per CTA; the radix plan is the host's (radix 4 while
+// the rest is a multiple of 4 above 4, then 4, 2, 3, 5, 7 in turn), so every
+// stage's radix, length and stride -- and with them every index division
+// below -- fold into constants.
+__host__ __device__ constexpr int plan_radix(int m, int st) {
+  int k = 0;
+  while (m % 4 == 0 && m > 4) {
+    if (k == st) return 4;
+    m /= 4;
+    ++k;
+  }
+  const int rs[5] = {4, 2, 3, 5, 7};
+  for (int q = 0; q < 5; ++q)
+    while (m % rs[q] == 0) {
+      if (k == st) return rs[q];
+      m /= rs[q];
+      ++k;
+    }
+  return 1;
+}
+__host__ __device__ constexpr int plan_nst(int m) {
+  int k = 0;
+  while (plan_radix(m, k) > 1) ++k;
+  return k;
+}
 
 // one Stockham stage of radix r on L lines: buffer cur -> cur^1
 template <typename T>
@@ -157,21 +167,23 @@ __device__ __forceinline__ void fft_stage(const LinePlan& pl, const Bufs<T>& B, 
     }
 }
 
+template <typename T, int MC, int ST, int NST, int LEN, int S>
+__device__ __forceinline__ void fft_stages_c(const LinePlan& pl, const Bufs<T>& B, int& cur, int L, int sign) {
+  if constexpr (ST < NST) {
+    constexpr int r = plan_radix(MC, ST);
+    fft_stage<T>(pl, B, cur, L, sign, MC, r, LEN, S);
+    __syncthreads();
+    cur ^= 1;
+    fft_stages_c<T, MC, ST + 1, NST, LEN / r, S * r>(pl, B, cur, L, sign);
+  }
+}
+
 template <typename T, int MC, int LC>
 __device__ int fft_lines(const LinePlan& pl, const Bufs<T>& B, int in, int Lrt, int sign) {
   const int L = LC ? LC : Lrt;
   int cur = in;
   if constexpr (MC > 0) {
-    int len = MC, s = 1;
-#pragma unroll
-    for (int st = 0; st < Pow2Plan<MC>::nst; ++st) {
-      const int r = Pow2Plan<MC>::radix(st);
-      fft_stage<T>(pl, B, cur, L, sign, MC, r, len, s);
-      __syncthreads();
-      cur ^= 1;
-      len /= r;
-      s *= r;
-    }
+    fft_stages_c<T, MC, 0, plan_nst(MC), MC, 1>(pl, B, cur, L, sign);
   } else {
     const int m = pl.m;
     int len = m, s = 1;
@@ -616,9 +628,9 @@ constexpr int xL() { return MC ? lines_per_cta(MC, x_maxL(MC), sizeof(T)) : 0; }
 template <typename T, int MC>
 constexpr int yL() { return MC ? lines_per_cta(MC, y_maxL(), sizeof(T)) : 0; }
 
-// the compile-time complex lengths (real lines of 64, 128, 256 and 512
-// points); other lengths take the runtime-length kernels
-#define CANSFZ_FOR_LENGTHS(X) X(32) X(64) X(128) X(256)
+// the compile-time complex lengths (real lines of 32 to 512 points with
+// factors 2 and 3); other lengths take the runtime-length kernels
+#define CANSFZ_FOR_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256)
 
 template <typename T, int MC>
 static void set_attr_len() {
