@@ -17,9 +17,10 @@
 // the same four terms in another order).
 //
 // ACDI: each face flux (advective part and regularisation part) is shared by
-// the two cells on either side.  The x- and y-faces of a level are computed
-// once into shared memory, the z-face k+1/2 of a column is carried in
-// registers to the next level as its k-1/2 face.  Every face expression is
+// the two cells on either side.  Each thread evaluates its cell's +x, +y and
+// +z faces together (x and y into shared memory, the z face carried in
+// registers to the next level as its k-1/2 face); 40 threads add the tile's
+// -x and -y boundary faces.  Every face expression is
 // the reference's with the two cells' roles swapped only inside sums and
 // products of two terms, so the results are bitwise those of the per-cell
 // form.
@@ -258,23 +259,37 @@ __global__ void __launch_bounds__(tile::NT) k_acdi_tile(Geo g, const DevScalars*
     cp_wait<1>();
     __syncthreads();  // plane k+1 is in; every thread is done with level k-1
     const int s0 = k % NSLOT, s1 = (k + 1) % NSLOT;
-    for (int f = tid; f < NF; f += NT) {
-      if (f < NFX) {  // x-face between plane cells (a, b+1) and (a+1, b+1)
-        const int a = f % (TX + 1), b = f / (TX + 1);
-        if (j0 + b <= g.ny && i0 + a <= g.nx + 1) {
-          const int q = a + PX * (b + 1);
-          face(0, dxi, s0, q, s0, q + 1, (T)__ldg(u + g.h(i0 - 1 + a, j0 + b, k)), &f_up[f], &f_rg[f]);
-        }
-      } else {  // y-face between plane cells (a+1, b) and (a+1, b+1)
-        const int e = f - NFX, a = e % TX, b = e / TX;
-        if (i0 + a <= g.nx && j0 + b <= g.ny + 1) {
-          const int q = (a + 1) + PX * b;
-          face(1, dyi, s0, q, s0, q + PX, (T)__ldg(v + g.h(i0 + a, j0 - 1 + b, k)), &f_up[f], &f_rg[f]);
-        }
+    T up_zp = T(0), rg_zp = T(0);
+    if (act) {
+      // the cell's own +x, +y and +z faces: three independent evaluations in
+      // one block of code, so that their dependency chains overlap
+      const int c = g.h(i, j, k);
+      const T vx = (T)__ldg(u + c), vy = (T)__ldg(v + c), vz = (T)__ldg(w + c);
+      T upx, rgx, upy, rgy;
+      face(0, dxi, s0, qc, s0, qc + 1, vx, &upx, &rgx);
+      face(1, dyi, s0, qc, s0, qc + PX, vy, &upy, &rgy);
+      face(2, (T)g.dzci[k], s0, qc, s1, qc, vz, &up_zp, &rg_zp);
+      const int fxp = ty * (TX + 1) + tx + 1, fyp = NFX + (ty + 1) * TX + tx;
+      f_up[fxp] = upx;
+      f_rg[fxp] = rgx;
+      f_up[fyp] = upy;
+      f_rg[fyp] = rgy;
+    }
+    // the tile's -x faces (x-face 0 of each row) and -y faces (y-face 0 of
+    // each column), one thread each
+    if (tid < TY) {
+      const int b = tid;
+      if (j0 + b <= g.ny) {
+        const int q = PX * (b + 1), f = b * (TX + 1);
+        face(0, dxi, s0, q, s0, q + 1, (T)__ldg(u + g.h(i0 - 1, j0 + b, k)), &f_up[f], &f_rg[f]);
+      }
+    } else if (tid < TY + TX) {
+      const int a = tid - TY;
+      if (i0 + a <= g.nx) {
+        const int q = a + 1, f = NFX + a;
+        face(1, dyi, s0, q, s0, q + PX, (T)__ldg(v + g.h(i0 + a, j0 - 1, k)), &f_up[f], &f_rg[f]);
       }
     }
-    T up_zp = T(0), rg_zp = T(0);
-    if (act) face(2, (T)g.dzci[k], s0, qc, s1, qc, (T)__ldg(w + g.h(i, j, k)), &up_zp, &rg_zp);
     const double psi_c = s_psi[s0 * PXY + qc];  // read before the barrier: the slot is refilled next level
     __syncthreads();
     if (act) {
