@@ -35,11 +35,13 @@ namespace {
 template <typename T>
 __device__ __forceinline__ T sqr(T x) { return x * x; }
 
+template <int TYV>
 int tile_kz(const Geo& g) {
+  using S = tile::Shape<TYV>;
   // about six waves of four resident blocks on each of 148 SMs, so the last
   // partial wave costs little; at least 8 levels per block (each block loads
   // two planes and evaluates one face/vertex plane beyond its own levels)
-  const long long xy = (long long)((g.nx + tile::TX - 1) / tile::TX) * ((g.ny + tile::TY - 1) / tile::TY);
+  const long long xy = (long long)((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
   long long kz = (xy * g.nz) / (148LL * 24);
   if (kz < 8) kz = 8;
   if (kz > 64) kz = 64;
@@ -51,12 +53,15 @@ int tile_kz(const Geo& g) {
 // ---------------------------------------------------------------------------
 // Youngs normals and curvature
 // ---------------------------------------------------------------------------
-template <typename TI>
-__global__ void __launch_bounds__(tile::NT) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+template <typename TI, int TYV>
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
                                                           const TI* __restrict__ phi, TI* __restrict__ normx,
                                                           TI* __restrict__ normy, TI* __restrict__ normz,
                                                           TI* __restrict__ kappa) {
   using namespace tile;
+  using SH = Shape<TYV>;
+  constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+  (void)TY;
   typedef TI T;
   constexpr int VX = TX + 1, VY = TY + 1, VXY = VX * VY;  // vertices of the tile's cells in one plane
   __shared__ T pl[NSLOT][PXY];
@@ -70,7 +75,7 @@ __global__ void __launch_bounds__(tile::NT) k_youngs_tile(Geo g, const DevScalar
     T* dst = pl[kk % NSLOT];
     for (int q = tid; q < PXY; q += NT) {
       int h;
-      const bool ok = plane_cell(g, i0, j0, kk, q, &h);
+      const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
       cp_async(dst + q, phi + (ok ? h : 0), ok);
     }
     cp_commit();
@@ -176,9 +181,11 @@ __device__ __forceinline__ void acdi_face(const AcdiCoef<T>& cf, int dir, T dli,
   *rg = dpsi - sharp;
 }
 
-template <typename TI, bool SDF>
+template <typename TI, bool SDF, int TYV>
 constexpr size_t acdi_smem() {
   using namespace tile;
+  using SH = Shape<TYV>;
+  constexpr int TX = SH::TX, TY = SH::TY, PXY = SH::PXY, NSLOT = SH::NSLOT;
   constexpr int NF = (TX + 1) * TY + TX * (TY + 1);
   return sizeof(double) * NSLOT * PXY + sizeof(TI) * (NSLOT * 3 * PXY + (SDF ? NSLOT * PXY : 0) + 2 * NF);
 }
@@ -187,13 +194,16 @@ constexpr size_t acdi_smem() {
 
 // UPD: psi_out = clip(psi + f1*d + f2*d_old); `dpsidt` holds d_old on entry
 // and d on exit.  Without UPD, dpsidt receives d.
-template <typename TI, bool SDF, bool UPD>
-__global__ void __launch_bounds__(tile::NT) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+template <typename TI, bool SDF, bool UPD, int TYV>
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
     const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
     const TI* __restrict__ phi, const double* __restrict__ psi, TI* __restrict__ dpsidt,
     TI* __restrict__ fx, TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out) {
   using namespace tile;
+  using SH = Shape<TYV>;
+  constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+  (void)TY;
   typedef TI T;
   constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1), NF = NFX + NFY;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -219,7 +229,7 @@ __global__ void __launch_bounds__(tile::NT) k_acdi_tile(Geo g, const DevScalars*
     const int s = kk % NSLOT;
     for (int q = tid; q < PXY; q += NT) {
       int h;
-      const bool ok = plane_cell(g, i0, j0, kk, q, &h);
+      const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
       const int hh = ok ? h : 0;
       cp_async(s_psi + s * PXY + q, psi + hh, ok);
       cp_async(s_n + (s * 3 + 0) * PXY + q, nx_ + hh, ok);
@@ -332,21 +342,26 @@ __global__ void __launch_bounds__(tile::NT) k_acdi_tile(Geo g, const DevScalars*
 // update, the pressure-split terms and mom_xyz_oth stay in FP64.
 // ---------------------------------------------------------------------------
 namespace {
-template <typename TI>
+template <typename TI, int TYV>
 constexpr size_t mom_smem() {
   using namespace tile;
+  using SH = Shape<TYV>;
+  constexpr int PXY = SH::PXY, NSLOT = SH::NSLOT;
   return (size_t)NSLOT * PXY * (4 * sizeof(double) + 3 * sizeof(TI));
 }
 }  // namespace
 
-template <typename TI>
-__global__ void __launch_bounds__(tile::NT, 3) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
+template <typename TI, int TYV>
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
     int kz, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const double* __restrict__ psi, const double* __restrict__ psio, const TI* __restrict__ fx,
     const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
     const double* __restrict__ po, const TI* __restrict__ kappa, TI* __restrict__ duo, TI* __restrict__ dvo,
     TI* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo, double* __restrict__ wo) {
   using namespace tile;
+  using SH = Shape<TYV>;
+  constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+  (void)TY;
   typedef TI T;
   extern __shared__ __align__(16) unsigned char smem[];
   double* s_u = reinterpret_cast<double*>(smem);  // each [NSLOT][PXY]
@@ -366,7 +381,7 @@ __global__ void __launch_bounds__(tile::NT, 3) k_momentum_tile(Geo g, Phys ph, c
     const int o = (kk % NSLOT) * PXY;
     for (int q = tid; q < PXY; q += NT) {
       int h;
-      const bool ok = plane_cell(g, i0, j0, kk, q, &h);
+      const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
       const int hh = ok ? h : 0;
       cp_async(s_u + o + q, u + hh, ok);
       cp_async(s_v + o + q, v + hh, ok);
@@ -587,30 +602,61 @@ __global__ void __launch_bounds__(tile::NT, 3) k_momentum_tile(Geo g, Phys ph, c
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+template <typename TI, int TYV>
+static void youngs_go(const Launch& L, const Geo& g, const DevScalars* sc, const TI* phi, TI* nx, TI* ny, TI* nz,
+                      TI* kappa) {
+  using S = tile::Shape<TYV>;
+  const int kz = tile_kz<TYV>(g);
+  k_youngs_tile<TI, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), 0, L.st>>>(g, sc, kz, phi, nx, ny, nz,
+                                                                                    kappa);
+}
+
 template <typename TI>
 void launch_youngs_t(const Launch& L, const Geo& g, const DevScalars* sc, const TI* phi, TI* nx, TI* ny, TI* nz,
                      TI* kappa) {
-  const int kz = tile_kz(g);
-  k_youngs_tile<TI><<<tile::grid_of(g, kz), dim3(tile::TX, tile::TY), 0, L.st>>>(g, sc, kz, phi, nx, ny, nz, kappa);
+  if (tile::rows_of(g) == 2) youngs_go<TI, 2>(L, g, sc, phi, nx, ny, nz, kappa);
+  else youngs_go<TI, 8>(L, g, sc, phi, nx, ny, nz, kappa);
 }
 
-template <typename TI, bool SDF, bool UPD>
+template <typename TI, bool SDF, bool UPD, int TYV>
 static void acdi_go(const Launch& L, const Geo& g, const DevScalars* sc, const double* u, const double* v,
                     const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi, const double* psi,
                     double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
-  const int kz = tile_kz(g);
-  k_acdi_tile<TI, SDF, UPD><<<tile::grid_of(g, kz), dim3(tile::TX, tile::TY), acdi_smem<TI, SDF>(), L.st>>>(
-      g, sc, kz, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz, psi_out);
+  using S = tile::Shape<TYV>;
+  const int kz = tile_kz<TYV>(g);
+  k_acdi_tile<TI, SDF, UPD, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), acdi_smem<TI, SDF, TYV>(),
+                                   L.st>>>(g, sc, kz, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz, psi_out);
+}
+
+template <typename TI, int TYV>
+static void acdi_pick(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, bool upd, const double* u,
+                      const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
+                      const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
+  if (sdf && upd) acdi_go<TI, true, true, TYV>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+  else if (sdf) acdi_go<TI, true, false, TYV>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+  else if (upd) acdi_go<TI, false, true, TYV>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+  else acdi_go<TI, false, false, TYV>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
 }
 
 template <typename TI>
 void launch_acdi_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf, bool upd, const double* u,
                    const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
                    const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
-  if (sdf && upd) acdi_go<TI, true, true>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
-  else if (sdf) acdi_go<TI, true, false>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
-  else if (upd) acdi_go<TI, false, true>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
-  else acdi_go<TI, false, false>(L, g, sc, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+  if (tile::rows_of(g) == 2)
+    acdi_pick<TI, 2>(L, g, sc, sdf, upd, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+  else
+    acdi_pick<TI, 8>(L, g, sc, sdf, upd, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
+}
+
+template <typename TI, int TYV>
+static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
+                        const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
+                        const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
+                        TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
+  using S = tile::Shape<TYV>;
+  const int kz = tile_kz<TYV>(g);
+  k_momentum_tile<TI, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), mom_smem<TI, TYV>(), L.st>>>(
+      g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
 }
 
 template <typename TI>
@@ -618,9 +664,10 @@ void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevS
                        const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
                        const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
                        TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
-  const int kz = tile_kz(g);
-  k_momentum_tile<TI><<<tile::grid_of(g, kz), dim3(tile::TX, tile::TY), mom_smem<TI>(), L.st>>>(
-      g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+  if (tile::rows_of(g) == 2)
+    momentum_go<TI, 2>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+  else
+    momentum_go<TI, 8>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
 }
 
 template void launch_momentum_t<double>(const Launch&, const Geo&, const Phys&, const DevScalars*, const double*,
@@ -643,26 +690,25 @@ template void launch_acdi_t<float>(const Launch&, const Geo&, const DevScalars*,
                                    const float*, const double*, double*, float*, float*, float*, float*);
 
 // the ACDI and momentum tiles use more than the default 48 KB of dynamic shared memory
+template <typename TI, bool SDF, bool UPD, int TYV>
+static void acdi_attr() {
+  cudaFuncSetAttribute(k_acdi_tile<TI, SDF, UPD, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)acdi_smem<TI, SDF, TYV>());
+}
+template <typename TI, int TYV>
+static void tile_attrs() {
+  cudaFuncSetAttribute(k_momentum_tile<TI, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<TI, TYV>());
+  acdi_attr<TI, true, true, TYV>();
+  acdi_attr<TI, true, false, TYV>();
+  acdi_attr<TI, false, true, TYV>();
+  acdi_attr<TI, false, false, TYV>();
+}
 void tiles_set_attributes() {
-  cudaFuncSetAttribute(k_momentum_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)mom_smem<double>());
-  cudaFuncSetAttribute(k_momentum_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem<float>());
-  cudaFuncSetAttribute(k_acdi_tile<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<double, true>());
-  cudaFuncSetAttribute(k_acdi_tile<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<double, true>());
-  cudaFuncSetAttribute(k_acdi_tile<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<double, false>());
-  cudaFuncSetAttribute(k_acdi_tile<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<double, false>());
-  cudaFuncSetAttribute(k_acdi_tile<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<float, true>());
-  cudaFuncSetAttribute(k_acdi_tile<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<float, true>());
-  cudaFuncSetAttribute(k_acdi_tile<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<float, false>());
-  cudaFuncSetAttribute(k_acdi_tile<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)acdi_smem<float, false>());
+  tile_attrs<double, 8>();
+  tile_attrs<float, 8>();
+  tile_attrs<double, 2>();
+  tile_attrs<float, 2>();
 }
 
 }  // namespace cansfz

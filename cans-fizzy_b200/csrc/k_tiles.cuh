@@ -14,9 +14,15 @@
 namespace cansfz {
 namespace tile {
 
-constexpr int TX = 32, TY = 8, NT = TX * TY;
-constexpr int PX = TX + 2, PY = TY + 2, PXY = PX * PY;  // a plane of cells with a one-cell halo
-constexpr int NSLOT = 3;                                // ring of planes k-1, k, k+1 (k+2 in flight)
+// Tile shape: 32 x TYV columns.  TYV = 8 for 3-D grids; TYV = 2 for the
+// reference's 2-D convention (ny = 2), where an 8-row tile would leave three
+// quarters of its threads idle.
+template <int TYV>
+struct Shape {
+  static constexpr int TX = 32, TY = TYV, NT = TX * TY;
+  static constexpr int PX = TX + 2, PY = TY + 2, PXY = PX * PY;  // a plane of cells with a one-cell halo
+  static constexpr int NSLOT = 3;                                // ring of planes k-1, k, k+1 (k+2 in flight)
+};
 
 __device__ __forceinline__ void cp_async(void* sdst, const double* gsrc, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -34,6 +40,7 @@ __device__ __forceinline__ void cp_wait() {
 
 // Position of plane-slot element q (0 <= q < PXY) in the halo layout; false
 // when the cell lies outside the array (beyond ghost nx+1 or ny+1).
+template <int PX>
 __device__ __forceinline__ bool plane_cell(const Geo& g, int i0, int j0, int kk, int q, int* h) {
   const int a = q % PX, b = q / PX;
   const int ii = i0 - 1 + a, jj = j0 - 1 + b;
@@ -41,9 +48,14 @@ __device__ __forceinline__ bool plane_cell(const Geo& g, int i0, int j0, int kk,
   return ii <= g.nx + 1 && jj <= g.ny + 1;
 }
 
+template <int TYV>
 inline dim3 grid_of(const Geo& g, int kz) {
-  return dim3((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + kz - 1) / kz);
+  using S = Shape<TYV>;
+  return dim3((g.nx + S::TX - 1) / S::TX, (g.ny + S::TY - 1) / S::TY, (g.nz + kz - 1) / kz);
 }
+
+// the tile shape of a grid: 2 rows for ny <= 2, else 8
+inline int rows_of(const Geo& g) { return g.ny <= 2 ? 2 : 8; }
 
 }  // namespace tile
 }  // namespace cansfz
