@@ -135,6 +135,7 @@ struct PoissonPlan {
 struct Launch {
   cudaStream_t st;
   int nsm;
+  int batched;  // 1 while an ensemble graph is captured: other cases fill the GPU, so kernels favour fewer, larger blocks
 };
 
 // optional stage marker of the step profiler (CUDA events between stages)

@@ -963,7 +963,9 @@ int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
       for (int q = 0; q < n; ++q) {
         cansfz_ctx* c = e->cases[q];
         CK(cudaStreamWaitEvent(c->st, e->fork, 0));
+        c->L.batched = 1;
         enqueue_step(c);
+        c->L.batched = 0;
         CK(cudaEventRecord(e->join[q], c->st));
         CK(cudaStreamWaitEvent(e->st, e->join[q], 0));
       }

@@ -36,8 +36,11 @@ template <typename T>
 __device__ __forceinline__ T sqr(T x) { return x * x; }
 
 template <int TYV>
-int tile_kz(const Geo& g) {
+int tile_kz(const Geo& g, int batched) {
   using S = tile::Shape<TYV>;
+  // in an ensemble the other cases keep the GPU busy: 32 levels per block
+  // spend 6% on the two extra planes each block loads (25% at 8 levels)
+  if (batched) return g.nz < 32 ? g.nz : 32;
   // about six waves of four resident blocks on each of 148 SMs, so the last
   // partial wave costs little; at least 8 levels per block (each block loads
   // two planes and evaluates one face/vertex plane beyond its own levels)
@@ -606,7 +609,7 @@ template <typename TI, int TYV>
 static void youngs_go(const Launch& L, const Geo& g, const DevScalars* sc, const TI* phi, TI* nx, TI* ny, TI* nz,
                       TI* kappa) {
   using S = tile::Shape<TYV>;
-  const int kz = tile_kz<TYV>(g);
+  const int kz = tile_kz<TYV>(g, L.batched);
   k_youngs_tile<TI, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), 0, L.st>>>(g, sc, kz, phi, nx, ny, nz,
                                                                                     kappa);
 }
@@ -623,7 +626,7 @@ static void acdi_go(const Launch& L, const Geo& g, const DevScalars* sc, const d
                     const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi, const double* psi,
                     double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
   using S = tile::Shape<TYV>;
-  const int kz = tile_kz<TYV>(g);
+  const int kz = tile_kz<TYV>(g, L.batched);
   k_acdi_tile<TI, SDF, UPD, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), acdi_smem<TI, SDF, TYV>(),
                                    L.st>>>(g, sc, kz, u, v, w, nx, ny, nz, phi, psi, hist, fx, fy, fz, psi_out);
 }
@@ -654,7 +657,7 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
                         const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
                         TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
   using S = tile::Shape<TYV>;
-  const int kz = tile_kz<TYV>(g);
+  const int kz = tile_kz<TYV>(g, L.batched);
   k_momentum_tile<TI, TYV><<<tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), mom_smem<TI, TYV>(), L.st>>>(
       g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
 }

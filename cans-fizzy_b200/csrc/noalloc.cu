@@ -142,7 +142,7 @@ extern "C" int cansfz_solver_static(const int n[3], const char cbc[3][2], double
   cansfz::Geo g{};
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.sx = nx + 2; g.sxy = (nx + 2) * (ny + 2);
-  cansfz::Launch L{st, 0};
+  cansfz::Launch L{st, 0, 0};
   cansfz::launch_poisson(L, g, pl, nullptr, p);
   return cudaGetLastError() == cudaSuccess ? CANSFZ_OK : CANSFZ_ERR_CUDA;
 }
