@@ -340,6 +340,9 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
 // is carried in registers and the ring never needs three planes at once.
 // psio, p, po and kappa enter only at (0,0,0), (1,0,0), (0,1,0), (0,0,1):
 // read through the read-only cache, the own-column value carried upwards.
+// Those loads and the history reads are issued at the top of each level, so
+// that the stencil arithmetic hides their latency; holding them takes up to
+// 128 registers, two 256-thread blocks per SM.
 // The expressions are those of the per-point kernels (same operand order).
 // With TI = float the advection/diffusion RHS is evaluated in FP32; the AB2
 // update, the pressure-split terms and mom_xyz_oth stay in FP64.
@@ -355,7 +358,7 @@ constexpr size_t mom_smem() {
 }  // namespace
 
 template <typename TI, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT, 2) k_momentum_tile(Geo g, Phys ph, const DevScalars* __restrict__ sc,
     int kz, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const double* __restrict__ psi, const double* __restrict__ psio, const TI* __restrict__ fx,
     const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
@@ -448,6 +451,16 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g
 #define FLX(s, a, b) (rho * PU(s, a, b) + drho * s_fx[o##s + (a) + PX * (b)])
 #define FLY(s, a, b) (rho * PV(s, a, b) + drho * s_fy[o##s + (a) + PX * (b)])
 #define FLZ(s, a, b) (rho * PW(s, a, b) + drho * s_fz[o##s + (a) + PX * (b)])
+      // the level's loads from global memory, issued before the stencil
+      // arithmetic that hides their latency
+      const int c = g.h(i, j, k), t = g.t(i, j, k);
+      const double pso_x = __ldg(psio + c + 1), pso_y = __ldg(psio + c + sx), pso_z = __ldg(psio + c + sxy);
+      const double p_x = __ldg(p + c + 1), p_y = __ldg(p + c + sx), p_z = __ldg(p + c + sxy);
+      const double po_x = __ldg(po + c + 1), po_y = __ldg(po + c + sx), po_z = __ldg(po + c + sxy);
+      const double k_x = (double)__ldg(kappa + c + 1), k_y = (double)__ldg(kappa + c + sx),
+                   k_z = (double)__ldg(kappa + c + sxy);
+      const double hu0 = first ? 0. : (double)duo[t], hv0 = first ? 0. : (double)dvo[t],
+                   hw0 = first ? 0. : (double)dwo[t];
       const T dzci_c = (T)g.dzci[k], dzci_m = (T)g.dzci[k - 1], dzfi_c = (T)g.dzfi[k], dzfi_p = (T)g.dzfi[k + 1];
       // the three components one after another, each reading its stencil
       // from shared memory, so that few values are live at a time
@@ -531,9 +544,7 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g
                    dzci_c * ((dwdzp + dwdzp) * muzp - (dwdzm + dwdzm) * muzm);
       }
       // first AB2 update with the density ratio (src/rk.f90:86-101), FP64
-      const int c = g.h(i, j, k), t = g.t(i, j, k);
       const double ps_c = s_c[o0], ps_x = s_c[o0 + 1], ps_y = s_c[o0 + PX], ps_z = s_c[o1];
-      const double pso_x = __ldg(psio + c + 1), pso_y = __ldg(psio + c + sx), pso_z = __ldg(psio + c + sxy);
       const double rhox_n = rhod + drhod * 0.5 * (pso_c + pso_x);
       const double rhoy_n = rhod + drhod * 0.5 * (pso_c + pso_y);
       const double rhoz_n = rhod + drhod * 0.5 * (pso_c + pso_z);
@@ -541,8 +552,7 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g
       const double rhoy_p = rhod + drhod * 0.5 * (ps_c + ps_y);
       const double rhoz_p = rhod + drhod * 0.5 * (ps_c + ps_z);
       const double Ru = (double)dudt_aux, Rv = (double)dvdt_aux, Rw = (double)dwdt_aux;
-      const double Ruo = first ? Ru : (double)duo[t], Rvo = first ? Rv : (double)dvo[t],
-                   Rwo = first ? Rw : (double)dwo[t];
+      const double Ruo = first ? Ru : hu0, Rvo = first ? Rv : hv0, Rwo = first ? Rw : hw0;
       const double irx = 1. / rhox_p, iry = 1. / rhoy_p, irz = 1. / rhoz_p;
       const double un = s_u[o0] * rhox_n * irx + (f1 * Ru + f2 * Ruo) * irx;
       const double vn = s_v[o0] * rhoy_n * iry + (f1 * Rv + f2 * Rvo) * iry;
@@ -551,10 +561,6 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 3) k_momentum_tile(Geo g
       dvo[t] = dvdt_aux;
       dwo[t] = dwdt_aux;
       // mom_xyz_oth with pn = p (src/mom.f90:912-1038), FP64
-      const double p_x = __ldg(p + c + 1), p_y = __ldg(p + c + sx), p_z = __ldg(p + c + sxy);
-      const double po_x = __ldg(po + c + 1), po_y = __ldg(po + c + sx), po_z = __ldg(po + c + sxy);
-      const double k_x = (double)__ldg(kappa + c + 1), k_y = (double)__ldg(kappa + c + sx),
-                   k_z = (double)__ldg(kappa + c + sxy);
       const double q_ccc = (1. + dt_r) * p_c - dt_r * po_c;
       const double q_pcc = (1. + dt_r) * p_x - dt_r * po_x;
       const double q_cpc = (1. + dt_r) * p_y - dt_r * po_y;
