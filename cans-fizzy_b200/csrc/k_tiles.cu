@@ -14,13 +14,17 @@
 // vertices.  The vertex gradient is evaluated in the form the reference uses
 // for the (+x,+y,+z) vertex of its lower cell, so a vertex that the
 // reference evaluates from another cell may differ in the last bit (sums of
-// the same four terms in another order).
+// the same four terms in another order).  The vertex plane of level k+1 and
+// the cells of level k are evaluated in the same pass (three vertex planes,
+// four cell planes in the ring), so each level needs one barrier.
 //
 // ACDI: each face flux (advective part and regularisation part) is shared by
 // the two cells on either side.  Each thread evaluates its cell's +x, +y and
 // +z faces together (x and y into shared memory, the z face carried in
 // registers to the next level as its k-1/2 face); 40 threads add the tile's
-// -x and -y boundary faces.  Every face expression is
+// -x and -y boundary faces.  The face velocities of level k+1 and the AB2
+// history of level k are loaded before level k's faces are evaluated, so that
+// the face arithmetic hides their latency.  Every face expression is
 // the reference's with the two cells' roles swapped only inside sums and
 // products of two terms, so the results are bitwise those of the per-cell
 // form.
@@ -63,33 +67,41 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_youngs_tile(Geo g, con
                                                           TI* __restrict__ kappa) {
   using namespace tile;
   using SH = Shape<TYV>;
-  constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+  constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY;
   (void)TY;
   typedef TI T;
   constexpr int VX = TX + 1, VY = TY + 1, VXY = VX * VY;  // vertices of the tile's cells in one plane
-  __shared__ T pl[NSLOT][PXY];
-  __shared__ T vn[2][3][VXY];  // normalised vertex gradients, planes k-1/2 and k+1/2
+  // cell planes m-1 .. m+2 around the level m being gathered (m+3 in
+  // flight), and three vertex planes: the two the cells of level m gather
+  // from and the one evaluated for level m+1 in the same pass
+  constexpr int NCP = 4, NVP = 3;
+  __shared__ T pl[NCP][PXY];
+  __shared__ T vn[NVP][3][VXY];
   if (HALTED(sc)) return;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
   const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
   const int kb = blockIdx.z * kz + 1, ke = min(kb + kz - 1, g.nz);
 
+  // cell plane kk (kb-1 <= kk <= ke+1) into its ring slot; an empty group
+  // past the top keeps the wait counts uniform
   auto issue = [&](int kk) {
-    T* dst = pl[kk % NSLOT];
-    for (int q = tid; q < PXY; q += NT) {
-      int h;
-      const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
-      cp_async(dst + q, phi + (ok ? h : 0), ok);
+    if (kk <= ke + 1) {
+      T* dst = pl[kk % NCP];
+      for (int q = tid; q < PXY; q += NT) {
+        int h;
+        const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
+        cp_async(dst + q, phi + (ok ? h : 0), ok);
+      }
     }
     cp_commit();
   };
   // vertex plane kk+1/2 from cell planes kk and kk+1
   auto vertices = [&](int kk) {
-    const T* lo = pl[kk % NSLOT];
-    const T* hi = pl[(kk + 1) % NSLOT];
-    T* ox = vn[kk & 1][0];
-    T* oy = vn[kk & 1][1];
-    T* oz = vn[kk & 1][2];
+    const T* lo = pl[kk % NCP];
+    const T* hi = pl[(kk + 1) % NCP];
+    T* ox = vn[(kk + NVP) % NVP][0];
+    T* oy = vn[(kk + NVP) % NVP][1];
+    T* oz = vn[(kk + NVP) % NVP][2];
     const T d1 = (T)g.dxi, d2 = (T)g.dyi, dz = (T)g.dzci[kk];
     for (int q = tid; q < VXY; q += NT) {
       const int a = q % VX, b = q / VX, s = a + PX * b;
@@ -108,24 +120,27 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_youngs_tile(Geo g, con
   issue(kb - 1);
   issue(kb);
   issue(kb + 1);
+  issue(kb + 2);
   cp_wait<1>();
-  __syncthreads();
+  __syncthreads();  // planes kb-1, kb, kb+1 are in
   vertices(kb - 1);
-  __syncthreads();  // plane kb-1's slot is refilled next
+  vertices(kb);
 
   const int i = i0 + tx, j = j0 + ty;
   const bool act = i <= g.nx && j <= g.ny;
   const T d1 = (T)g.dxi, d2 = (T)g.dyi;
   for (int k = kb; k <= ke; ++k) {
-    if (k + 2 <= ke + 1) issue(k + 2);
-    else cp_commit();
+    // plane k+3 goes into the slot of plane k-1, last read for vertex plane
+    // k-1/2 before the previous barrier
+    issue(k + 3);
     cp_wait<1>();
-    __syncthreads();  // plane k+1 is in; every thread is done with level k-1
-    vertices(k);
-    __syncthreads();
+    __syncthreads();  // plane k+2 is in; vertex planes k-1/2 and k+1/2 are complete
+    // one pass: vertex plane k+3/2 (for level k+1) and the cells of level k,
+    // which read the other two vertex planes
+    if (k + 1 <= ke) vertices(k + 1);
     if (act) {
-      const T* lo = vn[(k - 1) & 1][0];
-      const T* hi = vn[k & 1][0];
+      const T* lo = vn[(k - 1 + NVP) % NVP][0];
+      const T* hi = vn[k % NVP][0];
       const int vm = tx + VX * ty;  // the (-x,-y) vertex of the cell
       // vertex q: 0 (+,+,+) 1 (+,-,+) 2 (+,+,-) 3 (+,-,-) 4 (-,+,+) 5 (-,-,+) 6 (-,+,-) 7 (-,-,-)
       const int off[8] = {VX + 1, 1, VX + 1, 1, VX, 0, VX, 0};
@@ -227,6 +242,7 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
   cf.qg = T(0.25) * cf.gam;
   cf.is = T(1.) / seps;
   const T dxi = (T)g.dxi, dyi = (T)g.dyi;
+  const bool first2 = sc->first_rk2fl;
 
   auto issue = [&](int kk) {
     const int s = kk % NSLOT;
@@ -266,6 +282,11 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
          &rg_zm);
   __syncthreads();  // plane kb-1's slot is refilled next
 
+  T vx_n = T(0), vy_n = T(0), vz_n = T(0);
+  if (act) {
+    const int c = g.h(i, j, kb);
+    vx_n = (T)__ldg(u + c); vy_n = (T)__ldg(v + c); vz_n = (T)__ldg(w + c);
+  }
   for (int k = kb; k <= ke; ++k) {
     if (k + 2 <= ke + 1) issue(k + 2);
     else cp_commit();
@@ -273,11 +294,16 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
     __syncthreads();  // plane k+1 is in; every thread is done with level k-1
     const int s0 = k % NSLOT, s1 = (k + 1) % NSLOT;
     T up_zp = T(0), rg_zp = T(0);
+    T dO_pre = T(0);
     if (act) {
       // the cell's own +x, +y and +z faces: three independent evaluations in
       // one block of code, so that their dependency chains overlap
       const int c = g.h(i, j, k);
-      const T vx = (T)__ldg(u + c), vy = (T)__ldg(v + c), vz = (T)__ldg(w + c);
+      const T vx = vx_n, vy = vy_n, vz = vz_n;
+      if (k < ke) {
+        vx_n = (T)__ldg(u + c + g.sxy); vy_n = (T)__ldg(v + c + g.sxy); vz_n = (T)__ldg(w + c + g.sxy);
+      }
+      if (UPD && !first2) dO_pre = dpsidt[g.t(i, j, k)];
       T upx, rgx, upy, rgy;
       face(0, dxi, s0, qc, s0, qc + 1, vx, &upx, &rgx);
       face(1, dyi, s0, qc, s0, qc + PX, vy, &upy, &rgy);
@@ -315,7 +341,7 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
       const T d = -adv + rglr;
       const int c = g.h(i, j, k), t = g.t(i, j, k);
       if (UPD) {
-        const T dO = sc->first_rk2fl ? d : dpsidt[t];
+        const T dO = first2 ? d : dO_pre;
         psi_out[c] = fmin(fmax(0., psi_c + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
       }
       dpsidt[t] = d;
