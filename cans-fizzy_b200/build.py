@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCES = ["csrc/k_stencil.cu", "csrc/k_tiles.cu", "csrc/k_bc.cu", "csrc/k_poisson.cu", "csrc/context.cu", "csrc/noalloc.cu"]
 OUT = os.path.join(HERE, "cansfz", "libcansfz.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def nvcc() -> str:
@@ -34,7 +35,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d)):
             return OUT
-    cmd = [nvcc()] + ARCH + FLAGS + ["-o", OUT] + srcs
+    # one nvcc per source file, in parallel, then one link
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = [os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o") for src in srcs]
+    procs = []
+    for src, obj in zip(srcs, objs):
+        cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((src, subprocess.Popen(cmd, cwd=HERE)))
+    failed = [src for src, pr in procs if pr.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=HERE)

@@ -150,20 +150,31 @@ class Case:
 
 class Ensemble:
     """Independent cases advanced together: one CUDA graph launch per step
-    holds every case's step as a parallel branch (cansfz_ensemble_*)."""
+    holds every case's step as a parallel branch (cansfz_ensemble_*).  With
+    batch > 1, cases of the same grid and options share batched launches in
+    groups of up to `batch` cases."""
 
-    def __init__(self, cases):
+    def __init__(self, cases, batch: int = 1):
         self.lib = _L.load()
         self.cases = list(cases)
         arr = (ct.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
         h = ct.c_void_p()
         _L.check(self.lib.cansfz_ensemble_create(arr, len(self.cases), None, ct.byref(h)), "cansfz_ensemble_create")
         self.h = h
+        if batch != 1:
+            _L.check(self.lib.cansfz_ensemble_set_batching(self.h, int(batch)), "cansfz_ensemble_set_batching")
 
     def step(self, nsteps: int = 1):
         st = (ct.c_int * len(self.cases))()
         rc = self.lib.cansfz_ensemble_step(self.h, int(nsteps), st)
         return rc, list(st)
+
+    def groups(self):
+        """(number of case groups, cases in groups of two or more) of the
+        graph built at the last step."""
+        ng, gc = ct.c_int(), ct.c_int()
+        _L.check(self.lib.cansfz_ensemble_info(self.h, ct.byref(ng), ct.byref(gc)), "cansfz_ensemble_info")
+        return ng.value, gc.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -77,6 +77,8 @@ SIGNATURES = {
     "cansfz_ensemble_create": (I, [V, I, V, V]),
     "cansfz_ensemble_step": (I, [V, I, V]),
     "cansfz_ensemble_destroy": (I, [V]),
+    "cansfz_ensemble_set_batching": (I, [V, I]),
+    "cansfz_ensemble_info": (I, [V, ct.POINTER(I), ct.POINTER(I)]),
     "cansfz_solver_static": (I, [ct.POINTER(I), ct.c_char_p, D, V, V, V, V, V, V]),
 }
 

@@ -127,15 +127,27 @@ struct PoissonPlan {
   float* workf;          // FP32 spectral buffers of the mixed form
   float* work2f;
   int zsing;             // z operator singular (no Dirichlet wall): pin the (0,0) mode in FP32
+  // elimination factors of the z systems, which do not change between
+  // solves: 1/pivot and c/pivot per (column, level) in the spectral layout
+  // (null: the solve evaluates them on the fly)
+  double* zpiv;
+  double* zdf;
+  float* zpivf;
+  float* zdff;
 };
 
 // ---------------------------------------------------------------------------
 // kernel launchers (host functions), all on `st`
 // ---------------------------------------------------------------------------
+struct Recorder;  // batch.cuh
 struct Launch {
   cudaStream_t st;
   int nsm;
-  int batched;  // 1 while an ensemble graph is captured: other cases fill the GPU, so kernels favour fewer, larger blocks
+  // 1 while an ensemble graph is captured: other cases fill the GPU, so
+  // kernels favour fewer, larger blocks
+  int batched;
+  // set: launches are recorded for a batched replay instead of issued
+  Recorder* rec = nullptr;
 };
 
 // optional stage marker of the step profiler (CUDA events between stages)
@@ -236,6 +248,9 @@ void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
 
 // k_poisson.cu
 void poisson_set_attributes();
+// the z systems' elimination factors of `pl` (FP64, or FP32 for the mixed
+// form) into piv/df, evaluated exactly as the solve's forward sweep does
+void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool f32, void* piv, void* df);
 
 // z-marching tile kernels (k_tiles.cu), TI = double (drop-in) or float (mixed form)
 template <typename TI>

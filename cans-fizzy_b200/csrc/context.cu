@@ -11,9 +11,11 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "cansfz_internal.cuh"
 
 using namespace cansfz;
+
 
 #define CK(x)                                                                  \
   do {                                                                         \
@@ -273,6 +275,23 @@ bool factorize(int m, int radix[FFT_MAXSTAGES], int* nst) {
   return m == 1 && k <= FFT_MAXSTAGES;
 }
 
+// z solves with fewer columns than this read precomputed elimination factors
+bool zsolve_factored(const cansfz_ctx* c) { return (long long)c->g.nx * c->g.ny < 32768; }
+
+// FP32 spectral buffers and z factors of the mixed-form solve (once)
+int alloc_f32_solver(cansfz_ctx* c) {
+  const size_t nint = (size_t)c->g.tsize();
+  int rc;
+  if (!c->pl.workf && (rc = dalloc(c, &c->pl.workf, nint))) return rc;
+  if (c->pl.zper && !c->pl.work2f && (rc = dalloc(c, &c->pl.work2f, nint))) return rc;
+  if (!c->pl.zpivf && zsolve_factored(c)) {
+    if ((rc = dalloc(c, &c->pl.zpivf, nint)) || (rc = dalloc(c, &c->pl.zdff, nint))) return rc;
+    launch_z_factors(c->L, c->g, c->pl, true, c->pl.zpivf, c->pl.zdff);
+    CK(cudaGetLastError());
+  }
+  return CANSFZ_OK;
+}
+
 int setup_solver(cansfz_ctx* c) {
   const cansfz_params& P = c->P;
   const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
@@ -407,15 +426,20 @@ int setup_solver(cansfz_ctx* c) {
     rc = dalloc(c, &c->pl.work2, nint);
     if (rc) return rc;
   }
+  // the z systems' elimination factors, once per plan, where the solve has
+  // few columns: there the pivot recurrence's latency bounds the solve,
+  // while with many columns reading the factors costs more than evaluating
+  // them
+  if (zsolve_factored(c)) {
+    if ((rc = dalloc(c, &c->pl.zpiv, nint)) || (rc = dalloc(c, &c->pl.zdf, nint))) return rc;
+    launch_z_factors(c->L, c->g, c->pl, false, c->pl.zpiv, c->pl.zdf);
+    CK(cudaGetLastError());
+  }
   if (P.form == CANSFZ_FORM_MIXED) {
     if (!c->rhsb_zero) return CANSFZ_ERR_UNSUPPORTED;  // refinement assumes homogeneous pressure BCs
-    rc = dalloc(c, &c->pl.workf, nint);
-    if (rc) return rc;
-    if (c->pl.zper) {
-      rc = dalloc(c, &c->pl.work2f, nint);
-      if (rc) return rc;
-    }
+    if ((rc = alloc_f32_solver(c))) return rc;
   }
+  CK(cudaStreamSynchronize(c->st));
   return CANSFZ_OK;
 }
 
@@ -601,6 +625,34 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
   launch_step_reductions(L, g, c->ph, sc, c->partial, c->u[b], c->v[b], c->w[b]);
   MARK("gamma_chkdt_chkdiv");
 #undef MARK
+}
+
+// One step of case c recorded instead of issued.  Launches that do not go
+// through the recorder are caught by a throwaway stream capture: the record
+// is complete (the step can be replayed batched) when that capture is empty.
+int record_step(cansfz_ctx* c, Recorder* rec, bool* complete) {
+  *complete = false;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  c->L.rec = rec;
+  c->L.batched = 1;
+  enqueue_step(c);
+  c->L.rec = nullptr;
+  c->L.batched = 0;
+  CK(cudaStreamEndCapture(c->st, &g));
+  size_t nodes = 0;
+  const cudaError_t e = cudaGraphGetNodes(g, nullptr, &nodes);
+  cudaGraphDestroy(g);
+  CK(e);
+  *complete = nodes == 0 && !rec->e.empty();
+  return CANSFZ_OK;
+}
+
+bool same_record(const Recorder& a, const Recorder& b) {
+  if (a.e.size() != b.e.size()) return false;
+  for (size_t q = 0; q < a.e.size(); ++q)
+    if (!a.e[q].same_launch(b.e[q])) return false;
+  return true;
 }
 
 }  // namespace
@@ -896,6 +948,9 @@ struct cansfz_ensemble {
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int cur = 0;
+  int ngroups = 0, grouped = 0;  // case groups of the last graph built, cases in groups of two or more
+  void* argtab[2] = {nullptr, nullptr};  // the groups' argument tables of each parity's graph
+  int batch = 1;  // cases per batched launch chain (1: every case its own branch)
 };
 
 int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, cansfz_ensemble** out) {
@@ -918,6 +973,7 @@ int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, c
   e->join.resize(ncases, nullptr);
   for (int q = 0; ok && q < ncases; ++q)
     ok = cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) == cudaSuccess;
+
   if (!ok) {
     cansfz_ensemble_destroy(e);
     return CANSFZ_ERR_CUDA;
@@ -928,10 +984,13 @@ int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, c
 
 int cansfz_ensemble_destroy(cansfz_ensemble* e) {
   if (!e) return CANSFZ_ERR_ARG;
-  for (int q = 0; q < 2; ++q)
+  for (int q = 0; q < 2; ++q) {
     if (e->gexec[q]) cudaGraphExecDestroy(e->gexec[q]);
+    if (e->argtab[q]) cudaFree(e->argtab[q]);
+  }
   for (cudaEvent_t ev : e->join)
     if (ev) cudaEventDestroy(ev);
+
   if (e->fork) cudaEventDestroy(e->fork);
   // the stream is the caller's when one was given; a created one is released
   bool own = true;
@@ -957,17 +1016,105 @@ int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
   for (int s = 0; s < nsteps; ++s) {
     const int par = e->cur;
     if (!e->gexec[par]) {
+      // record every case's step; cases whose records agree launch for
+      // launch (same kernels, grids and shared memory: same sizes and
+      // options) form a group that is replayed as batched launches
+      std::vector<Recorder> rec(n);
+      std::vector<std::vector<int>> groups;
+      // branches in order of decreasing size, so that the longest steps
+      // start first
+      std::vector<int> order(n);
+      for (int q = 0; q < n; ++q) order[q] = q;
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return e->cases[x]->g.tsize() > e->cases[y]->g.tsize();
+      });
+      for (int q : order) {
+        bool complete = false;
+        if (e->batch > 1) {
+          if (int rc = record_step(e->cases[q], &rec[q], &complete)) return rc;
+        }
+        bool placed = false;
+        for (auto& gr : groups)
+          if (complete && gr.size() > 0 && !rec[gr[0]].e.empty() && same_record(rec[gr[0]], rec[q])) {
+            gr.push_back(q);
+            placed = true;
+            break;
+          }
+        if (!placed) {
+          groups.push_back({q});
+          if (!complete) rec[q].e.clear();  // never joined by another case
+        }
+      }
+      // a group runs as chains of at most e->batch cases, so that the
+      // latency-bound stages of one chain overlap the others' work
+      {
+        const size_t chain = (size_t)std::max(1, e->batch);
+        std::vector<std::vector<int>> split;
+        for (auto& gr : groups)
+          for (size_t q0 = 0; q0 < gr.size(); q0 += chain)
+            split.emplace_back(gr.begin() + q0, gr.begin() + std::min(gr.size(), q0 + chain));
+        groups.swap(split);
+      }
+      e->ngroups = (int)groups.size();
+      e->grouped = 0;
+      // argument tables: per group and launch, the cases' argument lists in
+      // case order, 16-byte aligned, in one device buffer
+      std::vector<std::vector<size_t>> off(groups.size());
+      size_t total = 0;
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const auto& gr = groups[gi];
+        if (gr.size() < 2) continue;
+        e->grouped += (int)gr.size();
+        for (const RecEntry& en : rec[gr[0]].e) {
+          if (en.prepare(en)) return CANSFZ_ERR_CUDA;
+          off[gi].push_back(total);
+          total += (gr.size() * en.args.size() + 15) / 16 * 16;
+        }
+      }
+      if (e->argtab[par]) {
+        cudaFree(e->argtab[par]);
+        e->argtab[par] = nullptr;
+      }
+      if (total > 0) {
+        std::vector<unsigned char> host(total, 0);
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+          const auto& gr = groups[gi];
+          if (gr.size() < 2) continue;
+          for (size_t p = 0; p < rec[gr[0]].e.size(); ++p) {
+            const size_t sz = rec[gr[0]].e[p].args.size();
+            for (size_t q = 0; q < gr.size(); ++q)
+              std::memcpy(host.data() + off[gi][p] + q * sz, rec[gr[q]].e[p].args.data(), sz);
+          }
+        }
+        CK(cudaMalloc(&e->argtab[par], total));
+        CK(cudaMemcpy(e->argtab[par], host.data(), total, cudaMemcpyHostToDevice));
+      }
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
       CK(cudaEventRecord(e->fork, e->st));
-      for (int q = 0; q < n; ++q) {
-        cansfz_ctx* c = e->cases[q];
-        CK(cudaStreamWaitEvent(c->st, e->fork, 0));
-        c->L.batched = 1;
-        enqueue_step(c);
-        c->L.batched = 0;
-        CK(cudaEventRecord(e->join[q], c->st));
-        CK(cudaStreamWaitEvent(e->st, e->join[q], 0));
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const auto& gr = groups[gi];
+        cansfz_ctx* c0 = e->cases[gr[0]];
+        cudaStream_t bs = c0->st;
+        CK(cudaStreamWaitEvent(bs, e->fork, 0));
+        if (gr.size() == 1) {
+          c0->L.batched = 1;
+          enqueue_step(c0);
+          c0->L.batched = 0;
+        } else {
+          const unsigned char* tab = static_cast<const unsigned char*>(e->argtab[par]);
+          for (size_t p = 0; p < rec[gr[0]].e.size(); ++p) {
+            const RecEntry& en = rec[gr[0]].e[p];
+            if (en.launch(en, (int)gr.size(), tab + off[gi][p], bs)) {
+              cudaGraph_t bad = nullptr;
+              cudaStreamEndCapture(e->st, &bad);
+              if (bad) cudaGraphDestroy(bad);
+              return CANSFZ_ERR_CUDA;
+            }
+          }
+        }
+        CK(cudaEventRecord(e->join[gr[0]], bs));
+        CK(cudaStreamWaitEvent(e->st, e->join[gr[0]], 0));
       }
       CK(cudaStreamEndCapture(e->st, &graph));
       CK(cudaGraphInstantiate(&e->gexec[par], graph, 0));
@@ -990,6 +1137,26 @@ int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
     if (c->last_status != CANSFZ_OK && worst == CANSFZ_OK) worst = c->last_status;
   }
   return worst;
+}
+
+int cansfz_ensemble_set_batching(cansfz_ensemble* e, int cases_per_launch) {
+  if (!e || cases_per_launch < 1) return CANSFZ_ERR_ARG;
+  if (cases_per_launch != e->batch) {
+    e->batch = cases_per_launch;
+    for (int q = 0; q < 2; ++q)
+      if (e->gexec[q]) {
+        cudaGraphExecDestroy(e->gexec[q]);
+        e->gexec[q] = nullptr;
+      }
+  }
+  return CANSFZ_OK;
+}
+
+int cansfz_ensemble_info(cansfz_ensemble* e, int* ngroups, int* grouped_cases) {
+  if (!e) return CANSFZ_ERR_ARG;
+  if (ngroups) *ngroups = e->ngroups;
+  if (grouped_cases) *grouped_cases = e->grouped;
+  return CANSFZ_OK;
 }
 
 int cansfz_step(cansfz_ctx* c, int nsteps) {
@@ -1425,10 +1592,9 @@ int cansfz_profile_stages(cansfz_ctx* c, int nsteps, double* ms, int maxstages, 
 int cansfz_solver_refined(cansfz_ctx* c, const double* rhs, double* p, int sweeps) {
   if (!c || !rhs || !p || sweeps < 0 || sweeps > 16) return CANSFZ_ERR_ARG;
   if (!c->rhsb_zero) return CANSFZ_ERR_UNSUPPORTED;
-  const size_t nint = (size_t)c->g.tsize(), H = (size_t)c->g.hsize();
+  const size_t H = (size_t)c->g.hsize();
   int rc;
-  if (!c->pl.workf && (rc = dalloc(c, &c->pl.workf, nint))) return rc;
-  if (c->pl.zper && !c->pl.work2f && (rc = dalloc(c, &c->pl.work2f, nint))) return rc;
+  if ((rc = alloc_f32_solver(c))) return rc;
   if (!c->res64 && (rc = dalloc(c, &c->res64, H))) return rc;
   DevScalars h{};
   if ((rc = call_scalars(c, h))) return rc;

@@ -7,7 +7,7 @@
 // Each stage is one launch over every field of a BcGroup; within a stage a
 // thread owns one point of the face plane and applies face 0 then face 1,
 // exactly as set_bc (src/bound.f90:126-293) writes them.
-#include "cansfz_internal.cuh"
+#include "batch.cuh"
 
 namespace cansfz {
 
@@ -81,14 +81,21 @@ __device__ __forceinline__ void bc_stage_point(const Geo& g, const BcField& F, E
 }
 
 template <int STAGE>
+struct BcStage {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const BcGroup& grp,
+      const DevScalars* __restrict__ sc) {
+    if (sc != nullptr && sc->halted) return;
+    const int fi = bk.y;
+    if (fi >= grp.nf) return;
+    const BcField& F = grp.f[fi];
+    const int q = bk.x * blockDim.x + threadIdx.x;
+    if (F.f32) bc_stage_point<STAGE, float>(g, F, static_cast<float*>(F.p), q);
+    else bc_stage_point<STAGE, double>(g, F, static_cast<double*>(F.p), q);
+  }
+};
+template <int STAGE>
 __global__ void k_bc_stage(Geo g, BcGroup grp, const DevScalars* __restrict__ sc) {
-  if (sc != nullptr && sc->halted) return;
-  const int fi = blockIdx.y;
-  if (fi >= grp.nf) return;
-  const BcField& F = grp.f[fi];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (F.f32) bc_stage_point<STAGE, float>(g, F, static_cast<float*>(F.p), q);
-  else bc_stage_point<STAGE, double>(g, F, static_cast<double*>(F.p), q);
+  BcStage<STAGE>::run(blk_here(), g, grp, sc);
 }
 
 void launch_bc_group(const Launch& L, const Geo& g, const BcGroup& grp, const DevScalars* sc) {
@@ -105,11 +112,11 @@ void launch_bc_group(const Launch& L, const Geo& g, const BcGroup& grp, const De
   const int tb = 256;
   if (any_per) {
     const int n = 2 * NX * NZ + 2 * NX * NY;
-    k_bc_stage<ST_PER><<<dim3((n + tb - 1) / tb, grp.nf), tb, 0, L.st>>>(g, grp, sc);
+    kgo<BcStage<ST_PER>, 256, 1>(L, k_bc_stage<ST_PER>, dim3((n + tb - 1) / tb, grp.nf), tb, 0, g, grp, sc);
   }
-  if (any_x) k_bc_stage<ST_X><<<dim3((NY * NZ + tb - 1) / tb, grp.nf), tb, 0, L.st>>>(g, grp, sc);
-  if (any_y) k_bc_stage<ST_Y><<<dim3((NX * NZ + tb - 1) / tb, grp.nf), tb, 0, L.st>>>(g, grp, sc);
-  if (any_z) k_bc_stage<ST_Z><<<dim3((NX * NY + tb - 1) / tb, grp.nf), tb, 0, L.st>>>(g, grp, sc);
+  if (any_x) kgo<BcStage<ST_X>, 256, 1>(L, k_bc_stage<ST_X>, dim3((NY * NZ + tb - 1) / tb, grp.nf), tb, 0, g, grp, sc);
+  if (any_y) kgo<BcStage<ST_Y>, 256, 1>(L, k_bc_stage<ST_Y>, dim3((NX * NZ + tb - 1) / tb, grp.nf), tb, 0, g, grp, sc);
+  if (any_z) kgo<BcStage<ST_Z>, 256, 1>(L, k_bc_stage<ST_Z>, dim3((NX * NY + tb - 1) / tb, grp.nf), tb, 0, g, grp, sc);
 }
 
 // updt_rhs_b, src/bound.f90:341-396 (c_or_f = 'c', so q = 0): add the BC

@@ -23,7 +23,7 @@
 // data: T = double is the drop-in FP64 solve; T = float is the spectral
 // solve of the mixed form, whose accuracy an FP64 residual refinement wins
 // back (launch_poisson_mixed).
-#include "cansfz_internal.cuh"
+#include "batch.cuh"
 
 namespace cansfz {
 
@@ -341,71 +341,87 @@ __device__ __forceinline__ Bufs<T> smem_bufs(T* sm, int m, int L) {
 // (src/fillps.f90:39-50).
 // ---------------------------------------------------------------------------
 template <typename T, bool FUSED, int MC, int LC>
+struct FftXFwd {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const double* __restrict__ src, const double* __restrict__ u,
+      const double* __restrict__ v, const double* __restrict__ w, const Phys& ph, T* __restrict__ work, int Lrt) {
+    if (HALTED(sc)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
+    const int L = LC ? LC : Lrt;
+    const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
+    const int nlines = g.ny * g.nz;
+    const int l0 = bk.x * L;
+    const double dti = FUSED ? sc->dti : 0.;
+    const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
+    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+      const int line = it / n, i = it - line * n;
+      const int gl = l0 + line;
+      double x = 0.;
+      if (gl < nlines) {
+        const int j = gl % g.ny + 1, k = gl / g.ny + 1;
+        const int c = g.h(i + 1, j, k);
+        if (FUSED) {
+          x = ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * dti * g.dzfi[k] +
+                         (__ldg(v + c) - __ldg(v + c - g.sx)) * dtidyi + (__ldg(u + c) - __ldg(u + c - 1)) * dtidxi);
+        } else {
+          x = __ldg(src + c);
+        }
+      }
+      T xv = (T)x;
+      if (pl.kind == 2 && (i & 1)) xv = -xv;  // sine kind: negate odd samples
+      str<T>(B, 0, fwd_pos(pl.kind, n, i), line, xv);
+    }
+    __syncthreads();
+    line_forward<T, false, MC, LC>(pl, B, L, [&](int line, int s, T val) {
+      const int gl = l0 + line;
+      if (gl < nlines) work[(size_t)gl * n + s] = val;
+    });
+  }
+};
+template <typename T, bool FUSED, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
     const double* __restrict__ src, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ w, Phys ph, T* __restrict__ work, int Lrt) {
-  if (HALTED(sc)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
-  const int L = LC ? LC : Lrt;
-  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
-  const int nlines = g.ny * g.nz;
-  const int l0 = blockIdx.x * L;
-  const double dti = FUSED ? sc->dti : 0.;
-  const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
-  for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
-    const int line = it / n, i = it - line * n;
-    const int gl = l0 + line;
-    double x = 0.;
-    if (gl < nlines) {
-      const int j = gl % g.ny + 1, k = gl / g.ny + 1;
-      const int c = g.h(i + 1, j, k);
-      if (FUSED) {
-        x = ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * dti * g.dzfi[k] +
-                       (__ldg(v + c) - __ldg(v + c - g.sx)) * dtidyi + (__ldg(u + c) - __ldg(u + c - 1)) * dtidxi);
-      } else {
-        x = __ldg(src + c);
-      }
-    }
-    T xv = (T)x;
-    if (pl.kind == 2 && (i & 1)) xv = -xv;  // sine kind: negate odd samples
-    str<T>(B, 0, fwd_pos(pl.kind, n, i), line, xv);
-  }
-  __syncthreads();
-  line_forward<T, false, MC, LC>(pl, B, L, [&](int line, int s, T val) {
-    const int gl = l0 + line;
-    if (gl < nlines) work[(size_t)gl * n + s] = val;
-  });
+  FftXFwd<T, FUSED, MC, LC>::run(blk_here(), g, pl, sc, src, u, v, w, ph, work, Lrt);
 }
 
 // ADD: dst += normfft * x (refinement correction) instead of dst = normfft * x
 template <typename T, bool ADD, int MC, int LC>
+struct FftXBwd {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
+      int Lrt) {
+    if (HALTED(sc)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
+    const int L = LC ? LC : Lrt;
+    const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
+    const int nlines = g.ny * g.nz;
+    const int l0 = bk.x * L;
+    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+      const int line = it / n, s = it - line * n;
+      const int gl = l0 + line;
+      str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
+    }
+    __syncthreads();
+    line_backward<T, false, MC, LC>(pl, B, L, [&](int line, int i, T val) {
+      const int gl = l0 + line;
+      if (gl < nlines) {
+        const int j = gl % g.ny + 1, k = gl / g.ny + 1;
+        const int c = g.h(i + 1, j, k);
+        if (ADD) dst[c] = dst[c] + (double)val * normfft;
+        else dst[c] = (double)val * normfft;
+      }
+    });
+  }
+};
+template <typename T, bool ADD, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
     const T* __restrict__ work, double normfft, double* __restrict__ dst, int Lrt) {
-  if (HALTED(sc)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m;
-  const int L = LC ? LC : Lrt;
-  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
-  const int nlines = g.ny * g.nz;
-  const int l0 = blockIdx.x * L;
-  for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
-    const int line = it / n, s = it - line * n;
-    const int gl = l0 + line;
-    str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
-  }
-  __syncthreads();
-  line_backward<T, false, MC, LC>(pl, B, L, [&](int line, int i, T val) {
-    const int gl = l0 + line;
-    if (gl < nlines) {
-      const int j = gl % g.ny + 1, k = gl / g.ny + 1;
-      const int c = g.h(i + 1, j, k);
-      if (ADD) dst[c] = dst[c] + (double)val * normfft;
-      else dst[c] = (double)val * normfft;
-    }
-  });
+  FftXBwd<T, ADD, MC, LC>::run(blk_here(), g, pl, sc, work, normfft, dst, Lrt);
 }
 
 // ---------------------------------------------------------------------------
@@ -413,34 +429,41 @@ __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const Dev
 // positions of one z plane; the tile is read and written row by row.
 // ---------------------------------------------------------------------------
 template <typename T, int DIR, int MC, int LC>
+struct FftY {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, T* __restrict__ work, int Lrt) {
+    if (HALTED(sc)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m, nx = g.nx;
+    const int L = LC ? LC : Lrt;
+    const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
+    const int i0 = bk.x * L, k = bk.y;
+    T* plane = work + (size_t)k * nx * n;
+    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+      const int line = it % L, j = it / L;
+      const int i = i0 + line;
+      T x = i < nx ? plane[(size_t)j * nx + i] : (T)0;
+      if (DIR > 0) {
+        if (pl.kind == 2 && (j & 1)) x = -x;
+        str<T>(B, 0, fwd_pos(pl.kind, n, j), line, x);
+      } else {
+        str<T>(B, 1, j, line, x);
+      }
+    }
+    __syncthreads();
+    auto out = [&](int line, int j, T val) {
+      const int i = i0 + line;
+      if (i < nx) plane[(size_t)j * nx + i] = val;
+    };
+    if (DIR > 0) line_forward<T, true, MC, LC>(pl, B, L, out);
+    else line_backward<T, true, MC, LC>(pl, B, L, out);
+  }
+};
+template <typename T, int DIR, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
                                                T* __restrict__ work, int Lrt) {
-  if (HALTED(sc)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  const int n = MC ? 2 * MC : pl.n, m = MC ? MC : pl.m, nx = g.nx;
-  const int L = LC ? LC : Lrt;
-  const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
-  const int i0 = blockIdx.x * L, k = blockIdx.y;
-  T* plane = work + (size_t)k * nx * n;
-  for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
-    const int line = it % L, j = it / L;
-    const int i = i0 + line;
-    T x = i < nx ? plane[(size_t)j * nx + i] : (T)0;
-    if (DIR > 0) {
-      if (pl.kind == 2 && (j & 1)) x = -x;
-      str<T>(B, 0, fwd_pos(pl.kind, n, j), line, x);
-    } else {
-      str<T>(B, 1, j, line, x);
-    }
-  }
-  __syncthreads();
-  auto out = [&](int line, int j, T val) {
-    const int i = i0 + line;
-    if (i < nx) plane[(size_t)j * nx + i] = val;
-  };
-  if (DIR > 0) line_forward<T, true, MC, LC>(pl, B, L, out);
-  else line_backward<T, true, MC, LC>(pl, B, L, out);
+  FftY<T, DIR, MC, LC>::run(blk_here(), g, pl, sc, work, Lrt);
 }
 
 // ---------------------------------------------------------------------------
@@ -546,49 +569,222 @@ __device__ void thomas_column(int n, const double* __restrict__ a, const double*
   }
 }
 
+// The elimination factors of one column, z(l) = 1/pivot(l) and
+// d(l) = c(l)*z(l), with the operations of the forward sweep above: they
+// depend on the matrix and the column's eigenvalue only, so they are
+// evaluated once per plan and the per-step solve reads them.
+template <typename T>
+struct ZFactors {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ lam,
+      const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c, int zsing,
+      T* __restrict__ piv, T* __restrict__ df) {
+    typedef Rn<T> R;
+    const int col = bk.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const double lm = __ldg(lam + col);
+    const bool pin = (sizeof(T) == 4) && zsing && lm == 0.;
+    T dprev = 0;
+    for (int l = 0; l < nz; ++l) {
+      const T z = piv_inv<T>(l, nz, (T)b[l], (T)lm, (T)a[l], dprev, pin);
+      const T d = R::mul((T)c[l], z);
+      piv[(size_t)l * ncol + col] = z;
+      df[(size_t)l * ncol + col] = d;
+      dprev = d;
+    }
+  }
+};
+template <typename T>
+__global__ void __launch_bounds__(128) k_z_factors(int ncol, int nz, const double* __restrict__ lam,
+    const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c, int zsing,
+    T* __restrict__ piv, T* __restrict__ df) {
+  ZFactors<T>::run(blk_here(), ncol, nz, lam, a, b, c, zsing, piv, df);
+}
+
+// The solve of thomas_column with the factors read instead of evaluated:
+// the same products and differences, so the same result bit for bit.  Each
+// chunk's column values and factors are loaded one chunk ahead.
+template <typename T>
+__device__ void thomas_factored(int n, const double* __restrict__ a, const T* __restrict__ piv,
+                                const T* __restrict__ df, T* __restrict__ col, size_t st) {
+  typedef Rn<T> R;
+  T pprev = 0;
+  const int nch = (n + ZCH - 1) / ZCH;
+  T pv[ZCH], zv[ZCH], nx[ZCH], nz_[ZCH];
+#pragma unroll
+  for (int q = 0; q < ZCH; ++q) {
+    pv[q] = (q < n) ? col[(size_t)q * st] : (T)0;
+    zv[q] = (q < n) ? piv[(size_t)q * st] : (T)0;
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    const int k0 = ch * ZCH, k1 = k0 + ZCH;
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) {
+      nx[q] = (k1 + q < n) ? col[(size_t)(k1 + q) * st] : (T)0;
+      nz_[q] = (k1 + q < n) ? piv[(size_t)(k1 + q) * st] : (T)0;
+    }
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) {
+      const int l = k0 + q;
+      if (l < n) {
+        const T pn = (l == 0) ? R::mul(pv[q], zv[q]) : R::mul(R::sub(pv[q], R::mul((T)a[l], pprev)), zv[q]);
+        pprev = pn;
+        pv[q] = pn;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) {
+      if (k0 + q < n) col[(size_t)(k0 + q) * st] = pv[q];
+      pv[q] = nx[q];
+      zv[q] = nz_[q];
+    }
+  }
+  // backward substitution from the top chunk down, the next lower chunk's
+  // values and factors loaded ahead
+  T pnext = 0;
+  const int top = nch - 1;
+#pragma unroll
+  for (int q = 0; q < ZCH; ++q) {
+    const int l = top * ZCH + q;
+    pv[q] = (l < n) ? col[(size_t)l * st] : (T)0;
+    zv[q] = (l < n) ? df[(size_t)l * st] : (T)0;
+  }
+  for (int ch = top; ch >= 0; --ch) {
+    const int k0 = ch * ZCH, km = k0 - ZCH;
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) {
+      nx[q] = (km >= 0) ? col[(size_t)(km + q) * st] : (T)0;
+      nz_[q] = (km >= 0) ? df[(size_t)(km + q) * st] : (T)0;
+    }
+#pragma unroll
+    for (int q = ZCH - 1; q >= 0; --q) {
+      const int l = k0 + q;
+      if (l < n) {
+        if (l < n - 1) pv[q] = R::sub(pv[q], R::mul(zv[q], pnext));
+        pnext = pv[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < ZCH; ++q) {
+      if (k0 + q < n) col[(size_t)(k0 + q) * st] = pv[q];
+      pv[q] = nx[q];
+      zv[q] = nz_[q];
+    }
+  }
+}
+
+template <typename T>
+struct ZSolveF {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ a,
+      const T* __restrict__ piv, const T* __restrict__ df, const DevScalars* __restrict__ sc,
+      T* __restrict__ work) {
+    if (HALTED(sc)) return;
+    const int col = bk.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    thomas_factored<T>(nz, a, piv + col, df + col, work + col, (size_t)ncol);
+  }
+};
+template <typename T>
+__global__ void __launch_bounds__(128) k_zsolve_f(int ncol, int nz, const double* __restrict__ a,
+    const T* __restrict__ piv, const T* __restrict__ df, const DevScalars* __restrict__ sc, T* __restrict__ work) {
+  ZSolveF<T>::run(blk_here(), ncol, nz, a, piv, df, sc, work);
+}
+
+template <typename T>
+struct ZSolve {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ lam,
+      const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+      const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
+    if (HALTED(sc)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* dchk = reinterpret_cast<T*>(smraw);  // [nch][blockDim]
+    const int col = bk.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const double lm = __ldg(lam + col);
+    const bool pin = (sizeof(T) == 4) && zsing && lm == 0.;
+    thomas_column<T>(nz, a, b, c, (T)lm, work + col, (size_t)ncol, dchk + threadIdx.x, blockDim.x, pin);
+  }
+};
 template <typename T>
 __global__ void __launch_bounds__(128) k_zsolve(int ncol, int nz, const double* __restrict__ lam,
     const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
     const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
-  if (HALTED(sc)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* dchk = reinterpret_cast<T*>(smraw);  // [nch][blockDim]
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncol) return;
-  const double lm = __ldg(lam + col);
-  const bool pin = (sizeof(T) == 4) && zsing && lm == 0.;
-  thomas_column<T>(nz, a, b, c, (T)lm, work + col, (size_t)ncol, dchk + threadIdx.x, blockDim.x, pin);
+  ZSolve<T>::run(blk_here(), ncol, nz, lam, a, b, c, sc, work, zsing);
 }
 
 // periodic z: gaussel_periodic (src/solver.f90:107-149)
 template <typename T>
+struct ZSolvePeriodic {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ lam,
+      const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+      const DevScalars* __restrict__ sc, T* __restrict__ work, T* __restrict__ work2) {
+    if (HALTED(sc)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* dchk = reinterpret_cast<T*>(smraw);
+    const int col = bk.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int n = nz;
+    const double lmd = __ldg(lam + col);
+    const T lm = (T)lmd;
+    T* p = work + col;
+    T* p2 = work2 + col;
+    const size_t st = (size_t)ncol;
+    // p1 = solution of the (n-1) system with the RHS, in place
+    thomas_column<T>(n - 1, a, b, c, lm, p, st, dchk + threadIdx.x, blockDim.x, false);
+    // p2 = solution with the spike RHS
+    for (int k = 0; k < n - 1; ++k) p2[(size_t)k * st] = 0;
+    p2[0] = (T)-a[0];
+    p2[(size_t)(n - 2) * st] = (T)-c[n - 2];
+    thomas_column<T>(n - 1, a, b, c, lm, p2, st, dchk + threadIdx.x, blockDim.x, false);
+    const T bbn = (T)b[n - 1] + lm;
+    const T den = bbn + (T)c[n - 1] * p2[0] + (T)a[n - 1] * p2[(size_t)(n - 2) * st] + (T)CANSFZ_EPS;
+    T pn = (p[(size_t)(n - 1) * st] - (T)c[n - 1] * p[0] - (T)a[n - 1] * p[(size_t)(n - 2) * st]) / den;
+    if (sizeof(T) == 4 && lmd == 0.) pn = 0;  // FP32: pin the singular mode
+    p[(size_t)(n - 1) * st] = pn;
+    for (int k = 0; k < n - 1; ++k) p[(size_t)k * st] = p[(size_t)k * st] + p2[(size_t)k * st] * pn;
+  }
+};
+template <typename T>
 __global__ void __launch_bounds__(128) k_zsolve_periodic(int ncol, int nz, const double* __restrict__ lam,
     const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
     const DevScalars* __restrict__ sc, T* __restrict__ work, T* __restrict__ work2) {
-  if (HALTED(sc)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* dchk = reinterpret_cast<T*>(smraw);
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncol) return;
-  const int n = nz;
-  const double lmd = __ldg(lam + col);
-  const T lm = (T)lmd;
-  T* p = work + col;
-  T* p2 = work2 + col;
-  const size_t st = (size_t)ncol;
-  // p1 = solution of the (n-1) system with the RHS, in place
-  thomas_column<T>(n - 1, a, b, c, lm, p, st, dchk + threadIdx.x, blockDim.x, false);
-  // p2 = solution with the spike RHS
-  for (int k = 0; k < n - 1; ++k) p2[(size_t)k * st] = 0;
-  p2[0] = (T)-a[0];
-  p2[(size_t)(n - 2) * st] = (T)-c[n - 2];
-  thomas_column<T>(n - 1, a, b, c, lm, p2, st, dchk + threadIdx.x, blockDim.x, false);
-  const T bbn = (T)b[n - 1] + lm;
-  const T den = bbn + (T)c[n - 1] * p2[0] + (T)a[n - 1] * p2[(size_t)(n - 2) * st] + (T)CANSFZ_EPS;
-  T pn = (p[(size_t)(n - 1) * st] - (T)c[n - 1] * p[0] - (T)a[n - 1] * p[(size_t)(n - 2) * st]) / den;
-  if (sizeof(T) == 4 && lmd == 0.) pn = 0;  // FP32: pin the singular mode
-  p[(size_t)(n - 1) * st] = pn;
-  for (int k = 0; k < n - 1; ++k) p[(size_t)k * st] = p[(size_t)k * st] + p2[(size_t)k * st] * pn;
+  ZSolvePeriodic<T>::run(blk_here(), ncol, nz, lam, a, b, c, sc, work, work2);
+}
+
+// periodic z with the precomputed factors (those of the first n-1 levels)
+template <typename T>
+struct ZSolvePeriodicF {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ lam,
+      const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+      const T* __restrict__ piv, const T* __restrict__ df, const DevScalars* __restrict__ sc,
+      T* __restrict__ work, T* __restrict__ work2) {
+    if (HALTED(sc)) return;
+    const int col = bk.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int n = nz;
+    const double lmd = __ldg(lam + col);
+    const T lm = (T)lmd;
+    T* p = work + col;
+    T* p2 = work2 + col;
+    const size_t st = (size_t)ncol;
+    thomas_factored<T>(n - 1, a, piv + col, df + col, p, st);
+    for (int k = 0; k < n - 1; ++k) p2[(size_t)k * st] = 0;
+    p2[0] = (T)-a[0];
+    p2[(size_t)(n - 2) * st] = (T)-c[n - 2];
+    thomas_factored<T>(n - 1, a, piv + col, df + col, p2, st);
+    const T bbn = (T)b[n - 1] + lm;
+    const T den = bbn + (T)c[n - 1] * p2[0] + (T)a[n - 1] * p2[(size_t)(n - 2) * st] + (T)CANSFZ_EPS;
+    T pn = (p[(size_t)(n - 1) * st] - (T)c[n - 1] * p[0] - (T)a[n - 1] * p[(size_t)(n - 2) * st]) / den;
+    if (sizeof(T) == 4 && lmd == 0.) pn = 0;  // FP32: pin the singular mode
+    p[(size_t)(n - 1) * st] = pn;
+    for (int k = 0; k < n - 1; ++k) p[(size_t)k * st] = p[(size_t)k * st] + p2[(size_t)k * st] * pn;
+  }
+};
+template <typename T>
+__global__ void __launch_bounds__(128) k_zsolve_periodic_f(int ncol, int nz, const double* __restrict__ lam,
+    const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+    const T* __restrict__ piv, const T* __restrict__ df, const DevScalars* __restrict__ sc, T* __restrict__ work,
+    T* __restrict__ work2) {
+  ZSolvePeriodicF<T>::run(blk_here(), ncol, nz, lam, a, b, c, piv, df, sc, work, work2);
 }
 
 // ---------------------------------------------------------------------------
@@ -597,19 +793,25 @@ __global__ void __launch_bounds__(128) k_zsolve_periodic(int ncol, int nz, const
 // src/debug.f90:100-106).  res = rhs - L(phi) on the interior; phi's ghost
 // layer must be filled (boundp) before.
 // ---------------------------------------------------------------------------
+struct Residual {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const DevScalars* __restrict__ sc,
+      const double* __restrict__ rhs, const double* __restrict__ phi, double* __restrict__ res) {
+    if (HALTED(sc)) return;
+    const int i = bk.x * blockDim.x + threadIdx.x + 1;
+    if (i > g.nx) return;
+    const int j = bk.y + 1, k = bk.z + 1;
+    const int c = g.h(i, j, k);
+    const double pc = __ldg(phi + c);
+    const double lap = (__ldg(phi + c + 1) - 2. * pc + __ldg(phi + c - 1)) * (g.dxi * g.dxi) +
+                       (__ldg(phi + c + g.sx) - 2. * pc + __ldg(phi + c - g.sx)) * (g.dyi * g.dyi) +
+                       ((__ldg(phi + c + g.sxy) - pc) * g.dzci[k] - (pc - __ldg(phi + c - g.sxy)) * g.dzci[k - 1]) *
+                           g.dzfi[k];
+    res[c] = __ldg(rhs + c) - lap;
+  }
+};
 __global__ void k_residual(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ rhs,
                            const double* __restrict__ phi, double* __restrict__ res) {
-  if (HALTED(sc)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i > g.nx) return;
-  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-  const int c = g.h(i, j, k);
-  const double pc = __ldg(phi + c);
-  const double lap = (__ldg(phi + c + 1) - 2. * pc + __ldg(phi + c - 1)) * (g.dxi * g.dxi) +
-                     (__ldg(phi + c + g.sx) - 2. * pc + __ldg(phi + c - g.sx)) * (g.dyi * g.dyi) +
-                     ((__ldg(phi + c + g.sxy) - pc) * g.dzci[k] - (pc - __ldg(phi + c - g.sxy)) * g.dzci[k - 1]) *
-                         g.dzfi[k];
-  res[c] = __ldg(rhs + c) - lap;
+  Residual::run(blk_here(), g, sc, rhs, phi, res);
 }
 
 // ---------------------------------------------------------------------------
@@ -622,11 +824,14 @@ constexpr int lines_per_cta(int m, int maxL, int tsize) {
   return L;
 }
 constexpr int x_maxL(int m) { return 2 * m >= 128 ? 8 : 32; }
-constexpr int y_maxL() { return 16; }
+// y lines per CTA: 16, and more for very short lines (ny = 2 in the 2-D
+// convention), which would otherwise leave most threads of a CTA idle and
+// launch nx/16 * nz CTAs of a few points each
+constexpr int y_maxL(int m) { return 2 * m >= 32 ? 16 : (2 * m >= 8 ? 64 : 256); }
 template <typename T, int MC>
 constexpr int xL() { return MC ? lines_per_cta(MC, x_maxL(MC), sizeof(T)) : 0; }
 template <typename T, int MC>
-constexpr int yL() { return MC ? lines_per_cta(MC, y_maxL(), sizeof(T)) : 0; }
+constexpr int yL() { return MC ? lines_per_cta(MC, y_maxL(MC), sizeof(T)) : 0; }
 
 // the compile-time complex lengths (real lines of 32 to 512 points with
 // factors 2 and 3); other lengths take the runtime-length kernels
@@ -670,11 +875,11 @@ static void x_forward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl,
   const dim3 grid((nlines + L - 1) / L);
   Phys pz{};
   if (fused)
-    k_fft_x_fwd<T, true, MC, xL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, nullptr, u, v, w, *ph,
-                                                                       wbuf<T>(pl), L);
+    kgo<FftXFwd<T, true, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_fwd<T, true, MC, xL<T, MC>()>, grid, 256, smem, g,
+                                                   pl.px, sc, nullptr, u, v, w, *ph, wbuf<T>(pl), L);
   else
-    k_fft_x_fwd<T, false, MC, xL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.px, sc, src, nullptr, nullptr,
-                                                                        nullptr, pz, wbuf<T>(pl), L);
+    kgo<FftXFwd<T, false, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_fwd<T, false, MC, xL<T, MC>()>, grid, 256, smem, g,
+                                                    pl.px, sc, src, nullptr, nullptr, nullptr, pz, wbuf<T>(pl), L);
 }
 
 template <typename T>
@@ -692,11 +897,15 @@ static void x_forward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, con
 template <typename T, int MC>
 static void y_pass_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
   const int m = pl.py.m < 1 ? 1 : pl.py.m;
-  const int L = MC ? yL<T, MC>() : lines_per_cta(m, y_maxL(), sizeof(T));
+  const int L = MC ? yL<T, MC>() : lines_per_cta(m, y_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const dim3 grid((g.nx + L - 1) / L, g.nz);
-  if (dir > 0) k_fft_y<T, 1, MC, yL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
-  else k_fft_y<T, -1, MC, yL<T, MC>()><<<grid, 256, smem, Lc.st>>>(g, pl.py, sc, wbuf<T>(pl), L);
+  if (dir > 0)
+    kgo<FftY<T, 1, MC, yL<T, MC>()>, 256, 1>(Lc, k_fft_y<T, 1, MC, yL<T, MC>()>, grid, 256, smem, g, pl.py, sc,
+                                             wbuf<T>(pl), L);
+  else
+    kgo<FftY<T, -1, MC, yL<T, MC>()>, 256, 1>(Lc, k_fft_y<T, -1, MC, yL<T, MC>()>, grid, 256, smem, g, pl.py, sc,
+                                              wbuf<T>(pl), L);
 }
 
 template <typename T>
@@ -709,18 +918,44 @@ static void y_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const 
   }
 }
 
+template <typename T> static const T* zpiv(const PoissonPlan& pl);
+template <> const double* zpiv<double>(const PoissonPlan& pl) { return pl.zpiv; }
+template <> const float* zpiv<float>(const PoissonPlan& pl) { return pl.zpivf; }
+template <typename T> static const T* zdf(const PoissonPlan& pl);
+template <> const double* zdf<double>(const PoissonPlan& pl) { return pl.zdf; }
+template <> const float* zdf<float>(const PoissonPlan& pl) { return pl.zdff; }
+
+void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool f32, void* piv, void* df) {
+  const int ncol = g.nx * g.ny, tb = 128;
+  if (f32)
+    k_z_factors<float><<<(ncol + tb - 1) / tb, tb, 0, L.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, pl.zsing,
+                                                             static_cast<float*>(piv), static_cast<float*>(df));
+  else
+    k_z_factors<double><<<(ncol + tb - 1) / tb, tb, 0, L.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, pl.zsing,
+                                                              static_cast<double*>(piv), static_cast<double*>(df));
+}
+
 template <typename T>
 static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
   const int tb = 128;
+  if (zpiv<T>(pl) && zdf<T>(pl)) {
+    if (pl.zper)
+      kgo<ZSolvePeriodicF<T>, 128, 1>(Lc, k_zsolve_periodic_f<T>, (ncol + tb - 1) / tb, tb, 0, ncol, g.nz, pl.lam,
+                                      pl.a, pl.b, pl.c, zpiv<T>(pl), zdf<T>(pl), sc, wbuf<T>(pl), wbuf2<T>(pl));
+    else
+      kgo<ZSolveF<T>, 128, 1>(Lc, k_zsolve_f<T>, (ncol + tb - 1) / tb, tb, 0, ncol, g.nz, pl.a, zpiv<T>(pl),
+                              zdf<T>(pl), sc, wbuf<T>(pl));
+    return;
+  }
   const int nch = (g.nz + ZCH - 1) / ZCH;
   const size_t smem = (size_t)nch * tb * sizeof(T);
   if (pl.zper)
-    k_zsolve_periodic<T><<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc,
-                                                                     wbuf<T>(pl), wbuf2<T>(pl));
+    kgo<ZSolvePeriodic<T>, 128, 1>(Lc, k_zsolve_periodic<T>, (ncol + tb - 1) / tb, tb, smem, ncol, g.nz, pl.lam,
+                                   pl.a, pl.b, pl.c, sc, wbuf<T>(pl), wbuf2<T>(pl));
   else
-    k_zsolve<T><<<(ncol + tb - 1) / tb, tb, smem, Lc.st>>>(ncol, g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl),
-                                                            pl.zsing);
+    kgo<ZSolve<T>, 128, 1>(Lc, k_zsolve<T>, (ncol + tb - 1) / tb, tb, smem, ncol, g.nz, pl.lam, pl.a, pl.b, pl.c,
+                           sc, wbuf<T>(pl), pl.zsing);
 }
 
 template <typename T, bool ADD, int MC>
@@ -730,8 +965,8 @@ static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl
   const int L = MC ? xL<T, MC>() : lines_per_cta(m, x_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
-  k_fft_x_bwd<T, ADD, MC, xL<T, MC>()><<<(nlines + L - 1) / L, 256, smem, Lc.st>>>(g, pl.px, sc, wbuf<T>(pl),
-                                                                                   pl.normfft, dst, L);
+  kgo<FftXBwd<T, ADD, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_bwd<T, ADD, MC, xL<T, MC>()>, (nlines + L - 1) / L, 256,
+                                                smem, g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L);
 }
 
 template <typename T, bool ADD>
@@ -792,7 +1027,7 @@ void launch_poisson_f32(const Launch& L, const Geo& g, const PoissonPlan& pl, co
 void launch_residual(const Launch& L, const Geo& g, const DevScalars* sc, const double* rhs, const double* phi,
                      double* res) {
   const int bx = g.nx >= 128 ? 128 : (g.nx >= 64 ? 64 : 32);
-  k_residual<<<dim3((g.nx + bx - 1) / bx, g.ny, g.nz), bx, 0, L.st>>>(g, sc, rhs, phi, res);
+  kgo<Residual, 128, 1>(L, k_residual, dim3((g.nx + bx - 1) / bx, g.ny, g.nz), bx, 0, g, sc, rhs, phi, res);
 }
 
 }  // namespace cansfz

@@ -5,7 +5,7 @@
 // loop it computes; expressions keep the reference's operation order.
 #include <cfloat>
 
-#include "cansfz_internal.cuh"
+#include "batch.cuh"
 
 namespace cansfz {
 
@@ -23,6 +23,12 @@ static inline dim3 grd_interior(const Geo& g, dim3 b) {
   if (i > (g).nx) return;                                 \
   const int j = blockIdx.y + 1;                           \
   const int k = blockIdx.z + 1;
+// the same for a kernel body run with block index bk (batch.cuh)
+#define INTERIOR_IJK_B(g, bk)                             \
+  const int i = (bk).x * blockDim.x + threadIdx.x + 1;    \
+  if (i > (g).nx) return;                                 \
+  const int j = (bk).y + 1;                               \
+  const int k = (bk).z + 1;
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 #define LD(p, q) __ldg((p) + (q))
@@ -50,38 +56,48 @@ void launch_acdi_step(const Launch& L, const Geo& g, const DevScalars* sc, bool 
 // 0..n, then the flux divergence on the interior.
 // ---------------------------------------------------------------------------
 template <typename TI, bool SDF>
+struct ThincFlux {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const DevScalars* __restrict__ sc,
+      const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+      const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
+      const TI* __restrict__ phi, const double* __restrict__ psi, TI* __restrict__ fx, TI* __restrict__ fy,
+      TI* __restrict__ fz) {
+    typedef TI T;  // FP64 in the drop-in, FP32 in the mixed form
+    if (HALTED(sc)) return;
+    const int i = bk.x * blockDim.x + threadIdx.x;  // 0..n
+    if (i > g.nx) return;
+    const int j = bk.y, k = bk.z;
+    const T beta = (T)sc->beta;
+    const int c = g.h(i, j, k);
+    const T vel_x = (T)LD(u, c), vel_y = (T)LD(v, c), vel_z = (T)LD(w, c);
+    int ci, cj, ck;
+    T xx, yy, zz;
+    if (vel_x > T(0.)) { ci = c; xx = T(0.5); } else { ci = c + 1; xx = T(-0.5); }
+    if (vel_y > T(0.)) { cj = c; yy = T(0.5); } else { cj = c + g.sx; yy = T(-0.5); }
+    if (vel_z > T(0.)) { ck = c; zz = T(0.5); } else { ck = c + g.sxy; zz = T(-0.5); }
+    const T lnormx_x = LD(nx_, ci), lnormy_y = LD(ny_, cj), lnormz_z = LD(nz_, ck);
+    T d_x, d_y, d_z;
+    if (SDF) {
+      d_x = LD(phi, ci); d_y = LD(phi, cj); d_z = LD(phi, ck);
+    } else {
+      const T hb = T(-.5) / beta;
+      d_x = hb * log(T(1.) / ((T)LD(psi, ci) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
+      d_y = hb * log(T(1.) / ((T)LD(psi, cj) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
+      d_z = hb * log(T(1.) / ((T)LD(psi, ck) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
+    }
+    const T m2b = T(-2.) * beta;
+    fx[c] = vel_x * (T(1.) / (T(1.) + exp(m2b * (lnormx_x * xx + d_x))));
+    fy[c] = vel_y * (T(1.) / (T(1.) + exp(m2b * (lnormy_y * yy + d_y))));
+    fz[c] = vel_z * (T(1.) / (T(1.) + exp(m2b * (lnormz_z * zz + d_z))));
+  }
+};
+template <typename TI, bool SDF>
 __global__ void k_thinc_flux(Geo g, const DevScalars* __restrict__ sc,
     const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
     const TI* __restrict__ phi, const double* __restrict__ psi,
     TI* __restrict__ fx, TI* __restrict__ fy, TI* __restrict__ fz) {
-  typedef TI T;  // FP64 in the drop-in, FP32 in the mixed form
-  if (HALTED(sc)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 0..n
-  if (i > g.nx) return;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const T beta = (T)sc->beta;
-  const int c = g.h(i, j, k);
-  const T vel_x = (T)LD(u, c), vel_y = (T)LD(v, c), vel_z = (T)LD(w, c);
-  int ci, cj, ck;
-  T xx, yy, zz;
-  if (vel_x > T(0.)) { ci = c; xx = T(0.5); } else { ci = c + 1; xx = T(-0.5); }
-  if (vel_y > T(0.)) { cj = c; yy = T(0.5); } else { cj = c + g.sx; yy = T(-0.5); }
-  if (vel_z > T(0.)) { ck = c; zz = T(0.5); } else { ck = c + g.sxy; zz = T(-0.5); }
-  const T lnormx_x = LD(nx_, ci), lnormy_y = LD(ny_, cj), lnormz_z = LD(nz_, ck);
-  T d_x, d_y, d_z;
-  if (SDF) {
-    d_x = LD(phi, ci); d_y = LD(phi, cj); d_z = LD(phi, ck);
-  } else {
-    const T hb = T(-.5) / beta;
-    d_x = hb * log(T(1.) / ((T)LD(psi, ci) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
-    d_y = hb * log(T(1.) / ((T)LD(psi, cj) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
-    d_z = hb * log(T(1.) / ((T)LD(psi, ck) + T(CANSFZ_EPS)) - T(1.) + T(CANSFZ_EPS));
-  }
-  const T m2b = T(-2.) * beta;
-  fx[c] = vel_x * (T(1.) / (T(1.) + exp(m2b * (lnormx_x * xx + d_x))));
-  fy[c] = vel_y * (T(1.) / (T(1.) + exp(m2b * (lnormy_y * yy + d_y))));
-  fz[c] = vel_z * (T(1.) / (T(1.) + exp(m2b * (lnormz_z * zz + d_z))));
+  ThincFlux<TI, SDF>::run(blk_here(), g, sc, u, v, w, nx_, ny_, nz_, phi, psi, fx, fy, fz);
 }
 
 __global__ void k_thinc_div(Geo g, const DevScalars* __restrict__ sc, const double* __restrict__ fx,
@@ -96,19 +112,27 @@ __global__ void k_thinc_div(Geo g, const DevScalars* __restrict__ sc, const doub
 
 // flux divergence + rk_2fl update (history in place), src/vof_thinc_qq.f90:122-132, src/rk.f90:240-248
 template <typename TI>
+struct ThincDivUpdate {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const DevScalars* __restrict__ sc,
+      const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz,
+      const double* __restrict__ psi, TI* __restrict__ hist, double* __restrict__ psi_out) {
+    typedef TI T;
+    if (HALTED(sc)) return;
+    INTERIOR_IJK_B(g, bk)
+    const int c = g.h(i, j, k), t = g.t(i, j, k);
+    const T d = -((T)g.dxi * (LD(fx, c) - LD(fx, c - 1)) + (T)g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
+                  (T)g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
+    const T dO = sc->first_rk2fl ? d : hist[t];
+    psi_out[c] = fmin(fmax(0., LD(psi, c) + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
+    hist[t] = d;
+  }
+};
+template <typename TI>
 __global__ void k_thinc_div_update(Geo g, const DevScalars* __restrict__ sc, const TI* __restrict__ fx,
                                    const TI* __restrict__ fy, const TI* __restrict__ fz,
                                    const double* __restrict__ psi, TI* __restrict__ hist,
                                    double* __restrict__ psi_out) {
-  typedef TI T;
-  if (HALTED(sc)) return;
-  INTERIOR_IJK(g)
-  const int c = g.h(i, j, k), t = g.t(i, j, k);
-  const T d = -((T)g.dxi * (LD(fx, c) - LD(fx, c - 1)) + (T)g.dyi * (LD(fy, c) - LD(fy, c - g.sx)) +
-                (T)g.dzfi[k] * (LD(fz, c) - LD(fz, c - g.sxy)));
-  const T dO = sc->first_rk2fl ? d : hist[t];
-  psi_out[c] = fmin(fmax(0., LD(psi, c) + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
-  hist[t] = d;
+  ThincDivUpdate<TI>::run(blk_here(), g, sc, fx, fy, fz, psi, hist, psi_out);
 }
 
 template <typename TI>
@@ -116,10 +140,12 @@ void launch_thinc_step_t(const Launch& L, const Geo& g, const DevScalars* sc, bo
                          const double* v, const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi,
                          const double* psi, double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
   dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
-  if (sdf) k_thinc_flux<TI, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
-  else k_thinc_flux<TI, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  if (sdf) kgo<ThincFlux<TI, true>, 128, 1>(L, k_thinc_flux<TI, true>, gr, b, 0, g, sc, u, v, w, nx, ny, nz, phi, psi,
+      fx, fy, fz);
+  else kgo<ThincFlux<TI, false>, 128, 1>(L, k_thinc_flux<TI, false>, gr, b, 0, g, sc, u, v, w, nx, ny, nz, phi, psi,
+      fx, fy, fz);
   dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
-  k_thinc_div_update<TI><<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, psi, hist, psi_out);
+  kgo<ThincDivUpdate<TI>, 128, 1>(L, k_thinc_div_update<TI>, gi, bi, 0, g, sc, fx, fy, fz, psi, hist, psi_out);
 }
 template void launch_thinc_step_t<float>(const Launch&, const Geo&, const DevScalars*, bool, const double*,
                                          const double*, const double*, const float*, const float*, const float*,
@@ -137,8 +163,10 @@ void launch_thinc_transport(const Launch& L, const Geo& g, const DevScalars* sc,
                             const double* ny, const double* nz, const double* phi, const double* psi,
                             double* dpsidt, double* fx, double* fy, double* fz) {
   dim3 b(g.nx + 1 >= 128 ? 128 : 64), gr((g.nx + 1 + b.x - 1) / b.x, g.ny + 1, g.nz + 1);
-  if (sdf) k_thinc_flux<double, true><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
-  else k_thinc_flux<double, false><<<gr, b, 0, L.st>>>(g, sc, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+  if (sdf) kgo<ThincFlux<double, true>, 128, 1>(L, k_thinc_flux<double, true>, gr, b, 0, g, sc, u, v, w, nx, ny, nz,
+      phi, psi, fx, fy, fz);
+  else kgo<ThincFlux<double, false>, 128, 1>(L, k_thinc_flux<double, false>, gr, b, 0, g, sc, u, v, w, nx, ny, nz,
+      phi, psi, fx, fy, fz);
   dim3 bi = blk_interior(g), gi = grd_interior(g, bi);
   k_thinc_div<<<gi, bi, 0, L.st>>>(g, sc, fx, fy, fz, dpsidt);
 }
@@ -170,40 +198,54 @@ void launch_psi_update(const Launch& L, const Geo& g, const DevScalars* sc, cons
 // (src/vof_thinc_qq.f90:135-157): whole halo array
 // ---------------------------------------------------------------------------
 template <bool ACDI, typename TO>
+struct CmptPhi {
+  static __device__ __forceinline__ void run(const Blk& bk, int n, const DevScalars* __restrict__ sc,
+      const double* __restrict__ psi, TO* __restrict__ phi) {
+    if (HALTED(sc)) return;
+    const int q = bk.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const double ps = LD(psi, q);
+    if (ACDI) {
+      phi[q] = (TO)(sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS)));
+    } else {
+      const double pa = fmin(fmax(ps, CANSFZ_EPS), 1. - CANSFZ_EPS);
+      phi[q] = (TO)(0.5 / sc->beta * log(pa / (1. - pa)));
+    }
+  }
+};
+template <bool ACDI, typename TO>
 __global__ void k_cmpt_phi(int n, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
                            TO* __restrict__ phi) {
-  if (HALTED(sc)) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const double ps = LD(psi, q);
-  if (ACDI) {
-    phi[q] = (TO)(sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS)));
-  } else {
-    const double pa = fmin(fmax(ps, CANSFZ_EPS), 1. - CANSFZ_EPS);
-    phi[q] = (TO)(0.5 / sc->beta * log(pa / (1. - pa)));
-  }
+  CmptPhi<ACDI, TO>::run(blk_here(), n, sc, psi, phi);
 }
 
 void launch_cmpt_phi(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
                      double* phi) {
   const int n = g.hsize();
-  if (acdi) k_cmpt_phi<true, double><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
-  else k_cmpt_phi<false, double><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  if (acdi) kgo<CmptPhi<true, double>, 256, 1>(L, k_cmpt_phi<true, double>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
+  else kgo<CmptPhi<false, double>, 256, 1>(L, k_cmpt_phi<false, double>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
 }
 // the mixed form: phi evaluated in FP64 and stored in FP32
 // (narrow_only: Youngs without SDF normals works on psi itself, stored in FP32)
+struct Narrow {
+  static __device__ __forceinline__ void run(const Blk& bk, int n, const DevScalars* __restrict__ sc,
+      const double* __restrict__ src, float* __restrict__ dst) {
+    if (HALTED(sc)) return;
+    const int q = bk.x * blockDim.x + threadIdx.x;
+    if (q < n) dst[q] = (float)src[q];
+  }
+};
 __global__ void k_narrow(int n, const DevScalars* __restrict__ sc, const double* __restrict__ src,
                          float* __restrict__ dst) {
-  if (HALTED(sc)) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) dst[q] = (float)src[q];
+  Narrow::run(blk_here(), n, sc, src, dst);
 }
 void launch_cmpt_phi_f32(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
                          float* phi, bool narrow_only) {
   const int n = g.hsize();
-  if (narrow_only) k_narrow<<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
-  else if (acdi) k_cmpt_phi<true, float><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
-  else k_cmpt_phi<false, float><<<(n + 255) / 256, 256, 0, L.st>>>(n, sc, psi, phi);
+  if (narrow_only) kgo<Narrow, 256, 1>(L, k_narrow, (n + 255) / 256, 256, 0, n, sc, psi, phi);
+  else if (acdi) kgo<CmptPhi<true, float>, 256, 1>(L, k_cmpt_phi<true, float>, (n + 255) / 256, 256, 0, n, sc, psi,
+      phi);
+  else kgo<CmptPhi<false, float>, 256, 1>(L, k_cmpt_phi<false, float>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,19 +533,26 @@ void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const 
 // ---------------------------------------------------------------------------
 // fillps, src/fillps.f90:13-51
 // ---------------------------------------------------------------------------
+struct Fillps {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
+      const DevScalars* __restrict__ sc, const double* __restrict__ u, const double* __restrict__ v,
+      const double* __restrict__ w, double* __restrict__ p) {
+    if (HALTED(sc)) return;
+    INTERIOR_IJK_B(g, bk)
+    const double dti = sc->dti, dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
+    const int c = g.h(i, j, k);
+    p[c] = ph.rho0 * ((LD(w, c) - LD(w, c - g.sxy)) * dti * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * dtidyi +
+                      (LD(u, c) - LD(u, c - 1)) * dtidxi);
+  }
+};
 __global__ void k_fillps(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ u,
                          const double* __restrict__ v, const double* __restrict__ w, double* __restrict__ p) {
-  if (HALTED(sc)) return;
-  INTERIOR_IJK(g)
-  const double dti = sc->dti, dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
-  const int c = g.h(i, j, k);
-  p[c] = ph.rho0 * ((LD(w, c) - LD(w, c - g.sxy)) * dti * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * dtidyi +
-                    (LD(u, c) - LD(u, c - 1)) * dtidxi);
+  Fillps::run(blk_here(), g, ph, sc, u, v, w, p);
 }
 void launch_fillps(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                    const double* v, const double* w, double* p) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_fillps<<<gr, b, 0, L.st>>>(g, ph, sc, u, v, w, p);
+  kgo<Fillps, 128, 1>(L, k_fillps, gr, b, 0, g, ph, sc, u, v, w, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -534,25 +583,32 @@ void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScala
 // step in one pass: both read the correction phi, and updatep needs none of
 // the velocity ghost fills that follow correc.  32x8 point tiles of the halo
 // array; pout = phi + pp on the interior (the new pressure into the po slot).
+struct CorrecUpdatep {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
+      const DevScalars* __restrict__ sc, const double* __restrict__ p, double* __restrict__ u,
+      double* __restrict__ v, double* __restrict__ w, const double* __restrict__ pp, double* __restrict__ pout) {
+    if (HALTED(sc)) return;
+    const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k = bk.z;
+    if (i > g.nx + 1 || j > g.ny + 1) return;
+    const double dt = sc->dt, rhop = ph.rho0;
+    const int c = g.h(i, j, k);
+    const double pc = LD(p, c);
+    if (i <= g.nx) u[c] = u[c] - dt * g.dxi * (LD(p, c + 1) - pc) / rhop;
+    if (j <= g.ny) v[c] = v[c] - dt * g.dyi * (LD(p, c + g.sx) - pc) / rhop;
+    if (k <= g.nz) w[c] = w[c] - dt * g.dzci[k] * (LD(p, c + g.sxy) - pc) / rhop;
+    if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz) pout[c] = pc + LD(pp, c);
+  }
+};
 __global__ void __launch_bounds__(256) k_correc_updatep(Geo g, Phys ph, const DevScalars* __restrict__ sc,
                                                         const double* __restrict__ p, double* __restrict__ u,
                                                         double* __restrict__ v, double* __restrict__ w,
                                                         const double* __restrict__ pp, double* __restrict__ pout) {
-  if (HALTED(sc)) return;
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
-  if (i > g.nx + 1 || j > g.ny + 1) return;
-  const double dt = sc->dt, rhop = ph.rho0;
-  const int c = g.h(i, j, k);
-  const double pc = LD(p, c);
-  if (i <= g.nx) u[c] = u[c] - dt * g.dxi * (LD(p, c + 1) - pc) / rhop;
-  if (j <= g.ny) v[c] = v[c] - dt * g.dyi * (LD(p, c + g.sx) - pc) / rhop;
-  if (k <= g.nz) w[c] = w[c] - dt * g.dzci[k] * (LD(p, c + g.sxy) - pc) / rhop;
-  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz) pout[c] = pc + LD(pp, c);
+  CorrecUpdatep::run(blk_here(), g, ph, sc, p, u, v, w, pp, pout);
 }
 void launch_correc_updatep(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
                            double* u, double* v, double* w, const double* pp, double* pout) {
   const dim3 b(32, 8), gr((g.nx + 2 + 31) / 32, (g.ny + 2 + 7) / 8, g.nz + 2);
-  k_correc_updatep<<<gr, b, 0, L.st>>>(g, ph, sc, p, u, v, w, pp, pout);
+  kgo<CorrecUpdatep, 256, 1>(L, k_correc_updatep, gr, b, 0, g, ph, sc, p, u, v, w, pp, pout);
 }
 
 // updatep, src/updatep.f90:13-24
@@ -576,26 +632,42 @@ void launch_updatep_full(const Launch& L, const Geo& g, const double* pp, double
   const int n = g.hsize();
   k_add_full<<<(n + 255) / 256, 256, 0, L.st>>>(n, pp, p);
 }
+struct Copy {
+  static __device__ __forceinline__ void run(const Blk& bk, size_t n, const double* __restrict__ s,
+      double* __restrict__ d) {
+    const size_t q = (size_t)bk.x * blockDim.x + threadIdx.x;
+    if (q < n) d[q] = s[q];
+  }
+};
 __global__ void k_copy(size_t n, const double* __restrict__ s, double* __restrict__ d) {
-  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) d[q] = s[q];
+  Copy::run(blk_here(), n, s, d);
 }
 void launch_copy(const Launch& L, size_t n, const double* src, double* dst) {
-  k_copy<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, src, dst);
+  kgo<Copy, 256, 1>(L, k_copy, (unsigned)((n + 255) / 256), 256, 0, n, src, dst);
 }
+struct FillV {
+  static __device__ __forceinline__ void run(const Blk& bk, size_t n, double val, double* __restrict__ d) {
+    const size_t q = (size_t)bk.x * blockDim.x + threadIdx.x;
+    if (q < n) d[q] = val;
+  }
+};
 __global__ void k_fillv(size_t n, double val, double* __restrict__ d) {
-  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) d[q] = val;
+  FillV::run(blk_here(), n, val, d);
 }
 void launch_fill(const Launch& L, size_t n, double val, double* dst) {
-  k_fillv<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, val, dst);
+  kgo<FillV, 256, 1>(L, k_fillv, (unsigned)((n + 255) / 256), 256, 0, n, val, dst);
 }
+struct FillF {
+  static __device__ __forceinline__ void run(const Blk& bk, size_t n, float val, float* __restrict__ d) {
+    const size_t q = (size_t)bk.x * blockDim.x + threadIdx.x;
+    if (q < n) d[q] = val;
+  }
+};
 __global__ void k_fillf(size_t n, float val, float* __restrict__ d) {
-  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) d[q] = val;
+  FillF::run(blk_here(), n, val, d);
 }
 void launch_fill(const Launch& L, size_t n, float val, float* dst) {
-  k_fillf<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, val, dst);
+  kgo<FillF, 256, 1>(L, k_fillf, (unsigned)((n + 255) / 256), 256, 0, n, val, dst);
 }
 __global__ void k_widen(size_t n, const float* __restrict__ s, double* __restrict__ d) {
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -793,13 +865,19 @@ __global__ void k_chkdiv_part(Geo g, DevScalars* __restrict__ sc, int only_on_ch
     part[nb + bid] = m;
   }
 }
+struct SumPartials {
+  static __device__ __forceinline__ void run(const Blk& bk, int n, const double* __restrict__ part,
+      double* __restrict__ out, DevScalars* __restrict__ sc, int only_on_check) {
+    if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
+    double s = 0.;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) s += part[q];
+    s = block_sum(s);
+    if (threadIdx.x == 0) *out = s;
+  }
+};
 __global__ void k_sum_partials(int n, const double* __restrict__ part, double* __restrict__ out,
                                DevScalars* __restrict__ sc, int only_on_check) {
-  if (HALTED(sc) || (only_on_check && !sc->check_now)) return;
-  double s = 0.;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) s += part[q];
-  s = block_sum(s);
-  if (threadIdx.x == 0) *out = s;
+  SumPartials::run(blk_here(), n, part, out, sc, only_on_check);
 }
 __device__ __forceinline__ void chkdiv_finish(double small, DevScalars* sc, double divmax, int only_on_check) {
   sc->divmax = divmax;
@@ -821,7 +899,7 @@ void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partia
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
   const int oc = only_on_check ? 1 : 0;
   k_chkdiv_part<<<gr, b, 0, L.st>>>(g, sc, oc, partial, u, v, w);
-  k_sum_partials<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, &sc->divtot, sc, oc);
+  kgo<SumPartials, 1024, 1>(L, k_sum_partials, 1, 1024, 0, (int)(gr.x * gr.y * gr.z), partial, &sc->divtot, sc, oc);
   Phys ph{};
   ph.small = CANSFZ_EPS * 1.0e7;
   k_chkdiv_final<<<1, 1024, 0, L.st>>>(ph, sc, oc, (int)(gr.x * gr.y * gr.z), partial);
@@ -837,98 +915,119 @@ void launch_chkdiv(const Launch& L, const Geo& g, DevScalars* sc, double* partia
 // (used only for its NaN test) is summed in a fixed order.
 // ---------------------------------------------------------------------------
 constexpr int kReduceThreads = 256;
+struct StepReduce {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, DevScalars* __restrict__ sc, int acdi,
+      double* __restrict__ part, const double* __restrict__ u, const double* __restrict__ v,
+      const double* __restrict__ w) {
+    if (HALTED(sc)) return;
+    const bool chk = sc->check_now != 0;
+    if (!acdi && !chk) return;
+    double velmax = 0., dtimax = 0., divsum = 0., divmax = 0.;
+    const int nrows = g.ny * g.nz;
+    for (int r = bk.x; r < nrows; r += bk.nx) {
+      const int j = r % g.ny + 1, k = r / g.ny + 1;
+      for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+        const int c = g.h(i, j, k);
+        if (acdi) {
+          const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
+          const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
+          const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
+          velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+        }
+        if (chk) {
+          dtimax = fmax(dtimax, chkdt_cell(g, i, j, k, u, v, w));
+          const double div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +
+                             (LD(u, c) - LD(u, c - 1)) * g.dxi;
+          divsum += div;
+          divmax = fmax(divmax, fabs(div));
+        }
+      }
+    }
+    velmax = block_max(velmax);
+    dtimax = block_max(dtimax);
+    divsum = block_sum(divsum);
+    divmax = block_max(divmax);
+    if (threadIdx.x == 0) {
+      const int nb = bk.nx;
+      part[bk.x] = velmax;
+      part[nb + bk.x] = dtimax;
+      part[2 * nb + bk.x] = divsum;
+      part[3 * nb + bk.x] = divmax;
+    }
+  }
+};
 __global__ void __launch_bounds__(kReduceThreads) k_step_reduce(Geo g, DevScalars* __restrict__ sc, int acdi,
                                                                 double* __restrict__ part,
                                                                 const double* __restrict__ u,
                                                                 const double* __restrict__ v,
                                                                 const double* __restrict__ w) {
-  if (HALTED(sc)) return;
-  const bool chk = sc->check_now != 0;
-  if (!acdi && !chk) return;
-  double velmax = 0., dtimax = 0., divsum = 0., divmax = 0.;
-  const int nrows = g.ny * g.nz;
-  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
-    const int j = r % g.ny + 1, k = r / g.ny + 1;
-    for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
-      const int c = g.h(i, j, k);
-      if (acdi) {
-        const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
-        const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
-        const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
-        velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
-      }
-      if (chk) {
-        dtimax = fmax(dtimax, chkdt_cell(g, i, j, k, u, v, w));
-        const double div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +
-                           (LD(u, c) - LD(u, c - 1)) * g.dxi;
-        divsum += div;
-        divmax = fmax(divmax, fabs(div));
-      }
+  StepReduce::run(blk_here(), g, sc, acdi, part, u, v, w);
+}
+struct StepReduceFinal {
+  static __device__ __forceinline__ void run(const Blk& bk, const Phys& ph, DevScalars* __restrict__ sc, int nb,
+      const double* __restrict__ part) {
+    if (HALTED(sc)) return;
+    const bool chk = sc->check_now != 0;
+    if (!ph.acdi && !chk) return;
+    const double velmax = reduce_max_partials(nb, part);
+    const double dtimax = reduce_max_partials(nb, part + nb);
+    double s = 0.;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) s += part[2 * nb + q];
+    s = block_sum(s);
+    const double divmax = reduce_max_partials(nb, part + 3 * nb);
+    if (threadIdx.x != 0) return;
+    if (ph.acdi) gamma_finish(ph, sc, velmax, 1);
+    if (chk) {
+      chkdt_finish(ph, sc, dtimax, 1);
+      sc->divtot = s;
+      chkdiv_finish(CANSFZ_EPS * 1.0e7, sc, divmax, 1);
     }
   }
-  velmax = block_max(velmax);
-  dtimax = block_max(dtimax);
-  divsum = block_sum(divsum);
-  divmax = block_max(divmax);
-  if (threadIdx.x == 0) {
-    const int nb = gridDim.x;
-    part[blockIdx.x] = velmax;
-    part[nb + blockIdx.x] = dtimax;
-    part[2 * nb + blockIdx.x] = divsum;
-    part[3 * nb + blockIdx.x] = divmax;
-  }
-}
+};
 __global__ void k_step_reduce_final(Phys ph, DevScalars* __restrict__ sc, int nb, const double* __restrict__ part) {
-  if (HALTED(sc)) return;
-  const bool chk = sc->check_now != 0;
-  if (!ph.acdi && !chk) return;
-  const double velmax = reduce_max_partials(nb, part);
-  const double dtimax = reduce_max_partials(nb, part + nb);
-  double s = 0.;
-  for (int q = threadIdx.x; q < nb; q += blockDim.x) s += part[2 * nb + q];
-  s = block_sum(s);
-  const double divmax = reduce_max_partials(nb, part + 3 * nb);
-  if (threadIdx.x != 0) return;
-  if (ph.acdi) gamma_finish(ph, sc, velmax, 1);
-  if (chk) {
-    chkdt_finish(ph, sc, dtimax, 1);
-    sc->divtot = s;
-    chkdiv_finish(CANSFZ_EPS * 1.0e7, sc, divmax, 1);
-  }
+  StepReduceFinal::run(blk_here(), ph, sc, nb, part);
 }
 void launch_step_reductions(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                             const double* u, const double* v, const double* w) {
   const int nrows = g.ny * g.nz;
   int nb = (L.nsm > 0 ? L.nsm : 148) * 8;
   if (nb > nrows) nb = nrows;
-  k_step_reduce<<<nb, kReduceThreads, 0, L.st>>>(g, sc, ph.acdi, partial, u, v, w);
-  k_step_reduce_final<<<1, 1024, 0, L.st>>>(ph, sc, nb, partial);
+  kgo<StepReduce, 256, 1>(L, k_step_reduce, nb, kReduceThreads, 0, g, sc, ph.acdi, partial, u, v, w);
+  kgo<StepReduceFinal, 1024, 1>(L, k_step_reduce_final, 1, 1024, 0, ph, sc, nb, partial);
 }
 
 // bulk_mean_12_stag, src/utils.f90:68-136
+struct BulkPart {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
+      const DevScalars* __restrict__ sc, int idir, const double* __restrict__ gvr, const double* __restrict__ psi,
+      double* __restrict__ part) {
+    if (HALTED(sc)) return;
+    const int i = bk.x * blockDim.x + threadIdx.x + 1;
+    const int j = bk.y + 1, k = bk.z + 1;
+    double s = 0.;
+    if (i <= g.nx) {
+      const int c = g.h(i, j, k);
+      double pl;
+      if (idir == 1) pl = 0.5 * (LD(psi, c + 1) + LD(psi, c));
+      else if (idir == 2) pl = 0.5 * (LD(psi, c + g.sx) + LD(psi, c));
+      else pl = 0.5 * (LD(psi, c + g.sxy) + LD(psi, c));
+      s = (pl * ph.rho12[0] + (1. - pl) * ph.rho12[1]) * gvr[k];
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[bk.x + bk.nx * (bk.y + bk.ny * bk.z)] = s;
+  }
+};
 __global__ void k_bulk_part(Geo g, Phys ph, const DevScalars* __restrict__ sc, int idir,
                             const double* __restrict__ gvr, const double* __restrict__ psi,
                             double* __restrict__ part) {
-  if (HALTED(sc)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-  double s = 0.;
-  if (i <= g.nx) {
-    const int c = g.h(i, j, k);
-    double pl;
-    if (idir == 1) pl = 0.5 * (LD(psi, c + 1) + LD(psi, c));
-    else if (idir == 2) pl = 0.5 * (LD(psi, c + g.sx) + LD(psi, c));
-    else pl = 0.5 * (LD(psi, c + g.sxy) + LD(psi, c));
-    s = (pl * ph.rho12[0] + (1. - pl) * ph.rho12[1]) * gvr[k];
-  }
-  s = block_sum(s);
-  if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+  BulkPart::run(blk_here(), g, ph, sc, idir, gvr, psi, part);
 }
 void launch_bulk_mean(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial, int idir,
                       const double* gvr, const double* psi) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_bulk_part<<<gr, b, 0, L.st>>>(g, ph, sc, idir, gvr, psi, partial);
-  k_sum_partials<<<1, 1024, 0, L.st>>>((int)(gr.x * gr.y * gr.z), partial, &sc->rho_av[idir - 1], sc, 0);
+  kgo<BulkPart, 128, 1>(L, k_bulk_part, gr, b, 0, g, ph, sc, idir, gvr, psi, partial);
+  kgo<SumPartials, 1024, 1>(L, k_sum_partials, 1, 1024, 0, (int)(gr.x * gr.y * gr.z), partial, &sc->rho_av[idir - 1],
+      sc, 0);
 }
 
 // cmpt_mean_mass, src/output.f90:759-790
@@ -968,33 +1067,43 @@ void launch_mass(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, 
 // ---------------------------------------------------------------------------
 // step bookkeeping, src/main.f90:414-425 and :515-529
 // ---------------------------------------------------------------------------
+struct StepBegin {
+  static __device__ __forceinline__ void run(const Blk& bk, DevScalars* sc, int icheck) {
+    if (sc->status != CANSFZ_OK) sc->halted = 1;
+    if (sc->halted) return;
+    sc->istep = sc->istep + 1;
+    sc->time = sc->time + sc->dt;
+    const double dt_r = sc->dt / sc->dto;
+    sc->dt_r = dt_r;
+    sc->tm1 = 1. + 0.5 * dt_r;
+    sc->tm2 = -0.5 * dt_r;
+    sc->f1 = sc->tm1 * sc->dt;
+    sc->f2 = sc->tm2 * sc->dt;
+    sc->f12 = sc->f1 + sc->f2;
+    sc->dti = 1. / sc->dt;
+    sc->check_now = (icheck > 0 && (sc->istep % icheck) == 0) ? 1 : 0;
+  }
+};
 __global__ void k_step_begin(DevScalars* sc, int icheck) {
-  if (sc->status != CANSFZ_OK) sc->halted = 1;
-  if (sc->halted) return;
-  sc->istep = sc->istep + 1;
-  sc->time = sc->time + sc->dt;
-  const double dt_r = sc->dt / sc->dto;
-  sc->dt_r = dt_r;
-  sc->tm1 = 1. + 0.5 * dt_r;
-  sc->tm2 = -0.5 * dt_r;
-  sc->f1 = sc->tm1 * sc->dt;
-  sc->f2 = sc->tm2 * sc->dt;
-  sc->f12 = sc->f1 + sc->f2;
-  sc->dti = 1. / sc->dt;
-  sc->check_now = (icheck > 0 && (sc->istep % icheck) == 0) ? 1 : 0;
+  StepBegin::run(blk_here(), sc, icheck);
 }
 void launch_step_begin(const Launch& L, DevScalars* sc, int icheck) {
-  k_step_begin<<<1, 1, 0, L.st>>>(sc, icheck);
+  kgo<StepBegin, 1, 1>(L, k_step_begin, 1, 1, 0, sc, icheck);
 }
+struct StepEnd {
+  static __device__ __forceinline__ void run(const Blk& bk, DevScalars* sc) {
+    if (sc->halted) return;
+    sc->dto = sc->dt;
+    sc->first_rk = 0;
+    sc->first_rk2fl = 0;
+  }
+};
 __global__ void k_step_end(DevScalars* sc) {
-  if (sc->halted) return;
-  sc->dto = sc->dt;
-  sc->first_rk = 0;
-  sc->first_rk2fl = 0;
+  StepEnd::run(blk_here(), sc);
 }
 void launch_step_end(const Launch& L, const Phys& ph, DevScalars* sc) {
   (void)ph;
-  k_step_end<<<1, 1, 0, L.st>>>(sc);
+  kgo<StepEnd, 1, 1>(L, k_step_end, 1, 1, 0, sc);
 }
 
 }  // namespace cansfz

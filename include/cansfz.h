@@ -280,6 +280,16 @@ int cansfz_ensemble_create(cansfz_ctx* const* cases, int ncases, void* stream, c
  * the return value is the first non-zero of them (CANSFZ_OK if none).   */
 int cansfz_ensemble_step(cansfz_ensemble* ens, int nsteps, int* status_out);
 int cansfz_ensemble_destroy(cansfz_ensemble* ens);
+/* Batched launches (off by default, cases_per_launch = 1): cases of the same
+ * grid and options (they differ only in physical parameters, initial fields
+ * and time step) run as groups of up to cases_per_launch cases whose
+ * kernels are one launch per kernel for the whole group, each case with its
+ * own arguments; results are bit for bit those of the cases' own launches.
+ * Takes effect at the next step (the step graphs are rebuilt).           */
+int cansfz_ensemble_set_batching(cansfz_ensemble* ens, int cases_per_launch);
+/* After a step: the number of groups (a case that shares its launches with
+ * no other case is a group of one) and of cases in groups of two or more. */
+int cansfz_ensemble_info(cansfz_ensemble* ens, int* ngroups, int* grouped_cases);
 
 /* ---- allocation-free Poisson solve (no reference counterpart) ---------
  * solver_gpu for callers that may not allocate device memory while they
