@@ -197,19 +197,30 @@ void launch_psi_update(const Launch& L, const Geo& g, const DevScalars* sc, cons
 // acdi_cmpt_phi (src/acdi.f90:227-248), vof_thinc_cmpt_phi
 // (src/vof_thinc_qq.f90:135-157): whole halo array
 // ---------------------------------------------------------------------------
+constexpr int kPhiPer = 4;  // points per thread of k_cmpt_phi
 template <bool ACDI, typename TO>
 struct CmptPhi {
   static __device__ __forceinline__ void run(const Blk& bk, int n, const DevScalars* __restrict__ sc,
       const double* __restrict__ psi, TO* __restrict__ phi) {
     if (HALTED(sc)) return;
-    const int q = bk.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    const double ps = LD(psi, q);
-    if (ACDI) {
-      phi[q] = (TO)(sc->seps * log((ps + CANSFZ_EPS) / (1. - ps + CANSFZ_EPS)));
-    } else {
-      const double pa = fmin(fmax(ps, CANSFZ_EPS), 1. - CANSFZ_EPS);
-      phi[q] = (TO)(0.5 / sc->beta * log(pa / (1. - pa)));
+    // kPhiPer points per thread, a block's points contiguous: loads first
+    const int q0 = bk.x * blockDim.x * kPhiPer + threadIdx.x;
+    double ps[kPhiPer];
+#pragma unroll
+    for (int m = 0; m < kPhiPer; ++m) {
+      const int q = q0 + m * blockDim.x;
+      ps[m] = q < n ? LD(psi, q) : 0.;
+    }
+#pragma unroll
+    for (int m = 0; m < kPhiPer; ++m) {
+      const int q = q0 + m * blockDim.x;
+      if (q >= n) break;
+      if (ACDI) {
+        phi[q] = (TO)(sc->seps * log((ps[m] + CANSFZ_EPS) / (1. - ps[m] + CANSFZ_EPS)));
+      } else {
+        const double pa = fmin(fmax(ps[m], CANSFZ_EPS), 1. - CANSFZ_EPS);
+        phi[q] = (TO)(0.5 / sc->beta * log(pa / (1. - pa)));
+      }
     }
   }
 };
@@ -222,8 +233,9 @@ __global__ void k_cmpt_phi(int n, const DevScalars* __restrict__ sc, const doubl
 void launch_cmpt_phi(const Launch& L, const Geo& g, const DevScalars* sc, bool acdi, const double* psi,
                      double* phi) {
   const int n = g.hsize();
-  if (acdi) kgo<CmptPhi<true, double>, 256, 1>(L, k_cmpt_phi<true, double>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
-  else kgo<CmptPhi<false, double>, 256, 1>(L, k_cmpt_phi<false, double>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
+  const int nb = (n + 256 * kPhiPer - 1) / (256 * kPhiPer);
+  if (acdi) kgo<CmptPhi<true, double>, 256, 1>(L, k_cmpt_phi<true, double>, nb, 256, 0, n, sc, psi, phi);
+  else kgo<CmptPhi<false, double>, 256, 1>(L, k_cmpt_phi<false, double>, nb, 256, 0, n, sc, psi, phi);
 }
 // the mixed form: phi evaluated in FP64 and stored in FP32
 // (narrow_only: Youngs without SDF normals works on psi itself, stored in FP32)
@@ -243,9 +255,12 @@ void launch_cmpt_phi_f32(const Launch& L, const Geo& g, const DevScalars* sc, bo
                          float* phi, bool narrow_only) {
   const int n = g.hsize();
   if (narrow_only) kgo<Narrow, 256, 1>(L, k_narrow, (n + 255) / 256, 256, 0, n, sc, psi, phi);
-  else if (acdi) kgo<CmptPhi<true, float>, 256, 1>(L, k_cmpt_phi<true, float>, (n + 255) / 256, 256, 0, n, sc, psi,
-      phi);
-  else kgo<CmptPhi<false, float>, 256, 1>(L, k_cmpt_phi<false, float>, (n + 255) / 256, 256, 0, n, sc, psi, phi);
+  else if (acdi)
+    kgo<CmptPhi<true, float>, 256, 1>(L, k_cmpt_phi<true, float>, (n + 256 * kPhiPer - 1) / (256 * kPhiPer), 256, 0,
+                                      n, sc, psi, phi);
+  else
+    kgo<CmptPhi<false, float>, 256, 1>(L, k_cmpt_phi<false, float>, (n + 256 * kPhiPer - 1) / (256 * kPhiPer), 256,
+                                       0, n, sc, psi, phi);
 }
 
 // ---------------------------------------------------------------------------
@@ -583,20 +598,45 @@ void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScala
 // step in one pass: both read the correction phi, and updatep needs none of
 // the velocity ghost fills that follow correc.  32x8 point tiles of the halo
 // array; pout = phi + pp on the interior (the new pressure into the po slot).
+constexpr int kCorrecLevels = 4;  // z levels per thread of k_correc_updatep
 struct CorrecUpdatep {
+  // each thread owns one (i, j) column and kCorrecLevels consecutive levels:
+  // all loads first (p at level k+1 is the next level's own p), then the
+  // updates, so that a warp has many independent loads in flight
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
       const DevScalars* __restrict__ sc, const double* __restrict__ p, double* __restrict__ u,
       double* __restrict__ v, double* __restrict__ w, const double* __restrict__ pp, double* __restrict__ pout) {
+    constexpr int KC = kCorrecLevels;
     if (HALTED(sc)) return;
-    const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k = bk.z;
+    const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k0 = bk.z * KC;
     if (i > g.nx + 1 || j > g.ny + 1) return;
     const double dt = sc->dt, rhop = ph.rho0;
-    const int c = g.h(i, j, k);
-    const double pc = LD(p, c);
-    if (i <= g.nx) u[c] = u[c] - dt * g.dxi * (LD(p, c + 1) - pc) / rhop;
-    if (j <= g.ny) v[c] = v[c] - dt * g.dyi * (LD(p, c + g.sx) - pc) / rhop;
-    if (k <= g.nz) w[c] = w[c] - dt * g.dzci[k] * (LD(p, c + g.sxy) - pc) / rhop;
-    if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz) pout[c] = pc + LD(pp, c);
+    const int c0 = g.h(i, j, k0);
+    const bool xin = i <= g.nx, yin = j <= g.ny, ij_int = i >= 1 && xin && j >= 1 && yin;
+    double pc[KC + 1], px[KC], py[KC], uo[KC], vo[KC], wo[KC], pq[KC];
+#pragma unroll
+    for (int q = 0; q < KC; ++q) {
+      const int k = k0 + q, c = c0 + q * g.sxy;
+      if (k <= g.nz + 1) {
+        pc[q] = LD(p, c);
+        px[q] = xin ? LD(p, c + 1) : 0.;
+        py[q] = yin ? LD(p, c + g.sx) : 0.;
+        uo[q] = xin ? u[c] : 0.;
+        vo[q] = yin ? v[c] : 0.;
+        wo[q] = k <= g.nz ? w[c] : 0.;
+        pq[q] = (ij_int && k >= 1 && k <= g.nz) ? LD(pp, c) : 0.;
+      }
+    }
+    pc[KC] = (k0 + KC - 1 <= g.nz) ? LD(p, c0 + KC * g.sxy) : 0.;
+#pragma unroll
+    for (int q = 0; q < KC; ++q) {
+      const int k = k0 + q, c = c0 + q * g.sxy;
+      if (k > g.nz + 1) break;
+      if (xin) u[c] = uo[q] - dt * g.dxi * (px[q] - pc[q]) / rhop;
+      if (yin) v[c] = vo[q] - dt * g.dyi * (py[q] - pc[q]) / rhop;
+      if (k <= g.nz) w[c] = wo[q] - dt * g.dzci[k] * (pc[q + 1] - pc[q]) / rhop;
+      if (ij_int && k >= 1 && k <= g.nz) pout[c] = pc[q] + pq[q];
+    }
   }
 };
 __global__ void __launch_bounds__(256) k_correc_updatep(Geo g, Phys ph, const DevScalars* __restrict__ sc,
@@ -607,7 +647,7 @@ __global__ void __launch_bounds__(256) k_correc_updatep(Geo g, Phys ph, const De
 }
 void launch_correc_updatep(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
                            double* u, double* v, double* w, const double* pp, double* pout) {
-  const dim3 b(32, 8), gr((g.nx + 2 + 31) / 32, (g.ny + 2 + 7) / 8, g.nz + 2);
+  const dim3 b(32, 8), gr((g.nx + 2 + 31) / 32, (g.ny + 2 + 7) / 8, (g.nz + 2 + kCorrecLevels - 1) / kCorrecLevels);
   kgo<CorrecUpdatep, 256, 1>(L, k_correc_updatep, gr, b, 0, g, ph, sc, p, u, v, w, pp, pout);
 }
 
@@ -924,17 +964,46 @@ struct StepReduce {
     if (!acdi && !chk) return;
     double velmax = 0., dtimax = 0., divsum = 0., divmax = 0.;
     const int nrows = g.ny * g.nz;
-    for (int r = bk.x; r < nrows; r += bk.nx) {
-      const int j = r % g.ny + 1, k = r / g.ny + 1;
+    if (!chk) {
+      // Gamma only (every step): R rows per pass, their loads issued together
+      constexpr int R = 4;
       for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
-        const int c = g.h(i, j, k);
-        if (acdi) {
-          const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
-          const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
-          const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
-          velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+        for (int r0 = bk.x; r0 < nrows; r0 += R * bk.nx) {
+          double u0[R], u1[R], v0[R], v1[R], w0[R], w1[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            const int r = r0 + q * bk.nx;
+            if (r < nrows) {
+              const int c = g.h(i, r % g.ny + 1, r / g.ny + 1);
+              u0[q] = LD(u, c);
+              u1[q] = LD(u, c - 1);
+              v0[q] = LD(v, c);
+              v1[q] = LD(v, c - g.sx);
+              w0[q] = LD(w, c);
+              w1[q] = LD(w, c - g.sxy);
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            if (r0 + q * bk.nx >= nrows) break;
+            const double uc = 0.5 * (u0[q] + u1[q]);
+            const double vc = 0.5 * (v0[q] + v1[q]);
+            const double wc = 0.5 * (w0[q] + w1[q]);
+            velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+          }
         }
-        if (chk) {
+      }
+    } else {
+      for (int r = bk.x; r < nrows; r += bk.nx) {
+        const int j = r % g.ny + 1, k = r / g.ny + 1;
+        for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+          const int c = g.h(i, j, k);
+          if (acdi) {
+            const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
+            const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
+            const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
+            velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+          }
           dtimax = fmax(dtimax, chkdt_cell(g, i, j, k, u, v, w));
           const double div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +
                              (LD(u, c) - LD(u, c - 1)) * g.dxi;
