@@ -807,7 +807,7 @@ void launch_gamma(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc,
 __device__ __forceinline__ double chkdt_cell(const Geo& g, int i, int j, int k, const double* __restrict__ u,
                                              const double* __restrict__ v, const double* __restrict__ w) {
   const int c = g.h(i, j, k), sx = g.sx, sxy = g.sxy;
-  const double dxi = 1. / g.dx, dyi = 1. / g.dy;
+  const double dxi = recip_rn(g.dx), dyi = recip_rn(g.dy);
   const double ux = fabs(LD(u, c));
   const double vx = 0.25 * fabs(LD(v, c) + LD(v, c - sx) + LD(v, c + 1) + LD(v, c + 1 - sx));
   const double wx = 0.25 * fabs(LD(w, c) + LD(w, c - sxy) + LD(w, c + 1) + LD(w, c + 1 - sxy));

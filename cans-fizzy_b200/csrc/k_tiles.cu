@@ -111,7 +111,7 @@ struct YoungsTile {
         const T mx = T(0.25) * ((pcc + ppc + pcp + ppp) - (ccc + cpc + ccp + cpp)) * d1;
         const T my = T(0.25) * ((cpc + ppc + cpp + ppp) - (ccc + pcc + ccp + pcp)) * d2;
         const T mz = T(0.25) * ((ccp + pcp + cpp + ppp) - (ccc + pcc + cpc + ppc)) * dz;
-        const T inv = T(1.) / (sqrt(sqr(mx) + sqr(my) + sqr(mz)) + T(CANSFZ_EPS));
+        const T inv = recip_rn(sqrt(sqr(mx) + sqr(my) + sqr(mz)) + T(CANSFZ_EPS));
         ox[q] = mx * inv;
         oy[q] = my * inv;
         oz[q] = mz * inv;
@@ -157,7 +157,7 @@ struct YoungsTile {
         const T norm_x = T(.125) * (mx[0] + mx[1] + mx[2] + mx[3] + mx[4] + mx[5] + mx[6] + mx[7]);
         const T norm_y = T(.125) * (my[0] + my[1] + my[2] + my[3] + my[4] + my[5] + my[6] + my[7]);
         const T norm_z = T(.125) * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
-        const T inv = T(1.) / (sqrt(sqr(norm_x) + sqr(norm_y) + sqr(norm_z)) + T(CANSFZ_EPS));
+        const T inv = recip_rn(sqrt(sqr(norm_x) + sqr(norm_y) + sqr(norm_z)) + T(CANSFZ_EPS));
         const int c = g.h(i, j, k);
         normx[c] = norm_x * inv;
         normy[c] = norm_y * inv;
@@ -601,7 +601,7 @@ struct MomentumTile {
         const double rhoz_p = rhod + drhod * 0.5 * (ps_c + ps_z);
         const double Ru = (double)dudt_aux, Rv = (double)dvdt_aux, Rw = (double)dwdt_aux;
         const double Ruo = first ? Ru : hu0, Rvo = first ? Rv : hv0, Rwo = first ? Rw : hw0;
-        const double irx = 1. / rhox_p, iry = 1. / rhoy_p, irz = 1. / rhoz_p;
+        const double irx = recip_rn(rhox_p), iry = recip_rn(rhoy_p), irz = recip_rn(rhoz_p);
         const double un = s_u[o0] * rhox_n * irx + (f1 * Ru + f2 * Ruo) * irx;
         const double vn = s_v[o0] * rhoy_n * iry + (f1 * Rv + f2 * Rvo) * iry;
         const double wn = s_w[o0] * rhoz_n * irz + (f1 * Rw + f2 * Rwo) * irz;
