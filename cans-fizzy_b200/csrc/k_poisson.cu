@@ -823,7 +823,7 @@ constexpr int lines_per_cta(int m, int maxL, int tsize) {
   while (L > 1 && 4LL * m * (L | 1) * tsize > 96 * 1024) L >>= 1;
   return L;
 }
-constexpr int x_maxL(int m) { return 2 * m >= 128 ? 8 : 32; }
+constexpr int x_maxL(int m) { return 2 * m >= 128 ? 4 : 16; }
 // y lines per CTA: 16, and more for very short lines (ny = 2 in the 2-D
 // convention), which would otherwise leave most threads of a CTA idle and
 // launch nx/16 * nz CTAs of a few points each
