@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
 // read through the read-only cache, the own-column value carried upwards.
 // Those loads and the history reads are issued at the top of each level, so
 // that the stencil arithmetic hides their latency; holding them takes up to
-// 128 registers, two 256-thread blocks per SM.
+// 128 registers; the kernel runs on 32x4 tiles (128 threads), four blocks per
+// SM, so that a block's two barriers per level couple four warps, not eight.
 // The expressions are those of the per-point kernels (same operand order).
 // With TI = float the advection/diffusion RHS is evaluated in FP32; the AB2
 // update, the pressure-split terms and mom_xyz_oth stay in FP64.
@@ -657,7 +658,7 @@ struct MomentumTile {
   }
 };
 template <typename TI, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::NT, 2) k_momentum_tile(Geo g, Phys ph,
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT, 512 / tile::Shape<TYV>::NT) k_momentum_tile(Geo g, Phys ph,
     const DevScalars* __restrict__ sc, int kz, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ w, const double* __restrict__ psi, const double* __restrict__ psio,
     const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
@@ -724,7 +725,7 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
                         TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
   using S = tile::Shape<TYV>;
   const int kz = tile_kz<TYV>(g, L.batched);
-  kgo<MomentumTile<TI, TYV>, S::NT, 2>(L, k_momentum_tile<TI, TYV>, tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY),
+  kgo<MomentumTile<TI, TYV>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV>, tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY),
                                        mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po,
                                        kappa, duo, dvo, dwo, uo, vo, wo);
 }
@@ -737,7 +738,7 @@ void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevS
   if (tile::rows_of(g) == 2)
     momentum_go<TI, 2>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
   else
-    momentum_go<TI, 8>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+    momentum_go<TI, 4>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
 }
 
 template void launch_momentum_t<double>(const Launch&, const Geo&, const Phys&, const DevScalars*, const double*,
@@ -775,6 +776,10 @@ static void tile_attrs() {
   acdi_attr<TI, false, false, TYV>();
 }
 void tiles_set_attributes() {
+  cudaFuncSetAttribute(k_momentum_tile<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<double, 4>());
+  cudaFuncSetAttribute(k_momentum_tile<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<float, 4>());
   tile_attrs<double, 8>();
   tile_attrs<float, 8>();
   tile_attrs<double, 2>();
