@@ -91,7 +91,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=256, help="cube size of the droplet workload (profiling runs)")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--sweeps", type=int, default=2, help="refinement sweeps of the mixed form")
+    ap.add_argument("--sweeps", type=int, default=-1,
+                    help="refinement sweeps of the mixed form's FP32 Poisson solve (-1: the solve in FP64)")
     ap.add_argument("--config", default="c3a", choices=["c3a", "c1", "c3b", "c5", "c2"],
                     help="benchmark-matrix configuration (c3a: the metric's 256^3 ACDI case; c2: Poisson only)")
     ap.add_argument("--ensemble-steps", type=int, default=100,
@@ -382,12 +383,17 @@ def gpu_arm(args):
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64 state / f32 stencils+transforms",
+        "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else
+        ("f64 state, momentum and Poisson / f32 phase field" if args.sweeps < 0 else
+         "f64 state and momentum / f32 phase field and transforms"),
         "data": DATA,
         "config": {"workload": workload, "config": args.config,
                    "grid": [nx, ny, nz],
                    "form": "fp64 (drop-in)" if args.form == "fp64" else
-                           f"mixed (FP32 stencils and transforms, FP64 state, {args.sweeps} refinement sweeps)",
+                           ("mixed (FP32 phase-field stencils, fluxes, curvature and histories; FP64 state, "
+                            "momentum and Poisson solve)" if args.sweeps < 0 else
+                            f"mixed (FP32 phase field and transforms, FP64 state and momentum, {args.sweeps} "
+                            "refinement sweeps)"),
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": (f"inputs larger than L2 (each FP64 field {8 * (nx + 2) * (ny + 2) * (nz + 2) / 1e6:.0f} MB"
                           f"{' > ' if 8 * (nx + 2) * (ny + 2) * (nz + 2) > 126e6 else ' < '}126 MB; "

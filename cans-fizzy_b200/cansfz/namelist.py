@@ -104,7 +104,7 @@ SCHEMA = {
         "acdi_gam_factor": Var("r", (), (), 1.0),
         "acdi_gam_min": Var("r", (), (), _sp(1.0e-12)),
         "form": Var("s", (), (), "fp64"),
-        "refine_sweeps": Var("i", (), (), 2),
+        "refine_sweeps": Var("i", (), (), -1),
     },
     "cudecomp": {},
 }

@@ -435,7 +435,7 @@ int setup_solver(cansfz_ctx* c) {
     launch_z_factors(c->L, c->g, c->pl, false, c->pl.zpiv, c->pl.zdf);
     CK(cudaGetLastError());
   }
-  if (P.form == CANSFZ_FORM_MIXED) {
+  if (P.form == CANSFZ_FORM_MIXED && P.refine_sweeps >= 0) {
     if (!c->rhsb_zero) return CANSFZ_ERR_UNSUPPORTED;  // refinement assumes homogeneous pressure BCs
     if ((rc = alloc_f32_solver(c))) return rc;
   }
@@ -591,7 +591,7 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw");
     // fillps + updt_rhs_b + solver
-    if (c->mixed) {
+    if (c->mixed && c->sweeps >= 0) {
       // FP32 spectral solve + FP64-residual refinement sweeps
       launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->rhs64);
       MARK("fillps");
@@ -782,7 +782,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
     if ((rc = dalloc(c, f, I))) return fail(rc);
   if ((rc = setup_solver(c))) return fail(rc);
   c->mixed = P.form == CANSFZ_FORM_MIXED;
-  c->sweeps = P.refine_sweeps < 0 ? 0 : (P.refine_sweeps > 8 ? 8 : P.refine_sweeps);
+  c->sweeps = P.refine_sweeps < 0 ? -1 : (P.refine_sweeps > 8 ? 8 : P.refine_sweeps);
   if (c->mixed) {
     if ((rc = dalloc(c, &c->rhs64, H))) return fail(rc);
     if ((rc = dalloc(c, &c->res64, H))) return fail(rc);

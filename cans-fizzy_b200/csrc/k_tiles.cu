@@ -147,7 +147,7 @@ struct YoungsTile {
         // vertex q: 0 (+,+,+) 1 (+,-,+) 2 (+,+,-) 3 (+,-,-) 4 (-,+,+) 5 (-,-,+) 6 (-,+,-) 7 (-,-,-)
         const int off[8] = {VX + 1, 1, VX + 1, 1, VX, 0, VX, 0};
         T mx[8], my[8], mz[8];
-  #pragma unroll
+#pragma unroll
         for (int q = 0; q < 8; ++q) {
           const T* src = (q == 2 || q == 3 || q == 6 || q == 7) ? lo : hi;
           mx[q] = src[vm + off[q]];
@@ -392,8 +392,10 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const
 // 128 registers; the kernel runs on 32x4 tiles (128 threads), four blocks per
 // SM, so that a block's two barriers per level couple four warps, not eight.
 // The expressions are those of the per-point kernels (same operand order).
-// With TI = float the advection/diffusion RHS is evaluated in FP32; the AB2
-// update, the pressure-split terms and mom_xyz_oth stay in FP64.
+// The whole update is evaluated in FP64.  TI is the storage type of the phase
+// fluxes, the curvature and the AB2 histories: double in the drop-in, float
+// in the mixed form (an FP32 RHS was 3% faster and left a 1e-6 pressure
+// error; with the RHS in FP64 the mixed form's error is 5e-9).
 // ---------------------------------------------------------------------------
 namespace {
 template <typename TI, int TYV>
@@ -417,15 +419,15 @@ struct MomentumTile {
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
     (void)TY;
-    typedef TI T;
+    typedef double T;  // the RHS in FP64 for both storage types
     extern __shared__ __align__(16) unsigned char smem[];
     double* s_u = reinterpret_cast<double*>(smem);  // each [NSLOT][PXY]
     double* s_v = s_u + NSLOT * PXY;
     double* s_w = s_v + NSLOT * PXY;
     double* s_c = s_w + NSLOT * PXY;
-    T* s_fx = reinterpret_cast<T*>(s_c + NSLOT * PXY);
-    T* s_fy = s_fx + NSLOT * PXY;
-    T* s_fz = s_fy + NSLOT * PXY;
+    TI* s_fx = reinterpret_cast<TI*>(s_c + NSLOT * PXY);
+    TI* s_fy = s_fx + NSLOT * PXY;
+    TI* s_fz = s_fy + NSLOT * PXY;
     if (HALTED(sc)) return;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
     const int i0 = bk.x * TX + 1, j0 = bk.y * TY + 1;
@@ -493,13 +495,13 @@ struct MomentumTile {
       __syncthreads();  // planes k and k+1 are in; every thread is done with level k-1
       if (act) {
         const int o0 = (k % NSLOT) * PXY + qc, o1 = ((k + 1) % NSLOT) * PXY + qc;
-  #define PU(s, a, b) ((T)s_u[o##s + (a) + PX * (b)])
-  #define PV(s, a, b) ((T)s_v[o##s + (a) + PX * (b)])
-  #define PW(s, a, b) ((T)s_w[o##s + (a) + PX * (b)])
-  #define PC(s, a, b) ((T)s_c[o##s + (a) + PX * (b)])
-  #define FLX(s, a, b) (rho * PU(s, a, b) + drho * s_fx[o##s + (a) + PX * (b)])
-  #define FLY(s, a, b) (rho * PV(s, a, b) + drho * s_fy[o##s + (a) + PX * (b)])
-  #define FLZ(s, a, b) (rho * PW(s, a, b) + drho * s_fz[o##s + (a) + PX * (b)])
+#define PU(s, a, b) ((T)s_u[o##s + (a) + PX * (b)])
+#define PV(s, a, b) ((T)s_v[o##s + (a) + PX * (b)])
+#define PW(s, a, b) ((T)s_w[o##s + (a) + PX * (b)])
+#define PC(s, a, b) ((T)s_c[o##s + (a) + PX * (b)])
+#define FLX(s, a, b) (rho * PU(s, a, b) + drho * s_fx[o##s + (a) + PX * (b)])
+#define FLY(s, a, b) (rho * PV(s, a, b) + drho * s_fy[o##s + (a) + PX * (b)])
+#define FLZ(s, a, b) (rho * PW(s, a, b) + drho * s_fz[o##s + (a) + PX * (b)])
         // the level's loads from global memory, issued before the stencil
         // arithmetic that hides their latency
         const int c = g.h(i, j, k), t = g.t(i, j, k);
@@ -643,13 +645,13 @@ struct MomentumTile {
         u_ccm = PU(0, 0, 0); v_ccm = PV(0, 0, 0); w_ccm = PW(0, 0, 0); w_pcm = PW(0, 1, 0); w_cpm = PW(0, 0, 1);
         c_ccm = PC(0, 0, 0); c_pcm = PC(0, 1, 0); c_cpm = PC(0, 0, 1);
         flx_z_ccm = FLZ(0, 0, 0); flx_z_pcm = FLZ(0, 1, 0); flx_z_cpm = FLZ(0, 0, 1);
-  #undef PU
-  #undef PV
-  #undef PW
-  #undef PC
-  #undef FLX
-  #undef FLY
-  #undef FLZ
+#undef PU
+#undef PV
+#undef PW
+#undef PC
+#undef FLX
+#undef FLY
+#undef FLZ
         p_c = p_z; po_c = po_z; pso_c = pso_z; k_c = k_z;
       }
       __syncthreads();  // plane k's slot is refilled at the next level

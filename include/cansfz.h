@@ -78,7 +78,8 @@ typedef struct cansfz_params {
   int32_t brackbill;            /* _CAPILLARY_BRACKBILL_NORMALIZATION, default 1 */
   /* forms of this library (no reference counterpart) */
   int32_t form;                 /* CANSFZ_FORM_FP64 (drop-in) or CANSFZ_FORM_MIXED */
-  int32_t refine_sweeps;        /* mixed form: FP64-residual refinement sweeps */
+  int32_t refine_sweeps;        /* mixed form: FP64-residual refinement sweeps of the
+                                   FP32 Poisson solve; -1: the Poisson solve in FP64 */
   int32_t reserved[8];
 } cansfz_params;
 

@@ -3,7 +3,8 @@
 * Poisson only (the 256^3 configuration at a reduced size): FP32 spectral
   solve plus 0-3 FP64-residual refinement sweeps vs the FP64 solve; the
   error must fall with each sweep and reach FP64 level by the third.
-* Whole steps: the mixed form (FP32 transforms + 2 sweeps) vs the FP64
+* Whole steps: the mixed form (FP32 phase-field stencils, with the Poisson
+  solve in FP64 or in FP32 + 2 sweeps) vs the FP64
   oracle, error within the 1e-6 relative bound stated for that form.
 """
 import ctypes as ct
@@ -60,8 +61,10 @@ def _step_params(n=32, mixed=True, sweeps=2):
     return p, f
 
 
-def test_mixed_step_error_vs_oracle():
-    p, f = _step_params(32, True, 2)
+@pytest.mark.parametrize("sweeps", [2, -1])
+def test_mixed_step_error_vs_oracle(sweeps):
+    # sweeps = -1: FP32 stencils with the Poisson solve in FP64
+    p, f = _step_params(32, True, sweeps)
     g = C.Case(p)
     g.set_fields(*f)
     g.prepare()
