@@ -615,10 +615,17 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     // the parity flip), in one pass over phi
     launch_correc_updatep(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b], c->p[a], c->p[b]);
     MARK("correc_updatep");
-    run_bcuvw(c, true, c->u[b], c->v[b], c->w[b], sc);
-    MARK("bc_uvw_correc");
-    run_bcp(c, 0, c->p[b], sc);
-    MARK("bc_p");
+    {
+      // bounduvw after correc and boundp of the new pressure: independent
+      // fields, one launch per fill stage for the four
+      BcField F[3];
+      bc_vel(c, true, c->u[b], c->v[b], c->w[b], F);
+      const char(*cbc)[2];
+      const double(*bcv)[2];
+      scalar_bc_spec(c, 0, &cbc, &bcv);
+      run_bc(c, {F[0], F[1], F[2], bc_scalar(c, cbc, bcv, c->p[b])}, sc);
+    }
+    MARK("bc_uvw_p");
   }
   launch_step_end(L, c->ph, sc);
   // acdi_set_gamma, and on icheck steps chkdt + chkdiv, in one pass
