@@ -21,11 +21,12 @@
 // ACDI: each face flux (advective part and regularisation part) is shared by
 // the two cells on either side.  Each thread evaluates its cell's +x, +y and
 // +z faces together (x and y into shared memory, the z face carried in
-// registers to the next level as its k-1/2 face); 40 threads add the tile's
-// -x and -y boundary faces.  The face velocities of level k+1 and the AB2
-// history of level k are loaded before level k's faces are evaluated, so that
-// the face arithmetic hides their latency.  Every face expression is
-// the reference's with the two cells' roles swapped only inside sums and
+// registers to the next level as its k-1/2 face); one extra warp evaluates
+// the tile's 40 -x and -y boundary faces meanwhile, so that no cell warp
+// takes a fourth face evaluation per level.  The face velocities of level
+// k+1 and the AB2 history of level k are loaded before level k's faces are
+// evaluated, so that the face arithmetic hides their latency.  Every face
+// expression is the reference's with the two cells' roles swapped only inside sums and
 // products of two terms, so the results are bitwise those of the per-cell
 // form.
 #include "batch.cuh"
@@ -231,8 +232,8 @@ struct AcdiTile {
       TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out) {
     using namespace tile;
     using SH = Shape<TYV>;
-    constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
-    (void)TY;
+    constexpr int TX = SH::TX, TY = SH::TY, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+    constexpr int NTA = TX * (TY + 1);  // TY rows of cell threads and one warp for the tile's boundary faces
     typedef TI T;
     constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1), NF = NFX + NFY;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -257,7 +258,7 @@ struct AcdiTile {
 
     auto issue = [&](int kk) {
       const int s = kk % NSLOT;
-      for (int q = tid; q < PXY; q += NT) {
+      for (int q = tid; q < PXY; q += NTA) {
         int h;
         const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
         const int hh = ok ? h : 0;
@@ -279,7 +280,7 @@ struct AcdiTile {
     };
 
     const int i = i0 + tx, j = j0 + ty;
-    const bool act = i <= g.nx && j <= g.ny;
+    const bool act = ty < TY && i <= g.nx && j <= g.ny;
     const int qc = (tx + 1) + PX * (ty + 1);  // the thread's own cell in a plane
 
     issue(kb - 1);
@@ -326,21 +327,25 @@ struct AcdiTile {
         f_rg[fyp] = rgy;
       }
       // the tile's -x faces (x-face 0 of each row) and -y faces (y-face 0 of
-      // each column), one thread each
-      if (tid < TY) {
-        const int b = tid;
-        if (j0 + b <= g.ny) {
-          const int q = PX * (b + 1), f = b * (TX + 1);
-          face(0, dxi, s0, q, s0, q + 1, (T)__ldg(u + g.h(i0 - 1, j0 + b, k)), &f_up[f], &f_rg[f]);
-        }
-      } else if (tid < TY + TX) {
-        const int a = tid - TY;
-        if (i0 + a <= g.nx) {
-          const int q = a + 1, f = NFX + a;
-          face(1, dyi, s0, q, s0, q + PX, (T)__ldg(v + g.h(i0 + a, j0 - 1, k)), &f_up[f], &f_rg[f]);
+      // each column), by the extra warp while the cell warps evaluate their
+      // own three faces
+      if (ty == TY) {
+        for (int e = tx; e < TY + TX; e += TX) {
+          if (e < TY) {
+            if (j0 + e <= g.ny) {
+              const int q = PX * (e + 1), f = e * (TX + 1);
+              face(0, dxi, s0, q, s0, q + 1, (T)__ldg(u + g.h(i0 - 1, j0 + e, k)), &f_up[f], &f_rg[f]);
+            }
+          } else {
+            const int a = e - TY;
+            if (i0 + a <= g.nx) {
+              const int q = a + 1, f = NFX + a;
+              face(1, dyi, s0, q, s0, q + PX, (T)__ldg(v + g.h(i0 + a, j0 - 1, k)), &f_up[f], &f_rg[f]);
+            }
+          }
         }
       }
-      const double psi_c = s_psi[s0 * PXY + qc];  // read before the barrier: the slot is refilled next level
+      const double psi_c = act ? s_psi[s0 * PXY + qc] : 0.;  // read before the barrier: the slot is refilled next level
       __syncthreads();
       if (act) {
         const int fxm = ty * (TX + 1) + tx, fym = NFX + ty * TX + tx;
@@ -367,7 +372,7 @@ struct AcdiTile {
   }
 };
 template <typename TI, bool SDF, bool UPD, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+__global__ void __launch_bounds__(tile::Shape<TYV>::TX * (tile::Shape<TYV>::TY + 1)) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
     const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
     const TI* __restrict__ phi, const double* __restrict__ psi, TI* __restrict__ dpsidt,
@@ -695,8 +700,9 @@ static void acdi_go(const Launch& L, const Geo& g, const DevScalars* sc, const d
                     double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
   using S = tile::Shape<TYV>;
   const int kz = tile_kz<TYV>(g, L.batched);
-  kgo<AcdiTile<TI, SDF, UPD, TYV>, S::NT, 3>(L, k_acdi_tile<TI, SDF, UPD, TYV>, tile::grid_of<TYV>(g, kz),
-                                             dim3(S::TX, S::TY), acdi_smem<TI, SDF, TYV>(), g, sc, kz, u, v, w, nx,
+  kgo<AcdiTile<TI, SDF, UPD, TYV>, S::TX * (S::TY + 1), 3>(L, k_acdi_tile<TI, SDF, UPD, TYV>,
+                                             tile::grid_of<TYV>(g, kz),
+                                             dim3(S::TX, S::TY + 1), acdi_smem<TI, SDF, TYV>(), g, sc, kz, u, v, w, nx,
                                              ny, nz, phi, psi, hist, fx, fy, fz, psi_out);
 }
 
