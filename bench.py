@@ -431,18 +431,20 @@ def gpu_arm(args):
         _L.check(e2e_case.lib.cansfz_prepare(e2e_case.h), "prepare")
         for _ in range(ksteps):
             rc = e2e_case.lib.cansfz_step(e2e_case.h, 1)
-            _L.check(e2e_case.lib.cansfz_get_diag(e2e_case.h, _L.ct.byref(diag)), "get_diag")
+            _L.check(e2e_case.lib.cansfz_get_status(e2e_case.h, _L.ct.byref(diag)), "get_status")
             if rc:
                 break
+        _L.check(e2e_case.lib.cansfz_get_diag(e2e_case.h, _L.ct.byref(diag)), "get_diag")
         _L.check(e2e_case.lib.cansfz_get_fields(e2e_case.h, *ptrs, 0), "get_fields")
         torch.cuda.synchronize()
         te = allreduce_max(time.perf_counter() - t0, world)
         fb = 8 * int(np.prod(hshape))
         out["e2e"] = {"value": cells * ksteps * world / te, "unit": "cell-steps/s",
                       "h2d_bytes_per_step": 5 * fb / ksteps,
-                      "d2h_bytes_per_step": (5 * fb + ksteps * _L.ct.sizeof(_L.Diag)) / ksteps,
-                      "what": "set_fields from pinned host, prepare, K x (cansfz_step(1) + cansfz_get_diag), "
-                              "get_fields to pinned host; wall clock, max over ranks"}
+                      "d2h_bytes_per_step": (5 * fb + (ksteps + 1) * _L.ct.sizeof(_L.Diag)) / ksteps,
+                      "what": "set_fields from pinned host, prepare, K x (cansfz_step(1) + cansfz_get_status: "
+                              "time, dt, Gamma, status to the host every step), cansfz_get_diag (phase masses) "
+                              "and get_fields to pinned host at the end; wall clock, max over ranks"}
         e2e_case.close()
     # ---- CPU baseline (rank 0, N = 1)
     if world == 1 and not args.no_cpu_baseline:

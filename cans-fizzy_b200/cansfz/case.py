@@ -124,6 +124,12 @@ class Case:
         _L.check(self.lib.cansfz_get_diag(self.h, ct.byref(d)), "cansfz_get_diag")
         return d
 
+    def status(self) -> _L.Diag:
+        """The per-step scalars of diag() without the phase masses (NaN)."""
+        d = _L.Diag()
+        _L.check(self.lib.cansfz_get_status(self.h, ct.byref(d)), "cansfz_get_status")
+        return d
+
     def grid(self):
         nz = self.n[2]
         arrs = [np.zeros(nz + 2) for _ in range(6)]

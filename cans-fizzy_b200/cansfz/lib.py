@@ -43,6 +43,7 @@ SIGNATURES = {
     "cansfz_prepare": (I, [V]),
     "cansfz_step": (I, [V, I]),
     "cansfz_get_diag": (I, [V, ct.POINTER(Diag)]),
+    "cansfz_get_status": (I, [V, ct.POINTER(Diag)]),
     "cansfz_rk_2fl": (I, [V, PD, D, D, D, D] + [V] * 10),
     "cansfz_acdi_transport_pf": (I, [V, D, D] + [V] * 12),
     "cansfz_vof_thinc_transport_psi": (I, [V, D] + [V] * 12),

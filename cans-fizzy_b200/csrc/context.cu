@@ -1196,18 +1196,25 @@ int cansfz_step(cansfz_ctx* c, int nsteps) {
   return c->last_status;
 }
 
-int cansfz_get_diag(cansfz_ctx* c, cansfz_diag* d) {
+namespace {
+int fill_diag(cansfz_ctx* c, cansfz_diag* d, bool with_mass) {
   if (!c || !d) return CANSFZ_ERR_ARG;
-  launch_mass(c->L, c->g, c->ph, c->sc, c->partial, c->psi[c->cur], c->P.l[0] * c->P.l[1] * c->P.l[2]);
+  if (with_mass)
+    launch_mass(c->L, c->g, c->ph, c->sc, c->partial, c->psi[c->cur], c->P.l[0] * c->P.l[1] * c->P.l[2]);
   if (int rc = sync_status(c)) return rc;
   const DevScalars& h = *c->sc_host;
   std::memset(d, 0, sizeof(*d));
   d->time = h.time; d->istep = h.istep; d->dt = h.dt; d->dto = h.dto; d->dt_cfl = h.dt_cfl;
   d->gam = h.gam; d->seps = h.seps; d->divtot = h.divtot; d->divmax = h.divmax;
-  d->mass12[0] = h.mass12[0]; d->mass12[1] = h.mass12[1];
+  d->mass12[0] = with_mass ? h.mass12[0] : std::nan("");
+  d->mass12[1] = with_mass ? h.mass12[1] : std::nan("");
   d->status = h.status;
   return CANSFZ_OK;
 }
+}  // namespace
+
+int cansfz_get_diag(cansfz_ctx* c, cansfz_diag* d) { return fill_diag(c, d, true); }
+int cansfz_get_status(cansfz_ctx* c, cansfz_diag* d) { return fill_diag(c, d, false); }
 
 int cansfz_initgrid(int gtype, int nz, double gr, double lz, double* dzc, double* dzf, double* zc, double* zf) {
   if (nz < 1 || !dzc || !dzf || !zc || !zf) return CANSFZ_ERR_ARG;

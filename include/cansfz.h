@@ -131,6 +131,10 @@ int cansfz_prepare(cansfz_ctx* ctx);
  * conditions, after finishing the step that triggered them.              */
 int cansfz_step(cansfz_ctx* ctx, int nsteps);
 int cansfz_get_diag(cansfz_ctx* ctx, cansfz_diag* d);
+/* The per-step scalars of cansfz_get_diag (time, istep, dt, Gamma, status,
+ * divergence of the last check) without the phase-mass reduction, which the
+ * reference evaluates only on output steps: mass12 is set to NaN.        */
+int cansfz_get_status(cansfz_ctx* ctx, cansfz_diag* d);
 /* Device stream the context runs on (cudaStream_t). */
 void* cansfz_stream(cansfz_ctx* ctx);
 

@@ -62,3 +62,21 @@ def test_gpu_case_save_restore(tmp_path):
     # the restarted case takes an Euler first step (no AB2 history in the
     # files, as in the reference); it must step on from the restored count
     assert b.step(3) == 0 and b.diag().istep == 10
+
+
+@pytest.mark.gpu
+def test_gpu_status_is_diag_without_masses():
+    # cansfz_get_status: the per-step scalars of cansfz_get_diag, no mass reduction
+    from cansfz import case as C
+    from cansfz import workloads as W
+
+    p, f = W.droplets((32, 32, 32), (1.0, 1.0, 1.0), False, count=3, rmin=0.1, rmax=0.15, seed=7)
+    a = C.Case(p)
+    a.set_fields(*f)
+    a.prepare()
+    assert a.step(11) == 0  # past an icheck step: dt and divergence updated
+    s, d = a.status(), a.diag()
+    for nm in ("time", "istep", "dt", "dto", "dt_cfl", "gam", "seps", "divtot", "divmax", "status"):
+        assert getattr(s, nm) == getattr(d, nm), nm
+    assert np.isnan(s.mass12[0]) and np.isnan(s.mass12[1])
+    assert d.mass12[0] > 0 and d.mass12[1] > 0
