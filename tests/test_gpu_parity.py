@@ -175,9 +175,12 @@ def test_projection_procedures(small):
     assert abs(dtm[0] - o.call("chkdt_fields", u, v, w, 0.3, 0.01)) <= 1e-14 * dtm[0]
 
 
-@pytest.mark.parametrize("cbcpre", ["PPPPNN", "NNPPNN", "DDPPNN", "PPNNNN", "PPPPPP", "NNNNNN"])
-def test_poisson_bcs(cbcpre):
-    p = _nml(24, 16, 20, cbcpre, l=(1.0, 0.75, 1.2))
+@pytest.mark.parametrize("cbcpre,ng", [("PPPPNN", (24, 16, 20)), ("NNPPNN", (24, 16, 20)), ("DDPPNN", (24, 16, 20)),
+                                        ("PPNNNN", (24, 16, 20)), ("PPPPPP", (24, 16, 20)), ("NNNNNN", (24, 16, 20)),
+                                        # nx*ny >= 32768: the z solve evaluates its pivots on the fly
+                                        ("PPPPNN", (256, 128, 8)), ("PPPPPP", (256, 128, 8))])
+def test_poisson_bcs(cbcpre, ng):
+    p = _nml(*ng, cbcpre, l=(1.0, 0.75, 1.2))
     g, o = C.Case(p), O.Case(p)
     rng = np.random.default_rng(5)
     rhs = o.empty()
