@@ -98,6 +98,11 @@ class Case:
                  "cansfz_get_fields")
         return [o.reshape(self.hshape, order="F") for o in outs]
 
+    def set_scalar(self, s):
+        """The scalar s of a case built with params.scalar = 1 (halo layout)."""
+        a = np.ascontiguousarray(np.asarray(s, dtype=np.float64).reshape(-1, order="F"))
+        _L.check(self.lib.cansfz_set_scalar(self.h, a.ctypes.data_as(ct.c_void_p), 0), "cansfz_set_scalar")
+
     def get(self, name: str) -> np.ndarray:
         if name in ("u", "v", "w", "p", "psi"):
             return self.get_fields()[("u", "v", "w", "p", "psi").index(name)]

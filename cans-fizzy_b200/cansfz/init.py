@@ -152,6 +152,35 @@ def initflow(p: Params, inivel: str, time: float = 0.0):
     return u, v, w, pr
 
 
+def initscal(p: Params, inisca: str) -> np.ndarray:
+    """The scalar s (halo layout; ghosts zero) as initscal sets the interior
+    (src/initflow.f90:363-429): 'cou' and 'dhc' start from the Couette
+    profile between the z boundary values bcsca(0:1,3); 'dhc' then takes the
+    linear profile between the x boundary values; 'uni' is their z mean,
+    'zer' zero."""
+    nx, ny, nz = p.n
+    bc = np.array(p.bcsca[:]).reshape((2, 3), order="F")
+    g = zgrid(p)
+    zcn = g["zc"][1:-1] / p.l[2]
+    name = inisca.strip()
+    if name in ("cou", "dhc"):
+        s1d = 0.5 * (1.0 - 2.0 * zcn) * 1.0
+        s1d = s1d + 0.5
+        s1d = bc[0, 2] * s1d + bc[1, 2] * (1.0 - s1d)
+    elif name == "uni":
+        s1d = np.full(nz, 0.5 * (bc[0, 2] + bc[1, 2]))
+    elif name == "zer":
+        s1d = np.zeros(nz)
+    else:
+        raise ValueError(f"invalid name for initial scalar field {inisca!r}")
+    s = np.zeros((nx + 2, ny + 2, nz + 2), order="F")
+    s[1:-1, 1:-1, 1:-1] = s1d[None, None, :]
+    if name == "dhc":
+        xx = (np.arange(1, nx + 1) - 0.5) * (p.l[0] / p.ng[0]) / p.l[0]
+        s[1:-1, 1:-1, 1:-1] = ((1.0 - xx) * bc[0, 0] + xx * bc[1, 0])[:, None, None]
+    return s
+
+
 # ---------------------------------------------------------------------------
 # seeded synthetic inputs
 # ---------------------------------------------------------------------------

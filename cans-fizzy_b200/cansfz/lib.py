@@ -40,6 +40,7 @@ SIGNATURES = {
     "cansfz_set_fields": (I, [V, V, V, V, V, V, I]),
     "cansfz_get_fields": (I, [V, V, V, V, V, V, I]),
     "cansfz_get_aux": (I, [V, ct.c_char_p, V, I]),
+    "cansfz_set_scalar": (I, [V, V, I]),
     "cansfz_prepare": (I, [V]),
     "cansfz_step": (I, [V, I]),
     "cansfz_get_diag": (I, [V, ct.POINTER(Diag)]),
@@ -52,9 +53,11 @@ SIGNATURES = {
     "cansfz_acdi_set_gamma": (I, [V, D, V, V, V, PD]),
     "cansfz_cmpt_norm_curv_youngs": (I, [V] + [V] * 5),
     "cansfz_clip_field": (I, [V, D, D, V]),
-    "cansfz_rk": (I, [V, PD, D, D, PD] + [V] * 11),
+    "cansfz_rk": (I, [V, PD, D, D, PD] + [V] * 12),
     "cansfz_mom_xyz_ad": (I, [V] + [V] * 10),
-    "cansfz_mom_xyz_oth": (I, [V, D, PD] + [V] * 8),
+    "cansfz_mom_xyz_oth": (I, [V, D, PD] + [V] * 9),
+    "cansfz_scal_ad": (I, [V] + [V] * 9),
+    "cansfz_rk_scal": (I, [V, PD, D] + [V] * 9),
     "cansfz_fillps": (I, [V, D, V, V, V, V]),
     "cansfz_updt_rhs_b": (I, [V, V]),
     "cansfz_solver": (I, [V, V]),

@@ -101,6 +101,8 @@ SCHEMA = {
         "interface_capturing_vof": Var("l", (), (), False),
         "sdf_normals": Var("l", (), (), True),
         "capillary_brackbill_normalization": Var("l", (), (), True),
+        "scalar": Var("l", (), (), False),
+        "boussinesq_buoyancy": Var("l", (), (), False),
         "acdi_gam_factor": Var("r", (), (), 1.0),
         "acdi_gam_min": Var("r", (), (), _sp(1.0e-12)),
         "form": Var("s", (), (), "fp64"),
@@ -267,6 +269,43 @@ def parse(text: str, base: Namelist | None = None) -> Namelist:
 def read(path: str, base: Namelist | None = None) -> Namelist:
     with open(path) as f:
         return parse(f.read(), base)
+
+
+# defines of the reference's build.conf (configs/flags.mk turns KEY=1 into
+# -D_KEY) that select a code path of this library, the &cansfz switch each
+# sets, and the value flags.mk assumes when the key is absent
+BUILD_DEFINES = {
+    "INTERFACE_CAPTURING_VOF": ("interface_capturing_vof", False),
+    "SDF_NORMALS": ("sdf_normals", True),
+    "CAPILLARY_BRACKBILL_NORMALIZATION": ("capillary_brackbill_normalization", True),
+    "SCALAR": ("scalar", False),
+    "BOUSSINESQ_BUOYANCY": ("boussinesq_buoyancy", False),
+}
+
+
+def apply_build_conf(nl: Namelist, path: str) -> Namelist:
+    """Set the &cansfz switches from a reference build.conf (KEY=VALUE lines,
+    '#' comments; a define is on when its value is 1, configs/flags.mk:127-157).
+    _BOUSSINESQ_BUOYANCY acts only together with _SCALAR (src/mom.f90:930,1017).
+    A build this library does not provide raises ValueError: the HYPRE
+    variable-coefficient solver (CONSTANT_COEFFS_POISSON other than 1) and
+    SINGLE_PRECISION=1."""
+    vals = {}
+    with open(path) as f:
+        for line in f:
+            line = line.split("#", 1)[0].strip()
+            if "=" in line:
+                key, val = (x.strip() for x in line.split("=", 1))
+                vals[key] = val
+    if "CONSTANT_COEFFS_POISSON" in vals and vals["CONSTANT_COEFFS_POISSON"] != "1":
+        raise ValueError("CONSTANT_COEFFS_POISSON != 1 (the HYPRE solver) is not provided by this library")
+    if vals.get("SINGLE_PRECISION", "0") == "1":
+        raise ValueError("SINGLE_PRECISION=1 is not provided by this library (see the mixed form instead)")
+    g = nl.groups["cansfz"]
+    for key, (name, absent) in BUILD_DEFINES.items():
+        g[name] = (vals[key] == "1") if key in vals else absent
+    g["boussinesq_buoyancy"] = bool(g["boussinesq_buoyancy"]) and bool(g["scalar"])
+    return nl
 
 
 def write(nl: Namelist) -> str:

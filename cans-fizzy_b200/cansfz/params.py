@@ -44,6 +44,13 @@ class Params(ct.Structure):
         ("interface_capturing", ct.c_int32),
         ("sdf_normals", ct.c_int32),
         ("brackbill", ct.c_int32),
+        ("scalar", ct.c_int32),
+        ("boussinesq", ct.c_int32),
+        ("cbcsca", ct.c_char * 6),
+        ("bcsca", ct.c_double * 6),
+        ("ssource", ct.c_double),
+        ("ka12", ct.c_double * 2),
+        ("cp12", ct.c_double * 2),
         ("form", ct.c_int32),
         ("refine_sweeps", ct.c_int32),
         ("reserved", ct.c_int32 * 8),
@@ -112,6 +119,13 @@ def from_namelist(nl: _nml.Namelist) -> Params:
     p.interface_capturing = VOF_THINC if vof else ACDI
     p.sdf_normals = int(bool(nl["sdf_normals"]))
     p.brackbill = int(bool(nl["capillary_brackbill_normalization"]))
+    p.scalar = int(bool(nl["scalar"]))
+    p.boussinesq = int(bool(nl["boussinesq_buoyancy"]))
+    p.cbcsca = _chars(nl["cbcsca"])
+    p.bcsca[:] = _dbls(nl["bcsca"])
+    p.ssource = float(nl["ssource"])
+    p.ka12[:] = _dbls(nl["ka12"])
+    p.cp12[:] = _dbls(nl["cp12"])
     p.form = FORM_MIXED if str(nl["form"]).lower().startswith("mix") else FORM_FP64
     p.refine_sweeps = int(nl["refine_sweeps"])
     return p

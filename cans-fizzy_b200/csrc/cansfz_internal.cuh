@@ -53,6 +53,7 @@ struct DevScalars {
   int status;                        // CANSFZ_OK or the abort reason
   int halted;                        // 1 after an abort: later steps do nothing
   int first_rk, first_rk2fl;         // is_first of rk and rk_2fl (save attribute)
+  int first_scal;                    // is_first of rk_scal
   int check_now;                     // 1 on icheck steps
   // reduction slots
   unsigned long long max_bits[4];    // non-negative doubles as ordered bits
@@ -77,6 +78,12 @@ struct Phys {
   int sdf;         // _SDF_NORMALS
   int solve_ns, track;
   double mu_over_rho_max, rho_min, gmax;   // chkdt constants
+  // scalar transport (_SCALAR) and the Boussinesq buoyancy
+  int scalar, boussinesq;
+  double ka12[2], rhocp12[2];   // rhocp12 = rho12*cp12 (src/rk.f90:166)
+  double ssource;
+  double ka_rhocp_max;          // maxval(ka12/(rho12*cp12)), the chkdt constant
+  double rhobeta, drhobeta;     // rho2*beta2, rho1*beta1 - rho2*beta2
 };
 
 // ---------------------------------------------------------------------------
@@ -194,8 +201,8 @@ void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* 
                    const double* fy, const double* fz, const double* u, const double* v,
                    const double* w, const double* psi, double* du, double* dv, double* dw);
 void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
-                    const double* p, const double* psi, const double* kappa, const double* pn,
-                    const double* po, double* du, double* dv, double* dw);
+                    const double* p, const double* psi, const double* kappa, const double* s,
+                    const double* pn, const double* po, double* du, double* dv, double* dw);
 void launch_rk_update1(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
                        const double* psio, const double* psi, const double* du,
                        const double* dv, const double* dw, double* duo, double* dvo,
@@ -207,8 +214,21 @@ void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const 
                            const double* u, const double* v, const double* w,
                            const double* psi, const double* psio, const double* fx,
                            const double* fy, const double* fz, const double* p,
-                           const double* po, const double* kappa, double* duo,
+                           const double* po, const double* kappa, const double* s, double* duo,
                            double* dvo, double* dwo, double* uo, double* vo, double* wo);
+// scalar transport: scal_ad (src/scal.f90:13-66), and scal_ad with the AB2
+// update of rk_scal (src/rk.f90:133-191) in one pass (s_out interior; the
+// new dsdt into `hist`, the dsdtrko slot)
+template <typename TI>
+void launch_scal_ad(const Launch& L, const Geo& g, const Phys& ph, const TI* fx, const TI* fy, const TI* fz,
+                    const double* psi, const double* u, const double* v, const double* w, const double* s,
+                    double* dsdt);
+template <typename TI>
+void launch_scal_step(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const TI* fx,
+                      const TI* fy, const TI* fz, const double* psi, const double* psio, const double* u,
+                      const double* v, const double* w, const double* s, double* hist, double* s_out);
+void launch_scal_update(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* psi,
+                        const double* psio, const double* dsdt, double* hist, double* s);
 void launch_fillps(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
                    const double* u, const double* v, const double* w, double* p);
 void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
@@ -270,8 +290,8 @@ void launch_acdi_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf
 template <typename TI>
 void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                        const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
-                       const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
-                       TI* dvo, TI* dwo, double* uo, double* vo, double* wo);
+                       const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa,
+                       const double* s, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo, double* wo);
 void tiles_set_attributes();
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                     double* p, const StageMark* mk = nullptr);

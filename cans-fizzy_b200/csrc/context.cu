@@ -89,7 +89,9 @@ struct cansfz_ctx {
   double *fx = nullptr, *fy = nullptr, *fz = nullptr;
   double *hpsi = nullptr, *hu = nullptr, *hv = nullptr, *hw = nullptr;       // AB2 histories (interior)
   double *tu = nullptr, *tv = nullptr, *tw_ = nullptr, *tpsi = nullptr;     // per-procedure scratch (interior)
-  int cur = 0;  // index of the current u,v,w,psi and of p (= pn); po = p[cur^1]
+  // scalar (_SCALAR): s by parity like u,v,w,psi; the dsdtrko history (interior)
+  double *s[2]{}, *hs = nullptr;
+  int cur = 0;  // index of the current u,v,w,psi,s and of p (= pn); po = p[cur^1]
   // Poisson solver (initsolver)
   PoissonPlan pl{};
   double* d_solver = nullptr;  // lam, a, b, c, twiddles, rhsb
@@ -111,7 +113,7 @@ struct cansfz_ctx {
   DevScalars* sc = nullptr;       // the step scalars (device)
   DevScalars* sc_call = nullptr;  // scalars of a per-procedure call (device)
   DevScalars* sc_host = nullptr;  // pinned mirror
-  bool first_rk_call = true, first_rk2fl_call = true;
+  bool first_rk_call = true, first_rk2fl_call = true, first_rkscal_call = true;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool prepared = false;
@@ -208,6 +210,7 @@ void scalar_bc_spec(const cansfz_ctx* c, int which, const char (**cbc)[2], const
   if (which == 1) { *cbc = P.cbcpsi; *bc = P.bcpsi; }
   else if (which == 2) { *cbc = c->cbccur; *bc = c->bccur; }
   else if (which >= 3 && which <= 5) { *cbc = P.cbcnor[which - 3]; *bc = P.bcnor[which - 3]; }
+  else if (which == 6) { *cbc = P.cbcsca; *bc = P.bcsca; }
 }
 
 void run_bc(cansfz_ctx* c, std::initializer_list<BcField> fields, const DevScalars* sc) {
@@ -566,6 +569,19 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
       launch_fill(L, (size_t)g.hsize(), 0., c->fz);
     }
   }
+  if (P.scalar) {
+    // rk_scal + boundp(cbcsca), src/main.f90:460-463: the old scalar, the
+    // old velocity, the new and old phase and the phase fluxes
+    if (c->mixed)
+      launch_scal_step<float>(L, g, c->ph, sc, c->fxf, c->fyf, c->fzf, c->psi[b], c->psi[a], c->u[a], c->v[a],
+                              c->w[a], c->s[a], c->hs, c->s[b]);
+    else
+      launch_scal_step<double>(L, g, c->ph, sc, c->fx, c->fy, c->fz, c->psi[b], c->psi[a], c->u[a], c->v[a],
+                               c->w[a], c->s[a], c->hs, c->s[b]);
+    MARK("scalar");
+    run_bcp(c, 6, c->s[b], sc);
+    MARK("bc_scalar");
+  }
   if (!P.is_solve_ns) {
     const std::string iv(c->inivel);
     const int which = iv == "voy" ? 1 : (iv == "vox" ? 2 : 0);
@@ -579,14 +595,15 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     for (int d = 0; d < 3; ++d)
       if (std::fabs(P.gacc[d]) > 0. && is_pp(P.cbcpre[d]))
         launch_bulk_mean(L, g, c->ph, sc, c->partial, d + 1, c->d_grid + (d == 2 ? 5 : 4) * (g.nz + 2), c->psi[b]);
-    // rk: the whole momentum update in one pass
+    // rk: the whole momentum update in one pass (the buoyancy reads the new scalar)
+    const double* sb = c->ph.boussinesq ? c->s[b] : nullptr;
     if (c->mixed)
       launch_momentum_t<float>(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fxf, c->fyf,
-                               c->fzf, c->p[a], c->p[b], c->kappaf, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
+                               c->fzf, c->p[a], c->p[b], c->kappaf, sb, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
                                c->w[b]);
     else
       launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy,
-                            c->fz, c->p[a], c->p[b], c->kappa, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
+                            c->fz, c->p[a], c->p[b], c->kappa, sb, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
     MARK("momentum");
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw");
@@ -773,6 +790,14 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   ph.mu_over_rho_max = std::max(P.mu12[0] / P.rho12[0], P.mu12[1] / P.rho12[1]);
   ph.rho_min = std::min(P.rho12[0], P.rho12[1]);
   ph.gmax = std::max(std::fabs(P.gacc[0]), std::max(std::fabs(P.gacc[1]), std::fabs(P.gacc[2])));
+  // scalar transport; the buoyancy term exists only with the scalar (src/mom.f90:1017)
+  ph.scalar = P.scalar ? 1 : 0;
+  ph.boussinesq = (P.scalar && P.boussinesq) ? 1 : 0;
+  for (int q = 0; q < 2; ++q) { ph.ka12[q] = P.ka12[q]; ph.rhocp12[q] = P.rho12[q] * P.cp12[q]; }
+  ph.ssource = P.ssource;
+  ph.ka_rhocp_max = std::max(P.ka12[0] / (P.rho12[0] * P.cp12[0]), P.ka12[1] / (P.rho12[1] * P.cp12[1]));
+  ph.rhobeta = P.rho12[1] * P.beta12[1];
+  ph.drhobeta = P.rho12[0] * P.beta12[0] - P.rho12[1] * P.beta12[1];
   // acdi_set_epsilon (src/acdi.f90:16-30) and the THINC beta (src/param.f90:178)
   double dlmax = std::max(c->dl[0], c->dl[1]);
   for (int k = 0; k <= nz + 1; ++k) dlmax = std::max(dlmax, 1. / c->dzfi[k]);
@@ -787,6 +812,11 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
     if ((rc = dalloc(c, f, H))) return fail(rc);
   for (double** f : {&c->hpsi, &c->hu, &c->hv, &c->hw, &c->tu, &c->tv, &c->tw_, &c->tpsi})
     if ((rc = dalloc(c, f, I))) return fail(rc);
+  if (P.scalar) {
+    for (int q = 0; q < 2; ++q)
+      if ((rc = dalloc(c, &c->s[q], H))) return fail(rc);
+    if ((rc = dalloc(c, &c->hs, I))) return fail(rc);
+  }
   if ((rc = setup_solver(c))) return fail(rc);
   c->mixed = P.form == CANSFZ_FORM_MIXED;
   c->sweeps = P.refine_sweeps < 0 ? -1 : (P.refine_sweeps > 8 ? 8 : P.refine_sweeps);
@@ -813,6 +843,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   h.beta = c->beta;
   h.first_rk = 1;
   h.first_rk2fl = 1;
+  h.first_scal = 1;
   if ((rc = upload_scalars(c, c->sc, h))) return fail(rc);
   if (cudaStreamSynchronize(c->st) != cudaSuccess) return fail(CANSFZ_ERR_CUDA);
   *out = c;
@@ -861,6 +892,16 @@ int cansfz_get_fields(cansfz_ctx* c, double* u, double* v, double* w, double* p,
   return CANSFZ_OK;
 }
 
+int cansfz_set_scalar(cansfz_ctx* c, const double* s, int on_device) {
+  if (!c || !s) return CANSFZ_ERR_ARG;
+  if (!c->P.scalar) return CANSFZ_ERR_UNSUPPORTED;
+  const size_t bytes = (size_t)c->g.hsize() * sizeof(double);
+  CK(cudaMemcpyAsync(c->s[c->cur], s, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->prepared = false;
+  return CANSFZ_OK;
+}
+
 int cansfz_get_aux(cansfz_ctx* c, const char* name, double* out, int on_device) {
   if (!c || !name || !out) return CANSFZ_ERR_ARG;
   const std::string s(name);
@@ -883,6 +924,8 @@ int cansfz_get_aux(cansfz_ctx* c, const char* name, double* out, int on_device) 
   else if (s == "dudtrko") { src = c->hu; n = c->g.tsize(); }
   else if (s == "dvdtrko") { src = c->hv; n = c->g.tsize(); }
   else if (s == "dwdtrko") { src = c->hw; n = c->g.tsize(); }
+  else if (s == "s" && c->P.scalar) src = c->s[a];
+  else if (s == "dsdtrko" && c->P.scalar) { src = c->hs; n = c->g.tsize(); }
   else return CANSFZ_ERR_ARG;
   if (c->mixed) {  // FP32 intermediates, widened into scratch for the caller
     const float* f = nullptr;
@@ -920,6 +963,7 @@ int cansfz_prepare(cansfz_ctx* c) {
   run_bcuvw(c, false, c->u[a], c->v[a], c->w[a], sc);
   run_bcp(c, 0, c->p[a], sc);
   launch_copy(L, (size_t)c->g.hsize(), c->p[a], c->p[a ^ 1]);  // po = pn = p
+  if (P.scalar) run_bcp(c, 6, c->s[a], sc);
   run_bcp(c, 1, c->psi[a], sc);
   if (c->mixed) {
     normals_f32(c, c->psi[a], sc);
@@ -1348,22 +1392,26 @@ int cansfz_mom_xyz_ad(cansfz_ctx* c, const double* fx, const double* fy, const d
 }
 
 int cansfz_mom_xyz_oth(cansfz_ctx* c, double dt_r, const double rho_av[3], const double* p, const double* psi,
-                       const double* kappa, const double* pn, const double* po, double* dudt, double* dvdt,
-                       double* dwdt) {
+                       const double* kappa, const double* s, const double* pn, const double* po, double* dudt,
+                       double* dvdt, double* dwdt) {
   if (!c || !rho_av) return CANSFZ_ERR_ARG;
   DevScalars h{};
   h.dt_r = dt_r;
   for (int d = 0; d < 3; ++d) h.rho_av[d] = rho_av[d];
   if (int rc = call_scalars(c, h)) return rc;
-  launch_mom_oth(c->L, c->g, c->ph, c->sc_call, p, psi, kappa, pn, po, dudt, dvdt, dwdt);
+  if (c->ph.boussinesq && !s) return CANSFZ_ERR_ARG;
+  launch_mom_oth(c->L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr, pn, po, dudt, dvdt,
+                 dwdt);
   CK(cudaGetLastError());
   return CANSFZ_OK;
 }
 
 int cansfz_rk(cansfz_ctx* c, const double rkpar[2], double dt, double dt_r, const double rho_av[3], const double* psi,
-              const double* kappa, const double* p, const double* pn, const double* po, const double* psio,
-              const double* fx, const double* fy, const double* fz, double* u, double* v, double* w) {
+              const double* kappa, const double* p, const double* pn, const double* po, const double* s,
+              const double* psio, const double* fx, const double* fy, const double* fz, double* u, double* v,
+              double* w) {
   if (!c || !rkpar || !rho_av) return CANSFZ_ERR_ARG;
+  if (c->ph.boussinesq && !s) return CANSFZ_ERR_ARG;
   DevScalars h{};
   h.f1 = rkpar[0] * dt; h.f2 = rkpar[1] * dt; h.f12 = h.f1 + h.f2;
   h.dt_r = dt_r;
@@ -1377,9 +1425,36 @@ int cansfz_rk(cansfz_ctx* c, const double rkpar[2], double dt, double dt_r, cons
   launch_copy(L, (size_t)c->g.tsize(), c->tu, c->hu);
   launch_copy(L, (size_t)c->g.tsize(), c->tv, c->hv);
   launch_copy(L, (size_t)c->g.tsize(), c->tw_, c->hw);
-  launch_mom_oth(L, c->g, c->ph, c->sc_call, p, psi, kappa, pn, po, c->tu, c->tv, c->tw_);
+  launch_mom_oth(L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr, pn, po, c->tu, c->tv,
+                 c->tw_);
   launch_rk_update2(L, c->g, c->ph, c->sc_call, psi, c->tu, c->tv, c->tw_, u, v, w);
   c->first_rk_call = false;
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_scal_ad(cansfz_ctx* c, const double* fx, const double* fy, const double* fz, const double* psi,
+                   const double* u, const double* v, const double* w, const double* s, double* dsdt) {
+  if (!c) return CANSFZ_ERR_ARG;
+  if (!c->P.scalar) return CANSFZ_ERR_UNSUPPORTED;
+  launch_scal_ad<double>(c->L, c->g, c->ph, fx, fy, fz, psi, u, v, w, s, dsdt);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+int cansfz_rk_scal(cansfz_ctx* c, const double rkpar[2], double dt, const double* psi, const double* u,
+                   const double* v, const double* w, const double* psio, const double* fx, const double* fy,
+                   const double* fz, double* s) {
+  if (!c || !rkpar) return CANSFZ_ERR_ARG;
+  if (!c->P.scalar) return CANSFZ_ERR_UNSUPPORTED;
+  DevScalars h{};
+  h.f1 = rkpar[0] * dt; h.f2 = rkpar[1] * dt; h.f12 = h.f1 + h.f2;
+  h.first_scal = c->first_rkscal_call ? 1 : 0;
+  if (int rc = call_scalars(c, h)) return rc;
+  // src/rk.f90:169-190: scal_ad into scratch, then the update in place (history in ctx)
+  launch_scal_ad<double>(c->L, c->g, c->ph, fx, fy, fz, psi, u, v, w, s, c->tpsi);
+  launch_scal_update(c->L, c->g, c->ph, c->sc_call, psi, psio, c->tpsi, c->hs, s);
+  c->first_rkscal_call = false;
   CK(cudaGetLastError());
   return CANSFZ_OK;
 }
@@ -1428,7 +1503,8 @@ int cansfz_updatep(cansfz_ctx* c, const double* pp, double* p) {
 }
 
 int cansfz_boundp(cansfz_ctx* c, int which, double* p) {
-  if (!c || which < 0 || which > 5) return CANSFZ_ERR_ARG;
+  if (!c || which < 0 || which > 6) return CANSFZ_ERR_ARG;
+  if (which == 6 && !c->P.scalar) return CANSFZ_ERR_UNSUPPORTED;
   run_bcp(c, which, p, nullptr);
   CK(cudaGetLastError());
   return CANSFZ_OK;

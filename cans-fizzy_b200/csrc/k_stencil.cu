@@ -404,11 +404,13 @@ __device__ __forceinline__ AdOut mom_ad_cell(const Geo& g, const Phys& ph, int i
   return {dudt_aux, dvdt_aux, dwdt_aux};
 }
 
-// mom_xyz_oth, src/mom.f90:912-1038 (CONSTANT_COEFFS_POISSON, Brackbill per Phys)
+// mom_xyz_oth, src/mom.f90:912-1038 (CONSTANT_COEFFS_POISSON, Brackbill per
+// Phys; with s, the Boussinesq buoyancy of src/mom.f90:1017-1024)
 __device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, double dt_r, const double* rho_av,
                                               int i, int j, int k, const double* __restrict__ p,
                                               const double* __restrict__ psi, const double* __restrict__ kappa,
-                                              const double* __restrict__ pn, const double* __restrict__ po) {
+                                              const double* __restrict__ s, const double* __restrict__ pn,
+                                              const double* __restrict__ po) {
   const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
   const double dxi = g.dxi, dyi = g.dyi, dzci_c = g.dzci[k];
   const int ccc = g.h(i, j, k), pcc = ccc + 1, cpc = ccc + g.sx, ccp = ccc + g.sxy;
@@ -438,6 +440,15 @@ __device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, doub
   dudt_aux = dudt_aux - (dpdx_e + rhoxp * ph.irho0 * (dpdx - dpdx_e));
   dvdt_aux = dvdt_aux - (dpdy_e + rhoyp * ph.irho0 * (dpdy - dpdy_e));
   dwdt_aux = dwdt_aux - (dpdz_e + rhozp * ph.irho0 * (dpdz - dpdz_e));
+  if (s) {
+    const double s_ccc = LD(s, ccc), s_pcc = LD(s, pcc), s_cpc = LD(s, cpc), s_ccp = LD(s, ccp);
+    const double factorxp = ph.rhobeta + ph.drhobeta * psixp;
+    const double factoryp = ph.rhobeta + ph.drhobeta * psiyp;
+    const double factorzp = ph.rhobeta + ph.drhobeta * psizp;
+    dudt_aux = dudt_aux - ph.gacc[0] * factorxp * 0.5 * (s_pcc + s_ccc);
+    dvdt_aux = dvdt_aux - ph.gacc[1] * factoryp * 0.5 * (s_cpc + s_ccc);
+    dwdt_aux = dwdt_aux - ph.gacc[2] * factorzp * 0.5 * (s_ccp + s_ccc);
+  }
   return {dudt_aux, dvdt_aux, dwdt_aux};
 }
 
@@ -460,19 +471,20 @@ void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* 
 
 __global__ void k_mom_oth(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ p,
                           const double* __restrict__ psi, const double* __restrict__ kappa,
-                          const double* __restrict__ pn, const double* __restrict__ po,
-                          double* __restrict__ du, double* __restrict__ dv, double* __restrict__ dw) {
+                          const double* __restrict__ s, const double* __restrict__ pn,
+                          const double* __restrict__ po, double* __restrict__ du, double* __restrict__ dv,
+                          double* __restrict__ dw) {
   INTERIOR_IJK(g)
-  const AdOut r = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, pn, po);
+  const AdOut r = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, s, pn, po);
   const int t = g.t(i, j, k);
   du[t] = r.du; dv[t] = r.dv; dw[t] = r.dw;
 }
 
 void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
-                    const double* psi, const double* kappa, const double* pn, const double* po, double* du,
-                    double* dv, double* dw) {
+                    const double* psi, const double* kappa, const double* s, const double* pn, const double* po,
+                    double* du, double* dv, double* dw) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_mom_oth<<<gr, b, 0, L.st>>>(g, ph, sc, p, psi, kappa, pn, po, du, dv, dw);
+  k_mom_oth<<<gr, b, 0, L.st>>>(g, ph, sc, p, psi, kappa, s, pn, po, du, dv, dw);
 }
 
 // rk update 1 (src/rk.f90:86-101): u = u*rho_n/rho_p + (f1 R + f2 Ro)/rho_p; on the
@@ -540,10 +552,144 @@ void launch_rk_update2(const Launch& L, const Geo& g, const Phys& ph, const DevS
 void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                            const double* v, const double* w, const double* psi, const double* psio,
                            const double* fx, const double* fy, const double* fz, const double* p,
-                           const double* po, const double* kappa, double* duo, double* dvo, double* dwo,
-                           double* uo, double* vo, double* wo) {
-  launch_momentum_t<double>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+                           const double* po, const double* kappa, const double* s, double* duo, double* dvo,
+                           double* dwo, double* uo, double* vo, double* wo) {
+  launch_momentum_t<double>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo,
+                            wo);
 }
+
+// ---------------------------------------------------------------------------
+// scalar transport (_SCALAR): scal_ad, src/scal.f90:13-66, per interior cell
+// (the advecting flux is rho*cp*u + (rho1*cp1 - rho2*cp2)*psiflx; TI is the
+// storage type of the phase fluxes), and the AB2 update of rk_scal,
+// src/rk.f90:172-186
+// ---------------------------------------------------------------------------
+template <typename TI>
+__device__ __forceinline__ double scal_ad_cell(const Geo& g, const Phys& ph, int i, int j, int k,
+                                               const TI* __restrict__ fx, const TI* __restrict__ fy,
+                                               const TI* __restrict__ fz, const double* __restrict__ psi,
+                                               const double* __restrict__ u, const double* __restrict__ v,
+                                               const double* __restrict__ w, const double* __restrict__ s) {
+  const double ka = ph.ka12[1], dka = ph.ka12[0] - ph.ka12[1];
+  const double rhocp = ph.rhocp12[1], drhocp = ph.rhocp12[0] - ph.rhocp12[1];
+  const double dxi = g.dxi, dyi = g.dyi, dzfi_c = g.dzfi[k];
+  const int c = g.h(i, j, k), xm = c - 1, xp = c + 1, ym = c - g.sx, yp = c + g.sx, zm = c - g.sxy, zp = c + g.sxy;
+  const double s_c = LD(s, c), s_xp = LD(s, xp), s_xm = LD(s, xm), s_yp = LD(s, yp), s_ym = LD(s, ym),
+               s_zp = LD(s, zp), s_zm = LD(s, zm);
+  const double usip = 0.5 * (rhocp * LD(u, c) + drhocp * (double)LD(fx, c)) * (s_xp + s_c);
+  const double usim = 0.5 * (rhocp * LD(u, xm) + drhocp * (double)LD(fx, xm)) * (s_xm + s_c);
+  const double vsjp = 0.5 * (rhocp * LD(v, c) + drhocp * (double)LD(fy, c)) * (s_yp + s_c);
+  const double vsjm = 0.5 * (rhocp * LD(v, ym) + drhocp * (double)LD(fy, ym)) * (s_ym + s_c);
+  const double wskp = 0.5 * (rhocp * LD(w, c) + drhocp * (double)LD(fz, c)) * (s_zp + s_c);
+  const double wskm = 0.5 * (rhocp * LD(w, zm) + drhocp * (double)LD(fz, zm)) * (s_zm + s_c);
+  const double ps_c = LD(psi, c);
+  const double kaxp = ka + dka * 0.5 * (LD(psi, xp) + ps_c), kaxm = ka + dka * 0.5 * (ps_c + LD(psi, xm));
+  const double kayp = ka + dka * 0.5 * (LD(psi, yp) + ps_c), kaym = ka + dka * 0.5 * (ps_c + LD(psi, ym));
+  const double kazp = ka + dka * 0.5 * (LD(psi, zp) + ps_c), kazm = ka + dka * 0.5 * (ps_c + LD(psi, zm));
+  const double dsdxp = (s_xp - s_c) * dxi, dsdxm = (s_c - s_xm) * dxi;
+  const double dsdyp = (s_yp - s_c) * dyi, dsdym = (s_c - s_ym) * dyi;
+  const double dsdzp = (s_zp - s_c) * g.dzci[k], dsdzm = (s_c - s_zm) * g.dzci[k - 1];
+  return dxi * (-usip + usim) + dyi * (-vsjp + vsjm) + dzfi_c * (-wskp + wskm) +
+         ((kaxp * dsdxp - kaxm * dsdxm) * dxi + (kayp * dsdyp - kaym * dsdym) * dyi +
+          (kazp * dsdzp - kazm * dsdzm) * dzfi_c);
+}
+
+// s_new = s*rhocp_n/rhocp_p + (f1*dsdt + f2*dsdto + f12*ssource)/rhocp_p
+__device__ __forceinline__ double scal_update(const Phys& ph, const DevScalars* __restrict__ sc, double s_c,
+                                              double ps_c, double pso_c, double d, double dO) {
+  const double rhocp = ph.rhocp12[1], drhocp = ph.rhocp12[0] - ph.rhocp12[1];
+  const double rhocp_p = rhocp + drhocp * ps_c;
+  const double rhocp_n = rhocp + drhocp * pso_c;
+  return s_c * rhocp_n / rhocp_p + (sc->f1 * d + sc->f2 * dO + sc->f12 * ph.ssource) / rhocp_p;
+}
+
+template <typename TI>
+struct ScalAd {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph, const TI* __restrict__ fx,
+      const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ psi,
+      const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+      const double* __restrict__ s, double* __restrict__ dsdt) {
+    INTERIOR_IJK_B(g, bk)
+    dsdt[g.t(i, j, k)] = scal_ad_cell<TI>(g, ph, i, j, k, fx, fy, fz, psi, u, v, w, s);
+  }
+};
+template <typename TI>
+__global__ void k_scal_ad(Geo g, Phys ph, const TI* __restrict__ fx, const TI* __restrict__ fy,
+                          const TI* __restrict__ fz, const double* __restrict__ psi, const double* __restrict__ u,
+                          const double* __restrict__ v, const double* __restrict__ w, const double* __restrict__ s,
+                          double* __restrict__ dsdt) {
+  ScalAd<TI>::run(blk_here(), g, ph, fx, fy, fz, psi, u, v, w, s, dsdt);
+}
+template <typename TI>
+void launch_scal_ad(const Launch& L, const Geo& g, const Phys& ph, const TI* fx, const TI* fy, const TI* fz,
+                    const double* psi, const double* u, const double* v, const double* w, const double* s,
+                    double* dsdt) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  kgo<ScalAd<TI>, 128, 1>(L, k_scal_ad<TI>, gr, b, 0, g, ph, fx, fy, fz, psi, u, v, w, s, dsdt);
+}
+
+// the step's rk_scal in one pass: scal_ad of the old scalar, the AB2 update
+// into s_out (another buffer, so the stencil reads stay unmodified) and the
+// new dsdt into the history slot (the swap of src/rk.f90:190 is implicit)
+template <typename TI>
+struct ScalStep {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
+      const DevScalars* __restrict__ sc, const TI* __restrict__ fx, const TI* __restrict__ fy,
+      const TI* __restrict__ fz, const double* __restrict__ psi, const double* __restrict__ psio,
+      const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+      const double* __restrict__ s, double* __restrict__ hist, double* __restrict__ s_out) {
+    if (HALTED(sc)) return;
+    INTERIOR_IJK_B(g, bk)
+    const double d = scal_ad_cell<TI>(g, ph, i, j, k, fx, fy, fz, psi, u, v, w, s);
+    const int c = g.h(i, j, k), t = g.t(i, j, k);
+    const double dO = sc->first_scal ? d : hist[t];
+    s_out[c] = scal_update(ph, sc, LD(s, c), LD(psi, c), LD(psio, c), d, dO);
+    hist[t] = d;
+  }
+};
+template <typename TI>
+__global__ void k_scal_step(Geo g, Phys ph, const DevScalars* __restrict__ sc, const TI* __restrict__ fx,
+                            const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ psi,
+                            const double* __restrict__ psio, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w,
+                            const double* __restrict__ s, double* __restrict__ hist, double* __restrict__ s_out) {
+  ScalStep<TI>::run(blk_here(), g, ph, sc, fx, fy, fz, psi, psio, u, v, w, s, hist, s_out);
+}
+template <typename TI>
+void launch_scal_step(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const TI* fx,
+                      const TI* fy, const TI* fz, const double* psi, const double* psio, const double* u,
+                      const double* v, const double* w, const double* s, double* hist, double* s_out) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  kgo<ScalStep<TI>, 128, 1>(L, k_scal_step<TI>, gr, b, 0, g, ph, sc, fx, fy, fz, psi, psio, u, v, w, s, hist, s_out);
+}
+
+// the second loop of rk_scal alone (src/rk.f90:176-186), in place: dsdt from
+// scal_ad, the history slot takes it
+__global__ void k_scal_update(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ psi,
+                              const double* __restrict__ psio, const double* __restrict__ dsdt,
+                              double* __restrict__ hist, double* __restrict__ s) {
+  INTERIOR_IJK(g)
+  const int c = g.h(i, j, k), t = g.t(i, j, k);
+  const double d = dsdt[t];
+  const double dO = sc->first_scal ? d : hist[t];
+  s[c] = scal_update(ph, sc, s[c], LD(psi, c), LD(psio, c), d, dO);
+  hist[t] = d;
+}
+void launch_scal_update(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* psi,
+                        const double* psio, const double* dsdt, double* hist, double* s) {
+  dim3 b = blk_interior(g), gr = grd_interior(g, b);
+  k_scal_update<<<gr, b, 0, L.st>>>(g, ph, sc, psi, psio, dsdt, hist, s);
+}
+
+template void launch_scal_ad<double>(const Launch&, const Geo&, const Phys&, const double*, const double*,
+                                     const double*, const double*, const double*, const double*, const double*,
+                                     const double*, double*);
+template void launch_scal_step<double>(const Launch&, const Geo&, const Phys&, const DevScalars*, const double*,
+                                       const double*, const double*, const double*, const double*, const double*,
+                                       const double*, const double*, const double*, double*, double*);
+template void launch_scal_step<float>(const Launch&, const Geo&, const Phys&, const DevScalars*, const float*,
+                                      const float*, const float*, const double*, const double*, const double*,
+                                      const double*, const double*, const double*, double*, double*);
 
 // ---------------------------------------------------------------------------
 // fillps, src/fillps.f90:13-51
@@ -856,6 +1002,11 @@ __device__ __forceinline__ void chkdt_finish(const Phys& ph, DevScalars* sc, dou
     dtmax = 1. / dti;
     if (ph.track) dtmax = fmin(dtmax, 1. / dtipsi);
   }
+  if (ph.scalar) {  // the scalar's diffusion limit, src/chkdt.f90:88-93
+    dti = ph.ka_rhocp_max / (ph.dlmin * ph.dlmin);
+    if (dti == 0.) dti = 1.;
+    dtmax = fmin(dtmax, 1. / dti);
+  }
   sc->dt_cfl = dtmax;
   double dt = fmin(ph.cfl * dtmax, ph.dtmax);
   if (ph.dt_f > 0.) {
@@ -1165,6 +1316,7 @@ struct StepEnd {
     sc->dto = sc->dt;
     sc->first_rk = 0;
     sc->first_rk2fl = 0;
+    sc->first_scal = 0;
   }
 };
 __global__ void k_step_end(DevScalars* sc) {

@@ -401,6 +401,8 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::TX * (tile::Shape<TYV>::TY +
 // fluxes, the curvature and the AB2 histories: double in the drop-in, float
 // in the mixed form (an FP32 RHS was 3% faster and left a 1e-6 pressure
 // error; with the RHS in FP64 the mixed form's error is 5e-9).
+// BUOY adds the Boussinesq buoyancy of the scalar s (_SCALAR with
+// _BOUSSINESQ_BUOYANCY, src/mom.f90:1017-1024) after the pressure terms.
 // ---------------------------------------------------------------------------
 namespace {
 template <typename TI, int TYV>
@@ -412,14 +414,15 @@ constexpr size_t mom_smem() {
 }
 }  // namespace
 
-template <typename TI, int TYV>
+template <typename TI, int TYV, bool BUOY>
 struct MomentumTile {
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
       const DevScalars* __restrict__ sc, int kz, const double* __restrict__ u, const double* __restrict__ v,
       const double* __restrict__ w, const double* __restrict__ psi, const double* __restrict__ psio,
       const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
-      const double* __restrict__ po, const TI* __restrict__ kappa, TI* __restrict__ duo, TI* __restrict__ dvo,
-      TI* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo, double* __restrict__ wo) {
+      const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s,
+      TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
+      double* __restrict__ vo, double* __restrict__ wo) {
     using namespace tile;
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
@@ -643,6 +646,15 @@ struct MomentumTile {
         sdu = sdu - (dpdx_e + rhoxp * ph.irho0 * (dpdx - dpdx_e));
         sdv = sdv - (dpdy_e + rhoyp * ph.irho0 * (dpdy - dpdy_e));
         sdw = sdw - (dpdz_e + rhozp * ph.irho0 * (dpdz - dpdz_e));
+        if (BUOY) {
+          const double s_c = __ldg(s + c), s_x = __ldg(s + c + 1), s_y = __ldg(s + c + sx), s_z = __ldg(s + c + sxy);
+          const double factorxp = ph.rhobeta + ph.drhobeta * psixp;
+          const double factoryp = ph.rhobeta + ph.drhobeta * psiyp;
+          const double factorzp = ph.rhobeta + ph.drhobeta * psizp;
+          sdu = sdu - ph.gacc[0] * factorxp * 0.5 * (s_x + s_c);
+          sdv = sdv - ph.gacc[1] * factoryp * 0.5 * (s_y + s_c);
+          sdw = sdw - ph.gacc[2] * factorzp * 0.5 * (s_z + s_c);
+        }
         uo[c] = un + f12 * sdu * irx;
         vo[c] = vn + f12 * sdv * iry;
         wo[c] = wn + f12 * sdw * irz;
@@ -664,15 +676,16 @@ struct MomentumTile {
     (void)sxy;
   }
 };
-template <typename TI, int TYV>
+template <typename TI, int TYV, bool BUOY>
 __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 512 / tile::Shape<TYV>::NT) k_momentum_tile(Geo g, Phys ph,
     const DevScalars* __restrict__ sc, int kz, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ w, const double* __restrict__ psi, const double* __restrict__ psio,
     const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
-    const double* __restrict__ po, const TI* __restrict__ kappa, TI* __restrict__ duo, TI* __restrict__ dvo,
-    TI* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo, double* __restrict__ wo) {
-  MomentumTile<TI, TYV>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo,
-      uo, vo, wo);
+    const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s, TI* __restrict__ duo,
+    TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo, double* __restrict__ vo,
+    double* __restrict__ wo) {
+  MomentumTile<TI, TYV, BUOY>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo,
+      dvo, dwo, uo, vo, wo);
 }
 
 // ---------------------------------------------------------------------------
@@ -726,37 +739,44 @@ void launch_acdi_t(const Launch& L, const Geo& g, const DevScalars* sc, bool sdf
     acdi_pick<TI, 8>(L, g, sc, sdf, upd, u, v, w, nx, ny, nz, phi, psi, psi_out, hist, fx, fy, fz);
 }
 
-template <typename TI, int TYV>
+template <typename TI, int TYV, bool BUOY>
 static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                         const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
-                        const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
-                        TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
+                        const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa,
+                        const double* s, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
   using S = tile::Shape<TYV>;
   const int kz = tile_kz<TYV>(g, L.batched);
-  kgo<MomentumTile<TI, TYV>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV>, tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY),
-                                       mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po,
-                                       kappa, duo, dvo, dwo, uo, vo, wo);
+  kgo<MomentumTile<TI, TYV, BUOY>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, BUOY>, tile::grid_of<TYV>(g, kz),
+                                       dim3(S::TX, S::TY), mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
+                                       fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo, wo);
 }
 
 template <typename TI>
 void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                        const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
-                       const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa, TI* duo,
-                       TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
-  if (tile::rows_of(g) == 2)
-    momentum_go<TI, 2>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+                       const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa,
+                       const double* s, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo, double* wo) {
+  const bool two = tile::rows_of(g) == 2;
+  if (s && two)
+    momentum_go<TI, 2, true>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo, wo);
+  else if (s)
+    momentum_go<TI, 4, true>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo, wo);
+  else if (two)
+    momentum_go<TI, 2, false>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo,
+                              wo);
   else
-    momentum_go<TI, 4>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, duo, dvo, dwo, uo, vo, wo);
+    momentum_go<TI, 4, false>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo,
+                              wo);
 }
 
 template void launch_momentum_t<double>(const Launch&, const Geo&, const Phys&, const DevScalars*, const double*,
                                         const double*, const double*, const double*, const double*, const double*,
                                         const double*, const double*, const double*, const double*, const double*,
-                                        double*, double*, double*, double*, double*, double*);
+                                        const double*, double*, double*, double*, double*, double*, double*);
 template void launch_momentum_t<float>(const Launch&, const Geo&, const Phys&, const DevScalars*, const double*,
                                        const double*, const double*, const double*, const double*, const float*,
                                        const float*, const float*, const double*, const double*, const float*,
-                                       float*, float*, float*, double*, double*, double*);
+                                       const double*, float*, float*, float*, double*, double*, double*);
 template void launch_youngs_t<double>(const Launch&, const Geo&, const DevScalars*, const double*, double*, double*,
                                       double*, double*);
 template void launch_youngs_t<float>(const Launch&, const Geo&, const DevScalars*, const float*, float*, float*,
@@ -775,19 +795,24 @@ static void acdi_attr() {
                        (int)acdi_smem<TI, SDF, TYV>());
 }
 template <typename TI, int TYV>
-static void tile_attrs() {
-  cudaFuncSetAttribute(k_momentum_tile<TI, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+static void mom_attrs() {
+  cudaFuncSetAttribute(k_momentum_tile<TI, TYV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)mom_smem<TI, TYV>());
+  cudaFuncSetAttribute(k_momentum_tile<TI, TYV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<TI, TYV>());
+}
+template <typename TI, int TYV>
+static void tile_attrs() {
   acdi_attr<TI, true, true, TYV>();
   acdi_attr<TI, true, false, TYV>();
   acdi_attr<TI, false, true, TYV>();
   acdi_attr<TI, false, false, TYV>();
 }
 void tiles_set_attributes() {
-  cudaFuncSetAttribute(k_momentum_tile<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)mom_smem<double, 4>());
-  cudaFuncSetAttribute(k_momentum_tile<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)mom_smem<float, 4>());
+  mom_attrs<double, 4>();
+  mom_attrs<float, 4>();
+  mom_attrs<double, 2>();
+  mom_attrs<float, 2>();
   tile_attrs<double, 8>();
   tile_attrs<float, 8>();
   tile_attrs<double, 2>();

@@ -44,7 +44,7 @@ enum { CANSFZ_ACDI = 0, CANSFZ_VOF_THINC = 1 };    /* _INTERFACE_CAPTURING_VOF *
 enum { CANSFZ_FORM_FP64 = 0, CANSFZ_FORM_MIXED = 1 };
 
 /*
- * Run parameters: the namelists &dns and &two_fluid of input.nml
+ * Run parameters: the namelists &dns, &two_fluid and &scalar of input.nml
  * (src/param.f90:91-120) plus the derived quantities and the macros that the
  * reference fixes at compile time.  Character arrays keep Fortran order, e.g.
  * cbcvel(0:1,3,3) -> cbcvel[ivel][idir][ibound], so a bind(C) derived type
@@ -76,6 +76,14 @@ typedef struct cansfz_params {
   int32_t interface_capturing;  /* CANSFZ_ACDI (default) or CANSFZ_VOF_THINC   */
   int32_t sdf_normals;          /* _SDF_NORMALS, default 1                     */
   int32_t brackbill;            /* _CAPILLARY_BRACKBILL_NORMALIZATION, default 1 */
+  /* scalar transport: _SCALAR and _BOUSSINESQ_BUOYANCY (compile-time macros
+   * of the reference, default 0), &scalar, and ka12/cp12 of &two_fluid    */
+  int32_t scalar;               /* transport the scalar s (rk_scal every step) */
+  int32_t boussinesq;           /* buoyancy term in mom_xyz_oth (needs scalar) */
+  char    cbcsca[3][2];
+  double  bcsca[3][2];
+  double  ssource;
+  double  ka12[2], cp12[2];
   /* forms of this library (no reference counterpart) */
   int32_t form;                 /* CANSFZ_FORM_FP64 (drop-in) or CANSFZ_FORM_MIXED */
   int32_t refine_sweeps;        /* mixed form: FP64-residual refinement sweeps of the
@@ -117,15 +125,22 @@ int cansfz_set_fields(cansfz_ctx* ctx, const double* u, const double* v,
 int cansfz_get_fields(cansfz_ctx* ctx, double* u, double* v, double* w,
                       double* p, double* psi, int on_device);
 /* Read one auxiliary field (phi, kappa, normx, normy, normz, psiflx_x..z,
- * psio, pn, po) by name into a halo-layout buffer.                        */
+ * psio, pn, po; s with the scalar) by name into a halo-layout buffer.     */
 int cansfz_get_aux(cansfz_ctx* ctx, const char* name, double* out, int on_device);
+/* The scalar s (halo layout) of a case created with scalar = 1: the
+ * `copyin(s)` and restart read of s (src/main.f90:316-318,327-329);
+ * read it back with cansfz_get_aux(ctx, "s", ...).  CANSFZ_ERR_UNSUPPORTED
+ * without the scalar.                                                     */
+int cansfz_set_scalar(cansfz_ctx* ctx, const double* s, int on_device);
 
-/* Finish the start-up sequence after set_fields: BCs, phi, normals,
- * curvature, Gamma and the first chkdt (src/main.f90:337-412).            */
+/* Finish the start-up sequence after set_fields: BCs (the scalar's too),
+ * phi, normals, curvature, Gamma and the first chkdt
+ * (src/main.f90:337-412).                                                  */
 int cansfz_prepare(cansfz_ctx* ctx);
 
 /* Advance n time steps: the loop body of src/main.f90:422-562 (AB2 phase
- * update, momentum, projection, pressure update, Gamma every step,
+ * update, the scalar's rk_scal when built with it, momentum, projection,
+ * pressure update, Gamma every step,
  * chkdt/chkdiv every icheck).  Captured as a CUDA graph after the first
  * call.  Returns CANSFZ_ERR_DIVERGENCE / _NAN / _DT on the reference's abort
  * conditions, after finishing the step that triggered them.              */
@@ -185,11 +200,12 @@ int cansfz_cmpt_norm_curv_youngs(cansfz_ctx* ctx, const double* psi,
 int cansfz_clip_field(cansfz_ctx* ctx, double rmin, double rmax, double* p);
 
 /* rk (src/rk.f90:16-131): momentum AB2 with the density ratio, then the
- * pressure-split, surface-tension, gravity and body-force terms.  Keeps
- * the d?dtrk/d?dtrko histories in ctx.                                     */
+ * pressure-split, surface-tension, gravity, body-force and (boussinesq)
+ * buoyancy terms.  Keeps the d?dtrk/d?dtrko histories in ctx.  s: the
+ * scalar of the buoyancy term; NULL allowed without boussinesq.            */
 int cansfz_rk(cansfz_ctx* ctx, const double rkpar[2], double dt, double dt_r,
               const double rho_av[3], const double* psi, const double* kappa,
-              const double* p, const double* pn, const double* po,
+              const double* p, const double* pn, const double* po, const double* s,
               const double* psio, const double* psiflx_x, const double* psiflx_y,
               const double* psiflx_z, double* u, double* v, double* w);
 
@@ -201,8 +217,20 @@ int cansfz_mom_xyz_ad(cansfz_ctx* ctx, const double* psiflx_x, const double* psi
                       double* dudt, double* dvdt, double* dwdt);
 int cansfz_mom_xyz_oth(cansfz_ctx* ctx, double dt_r, const double rho_av[3],
                        const double* p, const double* psi, const double* kappa,
-                       const double* pn, const double* po,
+                       const double* s, const double* pn, const double* po,
                        double* dudt, double* dvdt, double* dwdt);
+
+/* scal_ad (src/scal.f90:13-66): dsdt (interior) of the scalar s advected
+ * by rho*cp*u + (rho1*cp1 - rho2*cp2)*psiflx and diffused with the phase-
+ * weighted ka12.  rk_scal (src/rk.f90:133-191): its AB2 update of s in
+ * place (interior), keeping dsdtrk/dsdtrko in ctx.  Both need scalar = 1. */
+int cansfz_scal_ad(cansfz_ctx* ctx, const double* psiflx_x, const double* psiflx_y,
+                   const double* psiflx_z, const double* psi, const double* u,
+                   const double* v, const double* w, const double* s, double* dsdt);
+int cansfz_rk_scal(cansfz_ctx* ctx, const double rkpar[2], double dt, const double* psi,
+                   const double* u, const double* v, const double* w, const double* psio,
+                   const double* psiflx_x, const double* psiflx_y, const double* psiflx_z,
+                   double* s);
 
 /* fillps (src/fillps.f90:13-51): p = rho0*div(u)/dt on the interior */
 int cansfz_fillps(cansfz_ctx* ctx, double dti, const double* u, const double* v,
@@ -223,7 +251,8 @@ int cansfz_correc(cansfz_ctx* ctx, double dt, const double* p,
 int cansfz_updatep(cansfz_ctx* ctx, const double* pp, double* p);
 
 /* boundp / bounduvw (src/bound.f90:15-124) with the context's BCs.
- * which: 0 = cbcpre, 1 = cbcpsi, 2 = cbccur (kappa), 3..5 = cbcnor(:,:,1..3) */
+ * which: 0 = cbcpre, 1 = cbcpsi, 2 = cbccur (kappa), 3..5 = cbcnor(:,:,1..3),
+ * 6 = cbcsca (the scalar)                                                  */
 int cansfz_boundp(cansfz_ctx* ctx, int which, double* p);
 int cansfz_bounduvw(cansfz_ctx* ctx, int is_correc, double* u, double* v, double* w);
 

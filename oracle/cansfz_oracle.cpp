@@ -559,14 +559,16 @@ static void mom_xyz_ad(const Dims& D, const double dli[3], const double* dzci, c
       }
 }
 
-// mom_xyz_oth, src/mom.f90:853-1039 (CONSTANT_COEFFS_POISSON on, BALANCED off, SCALAR off)
+// mom_xyz_oth, src/mom.f90:853-1039 (CONSTANT_COEFFS_POISSON on, BALANCED off).
+// s != nullptr: the _SCALAR + _BOUSSINESQ_BUOYANCY term (src/mom.f90:1017-1024)
 static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, double dt_r,
-                        const double rho12[2], const double bforce[3], const double gacc[3],
-                        double sigma, double rho0, const double rho_av[3], const double* p,
-                        const double* psi, const double* kappa, const double* pn,
-                        const double* po, double* dudt, double* dvdt, double* dwdt,
+                        const double rho12[2], const double beta12[2], const double bforce[3],
+                        const double gacc[3], double sigma, double rho0, const double rho_av[3],
+                        const double* p, const double* psi, const double* kappa, const double* s,
+                        const double* pn, const double* po, double* dudt, double* dvdt, double* dwdt,
                         bool brackbill) {
   const double rho = rho12[1], drho = rho12[0] - rho12[1];
+  const double rhobeta = rho12[1] * beta12[1], drhobeta = rho12[0] * beta12[0] - rho12[1] * beta12[1];
   const double dxi = dli[0], dyi = dli[1];
   const double surf_factor = brackbill ? sigma * 2. / (rho12[0] + rho12[1]) : sigma;
   const double rhox_av = rho_av[0], rhoy_av = rho_av[1], rhoz_av = rho_av[2];
@@ -603,9 +605,54 @@ static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, 
         dudt_aux = dudt_aux - (dpdx_e + rhoxp / rho0 * (dpdx - dpdx_e));
         dvdt_aux = dvdt_aux - (dpdy_e + rhoyp / rho0 * (dpdy - dpdy_e));
         dwdt_aux = dwdt_aux - (dpdz_e + rhozp / rho0 * (dpdz - dpdz_e));
+        if (s) {
+          const double s_ccc = s[ccc], s_pcc = s[pcc], s_cpc = s[cpc], s_ccp = s[ccp];
+          const double factorxp = rhobeta + drhobeta * psixp;
+          const double factoryp = rhobeta + drhobeta * psiyp;
+          const double factorzp = rhobeta + drhobeta * psizp;
+          dudt_aux = dudt_aux - gacc[0] * factorxp * 0.5 * (s_pcc + s_ccc);
+          dvdt_aux = dvdt_aux - gacc[1] * factoryp * 0.5 * (s_cpc + s_ccc);
+          dwdt_aux = dwdt_aux - gacc[2] * factorzp * 0.5 * (s_ccp + s_ccc);
+        }
         dudt[D.t(i, j, k)] = dudt_aux;
         dvdt[D.t(i, j, k)] = dvdt_aux;
         dwdt[D.t(i, j, k)] = dwdt_aux;
+      }
+}
+
+// scal_ad, src/scal.f90:13-66: advection by the phase-weighted heat-capacity
+// flux rho*cp*u + (rho1*cp1 - rho2*cp2)*psiflx and diffusion with the
+// face-interpolated conductivity; dsdt on the interior.
+static void scal_ad(const Dims& D, double dxi, double dyi, const double* dzci, const double* dzfi,
+                    const double ka12[2], const double rhocp12[2], const double* fx, const double* fy,
+                    const double* fz, const double* psi, const double* u, const double* v, const double* w,
+                    const double* s, double* dsdt) {
+  const double ka = ka12[1], dka = ka12[0] - ka12[1];
+  const double rhocp = rhocp12[1], drhocp = rhocp12[0] - rhocp12[1];
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= D.n3; ++k)
+    for (int j = 1; j <= D.n2; ++j)
+      for (int i = 1; i <= D.n1; ++i) {
+        const size_t c = D.h(i, j, k), xp = D.h(i + 1, j, k), xm = D.h(i - 1, j, k), yp = D.h(i, j + 1, k),
+                     ym = D.h(i, j - 1, k), zp = D.h(i, j, k + 1), zm = D.h(i, j, k - 1);
+        const double usip = 0.5 * (rhocp * u[c] + drhocp * fx[c]) * (s[xp] + s[c]);
+        const double usim = 0.5 * (rhocp * u[xm] + drhocp * fx[xm]) * (s[xm] + s[c]);
+        const double vsjp = 0.5 * (rhocp * v[c] + drhocp * fy[c]) * (s[yp] + s[c]);
+        const double vsjm = 0.5 * (rhocp * v[ym] + drhocp * fy[ym]) * (s[ym] + s[c]);
+        const double wskp = 0.5 * (rhocp * w[c] + drhocp * fz[c]) * (s[zp] + s[c]);
+        const double wskm = 0.5 * (rhocp * w[zm] + drhocp * fz[zm]) * (s[zm] + s[c]);
+        const double kaxp = ka + dka * 0.5 * (psi[xp] + psi[c]);
+        const double kaxm = ka + dka * 0.5 * (psi[c] + psi[xm]);
+        const double kayp = ka + dka * 0.5 * (psi[yp] + psi[c]);
+        const double kaym = ka + dka * 0.5 * (psi[c] + psi[ym]);
+        const double kazp = ka + dka * 0.5 * (psi[zp] + psi[c]);
+        const double kazm = ka + dka * 0.5 * (psi[c] + psi[zm]);
+        const double dsdxp = (s[xp] - s[c]) * dxi, dsdxm = (s[c] - s[xm]) * dxi;
+        const double dsdyp = (s[yp] - s[c]) * dyi, dsdym = (s[c] - s[ym]) * dyi;
+        const double dsdzp = (s[zp] - s[c]) * dzci[k], dsdzm = (s[c] - s[zm]) * dzci[k - 1];
+        dsdt[D.t(i, j, k)] = dxi * (-usip + usim) + dyi * (-vsjp + vsjm) + dzfi[k] * (-wskp + wskm) +
+                             ((kaxp * dsdxp - kaxm * dsdxm) * dxi + (kayp * dsdyp - kaym * dsdym) * dyi +
+                              (kazp * dsdzp - kazm * dsdzm) * dzfi[k]);
       }
 }
 
@@ -918,7 +965,9 @@ struct Case {
   // fields
   std::vector<double> u, v, w, p, pp, pn, po, psi, psio, phi, kappa, normx, normy, normz, fx, fy, fz;
   std::vector<double> du, dv, dw, duo, dvo, dwo, dpsi, dpsio;
-  bool rk_first = true, rk2_first = true, chkdt_first = true;
+  // scalar (_SCALAR): s with ghosts, the dsdtrk/dsdtrko histories of rk_scal
+  std::vector<double> s, ds, dso;
+  bool rk_first = true, rk2_first = true, chkdt_first = true, rks_first = true;
   double dlmin = 0.;
   double time = 0., dt = 0., dto = 0., dt_cfl = 0., gam = 0., divtot = 0., divmax = 0.;
   int64_t istep = 0;
@@ -1030,6 +1079,11 @@ static void setup(Case& C) {
                   &C.normx, &C.normy, &C.normz, &C.fx, &C.fy, &C.fz})
     f->assign(H, 0.);
   for (auto* f : {&C.du, &C.dv, &C.dw, &C.duo, &C.dvo, &C.dwo, &C.dpsi, &C.dpsio}) f->assign(I, 0.);
+  if (P.scalar) {
+    C.s.assign(H, 0.);
+    C.ds.assign(I, 0.);
+    C.dso.assign(I, 0.);
+  }
 }
 
 // solver, src/solver.f90:19-78 (single rank: the transposes are layout changes)
@@ -1148,6 +1202,11 @@ static double chkdt(Case& C) {
     if (dti == 0.) dti = 1.;
     dtmax = 1. / dti;
     if (P.is_track_interface) dtmax = std::min(dtmax, 1. / dtipsi);
+  }
+  if (P.scalar) {  // src/chkdt.f90:88-93
+    dti = std::max(P.ka12[0] / (P.rho12[0] * P.cp12[0]), P.ka12[1] / (P.rho12[1] * P.cp12[1])) / sq(C.dlmin);
+    if (dti == 0.) dti = 1.;
+    dtmax = std::min(dtmax, 1. / dti);
   }
   return dtmax;
 }
@@ -1275,6 +1334,7 @@ static void prepare(Case& C) {
   boundp(P.cbcpre, P.bcpre, C.T, C.dl, C.dzc.data(), C.p.data(), D);
   C.pn = C.p;
   C.po = C.pn;
+  if (P.scalar) boundp(P.cbcsca, P.bcsca, C.T, C.dl, C.dzc.data(), C.s.data(), D);
   boundp(P.cbcpsi, P.bcpsi, C.T, C.dl, C.dzc.data(), C.psi.data(), D);
   if (P.sdf_normals) cmpt_phi(C);
   norm_curv_and_bcs(C);
@@ -1309,6 +1369,36 @@ static void rk_2fl(Case& C, const double tm[2]) {
   std::swap(C.dpsi, C.dpsio);
 }
 
+// rk_scal, src/rk.f90:133-191: AB2 of the scalar with the heat-capacity
+// ratio of the old and new phase fields; the scalar's ghosts are filled by
+// the caller
+static void rk_scal_fields(Case& C, const double tm[2], double dt, const double* psi, const double* u,
+                           const double* v, const double* w, const double* psio, const double* fx, const double* fy,
+                           const double* fz, double* s) {
+  const cansfz_params& P = C.P;
+  const Dims& D = C.D;
+  const double factor1 = tm[0] * dt, factor2 = tm[1] * dt, factor12 = factor1 + factor2;
+  const double rhocp12[2] = {P.rho12[0] * P.cp12[0], P.rho12[1] * P.cp12[1]};
+  scal_ad(D, C.dli[0], C.dli[1], C.dzci.data(), C.dzfi.data(), P.ka12, rhocp12, fx, fy, fz, psi, u, v, w, s,
+          C.ds.data());
+  if (C.rks_first) { C.dso = C.ds; C.rks_first = false; }
+  const double rhocp = rhocp12[1], drhocp = rhocp12[0] - rhocp12[1];
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= D.n3; ++k)
+    for (int j = 1; j <= D.n2; ++j)
+      for (int i = 1; i <= D.n1; ++i) {
+        const size_t c = D.h(i, j, k), t = D.t(i, j, k);
+        const double rhocp_p = rhocp + drhocp * psi[c];
+        const double rhocp_n = rhocp + drhocp * psio[c];
+        s[c] = s[c] * rhocp_n / rhocp_p + (factor1 * C.ds[t] + factor2 * C.dso[t] + factor12 * P.ssource) / rhocp_p;
+      }
+  std::swap(C.ds, C.dso);
+}
+static void rk_scal(Case& C, const double tm[2]) {
+  rk_scal_fields(C, tm, C.dt, C.psi.data(), C.u.data(), C.v.data(), C.w.data(), C.psio.data(), C.fx.data(),
+                 C.fy.data(), C.fz.data(), C.s.data());
+}
+
 // rk, src/rk.f90:16-131
 static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3]) {
   const cansfz_params& P = C.P;
@@ -1336,9 +1426,9 @@ static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3])
         w[c] = w[c] * rhoz_n / rhoz_p + (factor1 * C.dw[t] + factor2 * C.dwo[t]) / rhoz_p;
       }
   std::swap(C.du, C.duo); std::swap(C.dv, C.dvo); std::swap(C.dw, C.dwo);
-  mom_xyz_oth(D, C.dli, C.dzci.data(), dt_r, P.rho12, P.bforce, P.gacc, P.sigma, C.rho0, rho_av, C.p.data(),
-              C.psi.data(), C.kappa.data(), C.pn.data(), C.po.data(), C.du.data(), C.dv.data(), C.dw.data(),
-              P.brackbill != 0);
+  mom_xyz_oth(D, C.dli, C.dzci.data(), dt_r, P.rho12, P.beta12, P.bforce, P.gacc, P.sigma, C.rho0, rho_av,
+              C.p.data(), C.psi.data(), C.kappa.data(), P.scalar && P.boussinesq ? C.s.data() : nullptr, C.pn.data(),
+              C.po.data(), C.du.data(), C.dv.data(), C.dw.data(), P.brackbill != 0);
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= D.n3; ++k)
     for (int j = 1; j <= D.n2; ++j)
@@ -1373,6 +1463,10 @@ static int step(Case& C) {
     std::fill(C.fx.begin(), C.fx.end(), 0.);
     std::fill(C.fy.begin(), C.fy.end(), 0.);
     std::fill(C.fz.begin(), C.fz.end(), 0.);
+  }
+  if (P.scalar) {  // src/main.f90:460-463
+    rk_scal(C, tm);
+    boundp(P.cbcsca, P.bcsca, C.T, C.dl, C.dzc.data(), C.s.data(), D);
   }
   if (!P.is_solve_ns) {
     initflow_prescribed(C, C.time);
@@ -1546,6 +1640,40 @@ static void initflow_prescribed(Case& C, double time) {
   initflow(C, C.inivel.c_str(), time, C.u.data(), C.v.data(), C.w.data(), C.p.data());
 }
 
+// initscal, src/initflow.f90:363-429, on the interior ('cou', 'dhc', 'uni',
+// 'zer'; no noise or mean set, as there).  The 'dhc' x coordinate
+// (ii-0.5)*dl(1)/l(1) starts from a default-real difference, exact here.
+static int initscal(const Case& C, const char* inisca, double* s) {
+  const cansfz_params& P = C.P;
+  const Dims& D = C.D;
+  const std::string nm(inisca);
+  std::vector<double> s1d(D.n3 + 1, 0.);
+  const double sref = 0.5 * (P.bcsca[2][0] + P.bcsca[2][1]);
+  if (nm == "cou" || nm == "dhc") {
+    for (int k = 1; k <= D.n3; ++k) {
+      const double z = C.zc[k] / P.l[2];
+      double v = .5 * (1. - 2. * z) * 1.;
+      v = v + 0.5;
+      s1d[k] = P.bcsca[2][0] * v + P.bcsca[2][1] * (1. - v);
+    }
+  } else if (nm == "uni") {
+    for (int k = 1; k <= D.n3; ++k) s1d[k] = sref;
+  } else if (nm != "zer") {
+    return CANSFZ_ERR_ARG;
+  }
+  for (int k = 1; k <= D.n3; ++k)
+    for (int j = 1; j <= D.n2; ++j)
+      for (int i = 1; i <= D.n1; ++i) s[D.h(i, j, k)] = s1d[k];
+  if (nm == "dhc")
+    for (int k = 1; k <= D.n3; ++k)
+      for (int j = 1; j <= D.n2; ++j)
+        for (int i = 1; i <= D.n1; ++i) {
+          const double xx = (double)((float)i - 0.5f) * C.dl[0] / P.l[0];
+          s[D.h(i, j, k)] = ((1. - xx) * P.bcsca[0][0] + xx * P.bcsca[0][1]);
+        }
+  return CANSFZ_OK;
+}
+
 }  // namespace orc
 
 // ===========================================================================
@@ -1594,6 +1722,8 @@ static std::vector<double>* field_by_name(Case* C, const char* name) {
   if (s == "dvdtrko") return &C->dvo;
   if (s == "dwdtrko") return &C->dwo;
   if (s == "dpsidtrko") return &C->dpsio;
+  if (s == "s" && C->P.scalar) return &C->s;
+  if (s == "dsdtrko" && C->P.scalar) return &C->dso;
   return nullptr;
 }
 
@@ -1623,6 +1753,19 @@ int orc_initflow(void* h, const char* inivel, double time) {
   C->inivel = inivel;
   initflow(*C, inivel, time, C->u.data(), C->v.data(), C->w.data(), C->p.data());
   return 0;
+}
+int orc_rk_scal(void* h, const double* rkpar, double dt, const double* psi, const double* u, const double* v,
+                const double* w, const double* psio, const double* fx, const double* fy, const double* fz,
+                double* s) {
+  Case* C = (Case*)h;
+  if (!C->P.scalar) return CANSFZ_ERR_ARG;
+  rk_scal_fields(*C, rkpar, dt, psi, u, v, w, psio, fx, fy, fz, s);
+  return CANSFZ_OK;
+}
+int orc_initscal(void* h, const char* inisca) {
+  Case* C = (Case*)h;
+  if (!C->P.scalar) return CANSFZ_ERR_ARG;
+  return initscal(*C, inisca, C->s.data());
 }
 void orc_prepare(void* h) { prepare(*(Case*)h); }
 int orc_step(void* h, int nsteps) {
@@ -1687,11 +1830,20 @@ void orc_mom_xyz_ad(void* h, const double* fx, const double* fy, const double* f
              dvdt, dwdt);
 }
 void orc_mom_xyz_oth(void* h, double dt_r, const double* rho_av, const double* p, const double* psi,
-                     const double* kappa, const double* pn, const double* po, double* dudt, double* dvdt,
-                     double* dwdt) {
+                     const double* kappa, const double* s, const double* pn, const double* po, double* dudt,
+                     double* dvdt, double* dwdt) {
   Case* C = (Case*)h;
-  mom_xyz_oth(C->D, C->dli, C->dzci.data(), dt_r, C->P.rho12, C->P.bforce, C->P.gacc, C->P.sigma, C->rho0, rho_av, p,
-              psi, kappa, pn, po, dudt, dvdt, dwdt, C->P.brackbill != 0);
+  const double* sb = C->P.scalar && C->P.boussinesq ? s : nullptr;
+  mom_xyz_oth(C->D, C->dli, C->dzci.data(), dt_r, C->P.rho12, C->P.beta12, C->P.bforce, C->P.gacc, C->P.sigma,
+              C->rho0, rho_av, p, psi, kappa, sb, pn, po, dudt, dvdt, dwdt, C->P.brackbill != 0);
+}
+void orc_scal_ad(void* h, const double* fx, const double* fy, const double* fz, const double* psi, const double* u,
+                 const double* v, const double* w, const double* s, double* dsdt) {
+  Case* C = (Case*)h;
+  const cansfz_params& P = C->P;
+  const double rhocp12[2] = {P.rho12[0] * P.cp12[0], P.rho12[1] * P.cp12[1]};
+  scal_ad(C->D, C->dli[0], C->dli[1], C->dzci.data(), C->dzfi.data(), P.ka12, rhocp12, fx, fy, fz, psi, u, v, w, s,
+          dsdt);
 }
 void orc_fillps(void* h, double dti, const double* u, const double* v, const double* w, double* p) {
   Case* C = (Case*)h;
@@ -1708,7 +1860,7 @@ void orc_correc(void* h, double dt, const double* p, double* u, double* v, doubl
 }
 void orc_updatep(void* h, const double* pp, double* p) { updatep(((Case*)h)->D, pp, p); }
 void orc_clip_field(void* h, double rmin, double rmax, double* p) { clip_field(((Case*)h)->D, rmin, rmax, p); }
-// which: 0 cbcpre, 1 cbcpsi, 2 cbccur, 3..5 cbcnor(:,:,1..3)
+// which: 0 cbcpre, 1 cbcpsi, 2 cbccur, 3..5 cbcnor(:,:,1..3), 6 cbcsca
 void orc_boundp(void* h, int which, double* p) {
   Case* C = (Case*)h;
   const cansfz_params& P = C->P;
@@ -1717,6 +1869,7 @@ void orc_boundp(void* h, int which, double* p) {
   if (which == 1) { cbc = P.cbcpsi; bc = P.bcpsi; }
   else if (which == 2) { cbc = C->cbccur; bc = C->bccur; }
   else if (which >= 3 && which <= 5) { cbc = P.cbcnor[which - 3]; bc = P.bcnor[which - 3]; }
+  else if (which == 6) { cbc = P.cbcsca; bc = P.bcsca; }
   boundp(cbc, bc, C->T, C->dl, C->dzc.data(), p, C->D);
 }
 void orc_bounduvw(void* h, int is_correc, double* u, double* v, double* w) {

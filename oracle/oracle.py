@@ -65,7 +65,10 @@ def lib():
             "orc_vof_thinc_cmpt_phi": (None, [V, D, P, P]),
             "orc_cmpt_norm_curv_youngs": (None, [V] + [P] * 5),
             "orc_mom_xyz_ad": (None, [V] + [P] * 10),
-            "orc_mom_xyz_oth": (None, [V, D] + [P] * 9),
+            "orc_mom_xyz_oth": (None, [V, D] + [P] * 10),
+            "orc_scal_ad": (None, [V] + [P] * 9),
+            "orc_initscal": (ct.c_int, [V, ct.c_char_p]),
+            "orc_rk_scal": (ct.c_int, [V, P, D] + [P] * 9),
             "orc_fillps": (None, [V, D, P, P, P, P]),
             "orc_updt_rhs_b": (None, [V, P]),
             "orc_solver": (None, [V, P]),
@@ -129,7 +132,7 @@ class Case:
         return np.zeros(self.hshape, order="F")
 
     def get(self, name: str) -> np.ndarray:
-        interior = name in ("dudtrko", "dvdtrko", "dwdtrko", "dpsidtrko")
+        interior = name in ("dudtrko", "dvdtrko", "dwdtrko", "dpsidtrko", "dsdtrko")
         a = np.zeros(self.n if interior else self.hshape, order="F")
         rc = lib().orc_get_field(self.h, name.encode(), ptr(a))
         if rc:
@@ -150,6 +153,11 @@ class Case:
 
     def initflow(self, inivel: str, time: float = 0.0):
         lib().orc_initflow(self.h, inivel.encode(), float(time))
+
+    def initscal(self, inisca: str):
+        rc = lib().orc_initscal(self.h, inisca.encode())
+        if rc:
+            raise ValueError(f"initscal: invalid name '{inisca}' or no scalar in this case")
 
     def set_inivel(self, inivel: str):
         lib().orc_set_inivel(self.h, inivel.encode())

@@ -5,6 +5,7 @@ conditions against the oracle's restatement of init2fl/initflow."""
 import ctypes as ct
 import os
 import re
+import subprocess
 
 import numpy as np
 
@@ -29,10 +30,27 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(lib.SIGNATURES)
 
 
-def test_params_layout_matches_c():
-    assert ct.sizeof(params.Params) == 720
-    assert params.Params.bcvel.offset == 112 and params.Params.sigma.offset == 584
-    assert ct.sizeof(lib.Diag) == 120
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and offsetof of the header's struct, from a C program built
+    against include/cansfz.h."""
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cansfz.h"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    return [int(x) for x in out]
+
+
+def test_params_layout_matches_c(tmp_path):
+    for cls, struct in ((params.Params, "cansfz_params"), (lib.Diag, "cansfz_diag")):
+        names = [f[0] for f in cls._fields_]
+        got = _c_layout(tmp_path, struct, names)
+        assert got[0] == ct.sizeof(cls), struct
+        assert got[1:] == [getattr(cls, n).offset for n in names], struct
 
 
 def test_status_strings_and_no_device_error():
@@ -130,3 +148,48 @@ def test_divfree_velocity_is_discretely_solenoidal():
     rms = np.sqrt(np.mean(u[1:-1, 1:-1, 1:-1] ** 2))
     assert 0.05 < rms < 0.2
     assert m[0] < 1e-12
+
+
+def test_initscal_matches_oracle():
+    p = _case_params(16, 6, 20, "NNPPNN", l=(1.0, 0.5, 1.5), gr=1.1)
+    p.scalar = 1
+    p.bcsca[:] = [-0.5, 0.5, 0.0, 0.0, 0.25, 0.75]
+    for name in ("zer", "uni", "cou", "dhc"):
+        a = init.initscal(p, name)
+        c = O.Case(p)
+        c.initscal(name)
+        assert np.array_equal(a[1:-1, 1:-1, 1:-1], c.get("s")[1:-1, 1:-1, 1:-1]), name
+    # 'dhc' is the x profile between the x boundary values, centred cells
+    s = init.initscal(p, "dhc")[1:-1, 1, 1]
+    assert np.allclose(s, -0.5 + (np.arange(16) + 0.5) / 16)
+    try:
+        init.initscal(p, "xyz")
+        raise AssertionError("invalid name accepted")
+    except ValueError:
+        pass
+
+
+def test_build_conf_switches(reference_dir, tmp_path):
+    # the reference's differentially heated cavity builds with _SCALAR and
+    # _BOUSSINESQ_BUOYANCY; its &scalar group and ka12/cp12 fill the params
+    case = os.path.join(reference_dir, "tests", "differentially_heated_cavity")
+    nl = namelist.read(os.path.join(case, "input.nml"))
+    namelist.apply_build_conf(nl, os.path.join(case, "build.conf"))
+    p = params.from_namelist(nl)
+    assert p.scalar == 1 and p.boussinesq == 1 and p.interface_capturing == params.ACDI
+    assert bytes(p.cbcsca) == b"DDPPNN" and list(p.bcsca)[:2] == [-0.5, 0.5]
+    assert nl["inisca"] == "dhc" and p.ka12[0] == p.ka12[1] > 0 and list(p.cp12) == [1.0, 1.0]
+    # _BOUSSINESQ_BUOYANCY without _SCALAR has no effect, as in the reference
+    conf = tmp_path / "build.conf"
+    conf.write_text("SCALAR=0   # off\nBOUSSINESQ_BUOYANCY=1\nINTERFACE_CAPTURING_VOF=1\nSDF_NORMALS=0\n")
+    nl = namelist.apply_build_conf(namelist.defaults(), str(conf))
+    p = params.from_namelist(nl)
+    assert p.scalar == 0 and p.boussinesq == 0 and p.interface_capturing == params.VOF_THINC
+    assert p.sdf_normals == 0 and p.brackbill == 1  # absent: flags.mk's default 1
+    for bad in ("CONSTANT_COEFFS_POISSON=0\n", "SINGLE_PRECISION=1\n"):
+        conf.write_text(bad)
+        try:
+            namelist.apply_build_conf(namelist.defaults(), str(conf))
+            raise AssertionError(bad)
+        except ValueError:
+            pass

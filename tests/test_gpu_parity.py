@@ -126,8 +126,8 @@ def test_momentum_procedures(small):
     for a, b in zip(outg, outo):
         assert _rel(a.get(), b) < 1e-12
     rho_av = [0.0, 0.0, 3.5]
-    g.call("mom_xyz_oth", 0.9, rho_av, dev["p"], dev["psi"], dev["k"], dev["pn"], dev["po"], *outg)
-    o.call("mom_xyz_oth", 0.9, np.array(rho_av), pp, psi, kap, pn, po, *outo)
+    g.call("mom_xyz_oth", 0.9, rho_av, dev["p"], dev["psi"], dev["k"], None, dev["pn"], dev["po"], *outg)
+    o.call("mom_xyz_oth", 0.9, np.array(rho_av), pp, psi, kap, None, pn, po, *outo)
     for a, b in zip(outg, outo):
         assert _rel(a.get(), b) < 1e-12
 

@@ -9,7 +9,14 @@ the parity checker of the CUDA path.
   tests/lid_driven_cavity, run through the oracle with the reference's own
   input files and acceptance criteria (read from the reference checkout at
   test time; skipped where it is absent).
+* tests/differentially_heated_cavity (the scalar with Boussinesq buoyancy):
+  its 50000 steps take the oracle about five minutes, so the full run is
+  recorded in tests/golden/dhc_oracle.json by tests/golden/make_dhc.py and
+  checked there against the test's acceptance value; the default suite
+  re-runs its first 500 steps against that record, and the full run repeats
+  with CANSFZ_LONG_TESTS=1.
 """
+import json
 import os
 
 import numpy as np
@@ -160,12 +167,17 @@ def test_uniform_phase_known_answers():
 
 def _run_reference_case(case_dir):
     nl = namelist.read(os.path.join(case_dir, "input.nml"))
+    conf = os.path.join(case_dir, "build.conf")
+    if os.path.exists(conf):
+        namelist.apply_build_conf(nl, conf)
     p = params.from_namelist(nl)
     c = O.Case(p)
     sph_file = os.path.join(case_dir, "spheres.in")
     sph = np.loadtxt(sph_file, ndmin=2) if os.path.exists(sph_file) else None
     c.init2fl(str(nl["inipsi"]), sph)
     c.initflow(str(nl["inivel"]))
+    if p.scalar:
+        c.initscal(str(nl["inisca"]))
     c.prepare()
     stop = nl["stop_type"]
     while True:
@@ -233,3 +245,62 @@ def test_reference_lid_driven_cavity(reference_dir):
     data = w[0]
     interp = np.interp(ref_v[:, 0], yp, 0.5 * (data[:, islice] + data[:, islice + 1]))
     np.testing.assert_allclose(interp, ref_v[:, 1], rtol=1e-1, atol=1e-1)
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _dhc_nusselt(c):
+    """The Nusselt number of tests/differentially_heated_cavity/test.py:9-13:
+    (s - tw)/(2*xp(1)) * (2*zp(1)) summed over the hot wall's first column."""
+    p = c.params
+    s = c.get("s")[1:-1, 1:-1, 1:-1]
+    tw = p.bcsca[0]
+    xp0, zp0 = 0.5 * p.l[0] / p.ng[0], 0.5 * p.l[2] / p.ng[2]
+    return float((1.0 / p.l[0]) * np.sum((s[0, 0, :] - tw) / (2.0 * xp0) * (2.0 * zp0)) * p.l[0] / (-tw))
+
+
+def test_dhc_record_and_first_steps():
+    """The recorded 50000-step oracle run meets the reference test's
+    acceptance value; the oracle still reproduces the record's 500th step."""
+    gold = json.load(open(os.path.join(GOLDEN, "dhc_oracle.json")))
+    nu = gold["oracle"][str(gold["steps"])]["nusselt"]
+    ref = gold["nusselt_reference"]
+    assert abs(nu - ref) <= gold["atol"] + gold["rtol"] * abs(ref)
+    nl = namelist.read(os.path.join(GOLDEN, "dhc_case.nml"))
+    p = params.from_namelist(nl)
+    c = O.Case(p)
+    c.init2fl(str(nl["inipsi"]))
+    c.initflow(str(nl["inivel"]))
+    c.initscal(str(nl["inisca"]))
+    c.prepare()
+    assert c.step(500) == 0
+    rec = gold["oracle"]["500"]
+    assert abs(_dhc_nusselt(c) - rec["nusselt"]) <= 1e-12 * abs(rec["nusselt"])
+    assert c.diag().time == rec["time"]
+
+
+def test_dhc_fixture_is_the_reference_input(reference_dir):
+    case = os.path.join(reference_dir, "tests", "differentially_heated_cavity")
+    nl = namelist.read(os.path.join(case, "input.nml"))
+    namelist.apply_build_conf(nl, os.path.join(case, "build.conf"))
+    a = params.from_namelist(nl)
+    b = params.from_namelist(namelist.read(os.path.join(GOLDEN, "dhc_case.nml")))
+    assert bytes(a) == bytes(b)
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(not os.environ.get("CANSFZ_LONG_TESTS"), reason="five minutes of oracle steps; the record "
+                    "in tests/golden/dhc_oracle.json holds this run (CANSFZ_LONG_TESTS=1 repeats it)")
+def test_reference_differentially_heated_cavity(reference_dir):
+    """tests/differentially_heated_cavity of the reference (50000 steps,
+    _SCALAR and _BOUSSINESQ_BUOYANCY from its build.conf): the hot wall's
+    Nusselt number vs the acceptance value of its test.py, rtol = atol = 1e-2."""
+    import re
+
+    case = os.path.join(reference_dir, "tests", "differentially_heated_cavity")
+    c, nl, d = _run_reference_case(case)
+    assert d.istep == int(nl["nstep"])
+    txt = open(os.path.join(case, "test.py")).read()
+    ref = float(re.search(r"nusselt_ref\s*=\s*([0-9.eE+-]+)", txt).group(1))
+    np.testing.assert_allclose([_dhc_nusselt(c)], [ref], rtol=1e-2, atol=1e-2)
