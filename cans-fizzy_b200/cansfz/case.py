@@ -106,7 +106,7 @@ class Case:
     def get(self, name: str) -> np.ndarray:
         if name in ("u", "v", "w", "p", "psi"):
             return self.get_fields()[("u", "v", "w", "p", "psi").index(name)]
-        interior = name.endswith("dtrko")
+        interior = name.endswith("dtrko") or name.startswith("surf")
         shape = self.n if interior else self.hshape
         out = np.zeros(int(np.prod(shape)))
         _L.check(self.lib.cansfz_get_aux(self.h, name.encode(), out.ctypes.data_as(ct.c_void_p), 0), name)

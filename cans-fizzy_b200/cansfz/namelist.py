@@ -101,6 +101,7 @@ SCHEMA = {
         "interface_capturing_vof": Var("l", (), (), False),
         "sdf_normals": Var("l", (), (), True),
         "capillary_brackbill_normalization": Var("l", (), (), True),
+        "balanced_capillary_pressure_split": Var("l", (), (), False),
         "scalar": Var("l", (), (), False),
         "boussinesq_buoyancy": Var("l", (), (), False),
         "acdi_gam_factor": Var("r", (), (), 1.0),
@@ -278,6 +279,7 @@ BUILD_DEFINES = {
     "INTERFACE_CAPTURING_VOF": ("interface_capturing_vof", False),
     "SDF_NORMALS": ("sdf_normals", True),
     "CAPILLARY_BRACKBILL_NORMALIZATION": ("capillary_brackbill_normalization", True),
+    "BALANCED_CAPILLARY_PRESSURE_SPLIT": ("balanced_capillary_pressure_split", False),
     "SCALAR": ("scalar", False),
     "BOUSSINESQ_BUOYANCY": ("boussinesq_buoyancy", False),
 }

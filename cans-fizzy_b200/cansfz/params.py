@@ -44,6 +44,7 @@ class Params(ct.Structure):
         ("interface_capturing", ct.c_int32),
         ("sdf_normals", ct.c_int32),
         ("brackbill", ct.c_int32),
+        ("balanced", ct.c_int32),
         ("scalar", ct.c_int32),
         ("boussinesq", ct.c_int32),
         ("cbcsca", ct.c_char * 6),
@@ -119,6 +120,7 @@ def from_namelist(nl: _nml.Namelist) -> Params:
     p.interface_capturing = VOF_THINC if vof else ACDI
     p.sdf_normals = int(bool(nl["sdf_normals"]))
     p.brackbill = int(bool(nl["capillary_brackbill_normalization"]))
+    p.balanced = int(bool(nl["balanced_capillary_pressure_split"]))
     p.scalar = int(bool(nl["scalar"]))
     p.boussinesq = int(bool(nl["boussinesq_buoyancy"]))
     p.cbcsca = _chars(nl["cbcsca"])

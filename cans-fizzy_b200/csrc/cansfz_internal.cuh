@@ -84,6 +84,7 @@ struct Phys {
   double ssource;
   double ka_rhocp_max;          // maxval(ka12/(rho12*cp12)), the chkdt constant
   double rhobeta, drhobeta;     // rho2*beta2, rho1*beta1 - rho2*beta2
+  int balanced;                 // _BALANCED_CAPILLARY_PRESSURE_SPLIT
 };
 
 // ---------------------------------------------------------------------------
@@ -164,6 +165,19 @@ struct Launch {
   Recorder* rec = nullptr;
 };
 
+// the surface-tension histories surf?_n, surf?_o of the balanced capillary
+// split (_BALANCED_CAPILLARY_PRESSURE_SPLIT, src/mom.f90:982-1032), interior
+// layout: a kernel reads n and o, writes the new force into out_n and, where
+// out_o is set, n into out_o (out_n = n, out_o = o: the reference's in-place
+// update; out_n = o and no out_o: the new force into the old slot, the
+// parity flip of the step then swaps the roles)
+struct SurfSplit {
+  const double* n[3];
+  const double* o[3];
+  double* out_n[3];
+  double* out_o[3];
+};
+
 // optional stage marker of the step profiler (CUDA events between stages)
 struct StageMark {
   void (*fn)(void* arg, const char* name);
@@ -202,7 +216,7 @@ void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* 
                    const double* w, const double* psi, double* du, double* dv, double* dw);
 void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
                     const double* p, const double* psi, const double* kappa, const double* s,
-                    const double* pn, const double* po, double* du, double* dv, double* dw);
+                    const SurfSplit* sp, const double* pn, const double* po, double* du, double* dv, double* dw);
 void launch_rk_update1(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc,
                        const double* psio, const double* psi, const double* du,
                        const double* dv, const double* dw, double* duo, double* dvo,
@@ -214,8 +228,8 @@ void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const 
                            const double* u, const double* v, const double* w,
                            const double* psi, const double* psio, const double* fx,
                            const double* fy, const double* fz, const double* p,
-                           const double* po, const double* kappa, const double* s, double* duo,
-                           double* dvo, double* dwo, double* uo, double* vo, double* wo);
+                           const double* po, const double* kappa, const double* s, const SurfSplit* sp,
+                           double* duo, double* dvo, double* dwo, double* uo, double* vo, double* wo);
 // scalar transport: scal_ad (src/scal.f90:13-66), and scal_ad with the AB2
 // update of rk_scal (src/rk.f90:133-191) in one pass (s_out interior; the
 // new dsdt into `hist`, the dsdtrko slot)
@@ -291,8 +305,10 @@ template <typename TI>
 void launch_momentum_t(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                        const double* v, const double* w, const double* psi, const double* psio, const TI* fx,
                        const TI* fy, const TI* fz, const double* p, const double* po, const TI* kappa,
-                       const double* s, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo, double* wo);
+                       const double* s, const SurfSplit* sp, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo,
+                       double* wo);
 void tiles_set_attributes();
+void momentum_set_attributes();
 void launch_poisson(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                     double* p, const StageMark* mk = nullptr);
 // mixed form: FP32 spectral solve (dst = S(src) or dst += S(src)) and the

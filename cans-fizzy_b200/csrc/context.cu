@@ -91,6 +91,8 @@ struct cansfz_ctx {
   double *tu = nullptr, *tv = nullptr, *tw_ = nullptr, *tpsi = nullptr;     // per-procedure scratch (interior)
   // scalar (_SCALAR): s by parity like u,v,w,psi; the dsdtrko history (interior)
   double *s[2]{}, *hs = nullptr;
+  // balanced capillary split: surf?_n = surf[cur][?], surf?_o = surf[cur^1][?] (interior)
+  double* surf[2][3]{};
   int cur = 0;  // index of the current u,v,w,psi,s and of p (= pn); po = p[cur^1]
   // Poisson solver (initsolver)
   PoissonPlan pl{};
@@ -597,13 +599,20 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
         launch_bulk_mean(L, g, c->ph, sc, c->partial, d + 1, c->d_grid + (d == 2 ? 5 : 4) * (g.nz + 2), c->psi[b]);
     // rk: the whole momentum update in one pass (the buoyancy reads the new scalar)
     const double* sb = c->ph.boussinesq ? c->s[b] : nullptr;
+    // balanced split: read surf[a] (n) and surf[b] (o), the new force into
+    // surf[b], which the parity flip makes the next step's n
+    SurfSplit split{};
+    if (c->ph.balanced)
+      for (int d = 0; d < 3; ++d) { split.n[d] = c->surf[a][d]; split.o[d] = c->surf[b][d]; split.out_n[d] = c->surf[b][d]; }
+    const SurfSplit* sp = c->ph.balanced ? &split : nullptr;
     if (c->mixed)
       launch_momentum_t<float>(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fxf, c->fyf,
-                               c->fzf, c->p[a], c->p[b], c->kappaf, sb, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
+                               c->fzf, c->p[a], c->p[b], c->kappaf, sb, sp, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
                                c->w[b]);
     else
       launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy,
-                            c->fz, c->p[a], c->p[b], c->kappa, sb, c->hu, c->hv, c->hw, c->u[b], c->v[b], c->w[b]);
+                            c->fz, c->p[a], c->p[b], c->kappa, sb, sp, c->hu, c->hv, c->hw, c->u[b], c->v[b],
+                            c->w[b]);
     MARK("momentum");
     run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
     MARK("bc_uvw");
@@ -729,6 +738,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   c->L.st = c->st;
   poisson_set_attributes();
   tiles_set_attributes();
+  momentum_set_attributes();
   for (int d = 0; d < 3; ++d) c->n[d] = P.ng[d];
   const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
   for (int d = 0; d < 3; ++d) {
@@ -798,6 +808,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   ph.ka_rhocp_max = std::max(P.ka12[0] / (P.rho12[0] * P.cp12[0]), P.ka12[1] / (P.rho12[1] * P.cp12[1]));
   ph.rhobeta = P.rho12[1] * P.beta12[1];
   ph.drhobeta = P.rho12[0] * P.beta12[0] - P.rho12[1] * P.beta12[1];
+  ph.balanced = P.balanced ? 1 : 0;
   // acdi_set_epsilon (src/acdi.f90:16-30) and the THINC beta (src/param.f90:178)
   double dlmax = std::max(c->dl[0], c->dl[1]);
   for (int k = 0; k <= nz + 1; ++k) dlmax = std::max(dlmax, 1. / c->dzfi[k]);
@@ -812,6 +823,10 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
     if ((rc = dalloc(c, f, H))) return fail(rc);
   for (double** f : {&c->hpsi, &c->hu, &c->hv, &c->hw, &c->tu, &c->tv, &c->tw_, &c->tpsi})
     if ((rc = dalloc(c, f, I))) return fail(rc);
+  if (P.balanced)  // zero, as src/main.f90:205-213 sets them
+    for (int q = 0; q < 2; ++q)
+      for (int d = 0; d < 3; ++d)
+        if ((rc = dalloc(c, &c->surf[q][d], I))) return fail(rc);
   if (P.scalar) {
     for (int q = 0; q < 2; ++q)
       if ((rc = dalloc(c, &c->s[q], H))) return fail(rc);
@@ -925,6 +940,11 @@ int cansfz_get_aux(cansfz_ctx* c, const char* name, double* out, int on_device) 
   else if (s == "dvdtrko") { src = c->hv; n = c->g.tsize(); }
   else if (s == "dwdtrko") { src = c->hw; n = c->g.tsize(); }
   else if (s == "s" && c->P.scalar) src = c->s[a];
+  else if (c->P.balanced && s.size() == 7 && s.compare(0, 4, "surf") == 0 && s[5] == '_' &&
+           (s[4] == 'x' || s[4] == 'y' || s[4] == 'z') && (s[6] == 'n' || s[6] == 'o')) {
+    src = c->surf[s[6] == 'n' ? a : a ^ 1][s[4] - 'x'];
+    n = c->g.tsize();
+  }
   else if (s == "dsdtrko" && c->P.scalar) { src = c->hs; n = c->g.tsize(); }
   else return CANSFZ_ERR_ARG;
   if (c->mixed) {  // FP32 intermediates, widened into scratch for the caller
@@ -1391,6 +1411,19 @@ int cansfz_mom_xyz_ad(cansfz_ctx* c, const double* fx, const double* fy, const d
   return CANSFZ_OK;
 }
 
+// the balanced-split histories of a per-procedure call: the reference's
+// in-place update (surf_o = surf_n, surf_n = new) on the current slots
+static SurfSplit call_split(const cansfz_ctx* c) {
+  SurfSplit sp{};
+  if (!c->ph.balanced) return sp;
+  const int a = c->cur;
+  for (int d = 0; d < 3; ++d) {
+    sp.n[d] = sp.out_n[d] = c->surf[a][d];
+    sp.o[d] = sp.out_o[d] = c->surf[a ^ 1][d];
+  }
+  return sp;
+}
+
 int cansfz_mom_xyz_oth(cansfz_ctx* c, double dt_r, const double rho_av[3], const double* p, const double* psi,
                        const double* kappa, const double* s, const double* pn, const double* po, double* dudt,
                        double* dvdt, double* dwdt) {
@@ -1400,7 +1433,9 @@ int cansfz_mom_xyz_oth(cansfz_ctx* c, double dt_r, const double rho_av[3], const
   for (int d = 0; d < 3; ++d) h.rho_av[d] = rho_av[d];
   if (int rc = call_scalars(c, h)) return rc;
   if (c->ph.boussinesq && !s) return CANSFZ_ERR_ARG;
-  launch_mom_oth(c->L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr, pn, po, dudt, dvdt,
+  const SurfSplit sp = call_split(c);
+  launch_mom_oth(c->L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr,
+                 c->ph.balanced ? &sp : nullptr, pn, po, dudt, dvdt,
                  dwdt);
   CK(cudaGetLastError());
   return CANSFZ_OK;
@@ -1425,7 +1460,9 @@ int cansfz_rk(cansfz_ctx* c, const double rkpar[2], double dt, double dt_r, cons
   launch_copy(L, (size_t)c->g.tsize(), c->tu, c->hu);
   launch_copy(L, (size_t)c->g.tsize(), c->tv, c->hv);
   launch_copy(L, (size_t)c->g.tsize(), c->tw_, c->hw);
-  launch_mom_oth(L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr, pn, po, c->tu, c->tv,
+  const SurfSplit sp = call_split(c);
+  launch_mom_oth(L, c->g, c->ph, c->sc_call, p, psi, kappa, c->ph.boussinesq ? s : nullptr,
+                 c->ph.balanced ? &sp : nullptr, pn, po, c->tu, c->tv,
                  c->tw_);
   launch_rk_update2(L, c->g, c->ph, c->sc_call, psi, c->tu, c->tv, c->tw_, u, v, w);
   c->first_rk_call = false;

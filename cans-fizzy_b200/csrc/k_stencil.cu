@@ -405,12 +405,13 @@ __device__ __forceinline__ AdOut mom_ad_cell(const Geo& g, const Phys& ph, int i
 }
 
 // mom_xyz_oth, src/mom.f90:912-1038 (CONSTANT_COEFFS_POISSON, Brackbill per
-// Phys; with s, the Boussinesq buoyancy of src/mom.f90:1017-1024)
+// Phys; with s, the Boussinesq buoyancy of src/mom.f90:1017-1024; with sp,
+// the balanced capillary split of src/mom.f90:982-1032)
 __device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, double dt_r, const double* rho_av,
                                               int i, int j, int k, const double* __restrict__ p,
                                               const double* __restrict__ psi, const double* __restrict__ kappa,
-                                              const double* __restrict__ s, const double* __restrict__ pn,
-                                              const double* __restrict__ po) {
+                                              const double* __restrict__ s, const SurfSplit* sp,
+                                              const double* __restrict__ pn, const double* __restrict__ po) {
   const double rho = ph.rho12[1], drho = ph.rho12[0] - ph.rho12[1];
   const double dxi = g.dxi, dyi = g.dyi, dzci_c = g.dzci[k];
   const int ccc = g.h(i, j, k), pcc = ccc + 1, cpc = ccc + g.sx, ccp = ccc + g.sxy;
@@ -433,13 +434,29 @@ __device__ __forceinline__ AdOut mom_oth_cell(const Geo& g, const Phys& ph, doub
   if (ph.brackbill) {  // _CAPILLARY_BRACKBILL_NORMALIZATION
     skappaxp = skappaxp * rhoxp; skappayp = skappayp * rhoyp; skappazp = skappazp * rhozp;
   }
-  dudt_aux = dudt_aux + skappaxp * (c_pcc - c_ccc) * dxi;
-  dvdt_aux = dvdt_aux + skappayp * (c_cpc - c_ccc) * dyi;
-  dwdt_aux = dwdt_aux + skappazp * (c_ccp - c_ccc) * dzci_c;
-  const double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
-  dudt_aux = dudt_aux - (dpdx_e + rhoxp * ph.irho0 * (dpdx - dpdx_e));
-  dvdt_aux = dvdt_aux - (dpdy_e + rhoyp * ph.irho0 * (dpdy - dpdy_e));
-  dwdt_aux = dwdt_aux - (dpdz_e + rhozp * ph.irho0 * (dpdz - dpdz_e));
+  const double surfx = skappaxp * (c_pcc - c_ccc) * dxi;
+  const double surfy = skappayp * (c_cpc - c_ccc) * dyi;
+  const double surfz = skappazp * (c_ccp - c_ccc) * dzci_c;
+  double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
+  double dpx = dpdx, dpy = dpdy, dpz = dpdz;
+  if (sp) {
+    const int t = g.t(i, j, k);
+    const double sxn = sp->n[0][t], syn = sp->n[1][t], szn = sp->n[2][t];
+    const double sxe = (1. + dt_r) * sxn - dt_r * sp->o[0][t];
+    const double sye = (1. + dt_r) * syn - dt_r * sp->o[1][t];
+    const double sze = (1. + dt_r) * szn - dt_r * sp->o[2][t];
+    dpx = dpx - surfx; dpy = dpy - surfy; dpz = dpz - surfz;
+    dpdx_e = dpdx_e - sxe; dpdy_e = dpdy_e - sye; dpdz_e = dpdz_e - sze;
+    if (sp->out_o[0]) { sp->out_o[0][t] = sxn; sp->out_o[1][t] = syn; sp->out_o[2][t] = szn; }
+    sp->out_n[0][t] = surfx; sp->out_n[1][t] = surfy; sp->out_n[2][t] = surfz;
+  } else {
+    dudt_aux = dudt_aux + surfx;
+    dvdt_aux = dvdt_aux + surfy;
+    dwdt_aux = dwdt_aux + surfz;
+  }
+  dudt_aux = dudt_aux - (dpdx_e + rhoxp * ph.irho0 * (dpx - dpdx_e));
+  dvdt_aux = dvdt_aux - (dpdy_e + rhoyp * ph.irho0 * (dpy - dpdy_e));
+  dwdt_aux = dwdt_aux - (dpdz_e + rhozp * ph.irho0 * (dpz - dpdz_e));
   if (s) {
     const double s_ccc = LD(s, ccc), s_pcc = LD(s, pcc), s_cpc = LD(s, cpc), s_ccp = LD(s, ccp);
     const double factorxp = ph.rhobeta + ph.drhobeta * psixp;
@@ -471,20 +488,22 @@ void launch_mom_ad(const Launch& L, const Geo& g, const Phys& ph, const double* 
 
 __global__ void k_mom_oth(Geo g, Phys ph, const DevScalars* __restrict__ sc, const double* __restrict__ p,
                           const double* __restrict__ psi, const double* __restrict__ kappa,
-                          const double* __restrict__ s, const double* __restrict__ pn,
-                          const double* __restrict__ po, double* __restrict__ du, double* __restrict__ dv,
-                          double* __restrict__ dw) {
+                          const double* __restrict__ s, const SurfSplit sp, int with_sp,
+                          const double* __restrict__ pn, const double* __restrict__ po, double* __restrict__ du,
+                          double* __restrict__ dv, double* __restrict__ dw) {
   INTERIOR_IJK(g)
-  const AdOut r = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, s, pn, po);
+  const AdOut r = mom_oth_cell(g, ph, sc->dt_r, sc->rho_av, i, j, k, p, psi, kappa, s, with_sp ? &sp : nullptr, pn,
+                               po);
   const int t = g.t(i, j, k);
   du[t] = r.du; dv[t] = r.dv; dw[t] = r.dw;
 }
 
 void launch_mom_oth(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
-                    const double* psi, const double* kappa, const double* s, const double* pn, const double* po,
-                    double* du, double* dv, double* dw) {
+                    const double* psi, const double* kappa, const double* s, const SurfSplit* sp, const double* pn,
+                    const double* po, double* du, double* dv, double* dw) {
   dim3 b = blk_interior(g), gr = grd_interior(g, b);
-  k_mom_oth<<<gr, b, 0, L.st>>>(g, ph, sc, p, psi, kappa, s, pn, po, du, dv, dw);
+  const SurfSplit none{};
+  k_mom_oth<<<gr, b, 0, L.st>>>(g, ph, sc, p, psi, kappa, s, sp ? *sp : none, sp ? 1 : 0, pn, po, du, dv, dw);
 }
 
 // rk update 1 (src/rk.f90:86-101): u = u*rho_n/rho_p + (f1 R + f2 Ro)/rho_p; on the
@@ -552,9 +571,9 @@ void launch_rk_update2(const Launch& L, const Geo& g, const Phys& ph, const DevS
 void launch_momentum_fused(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* u,
                            const double* v, const double* w, const double* psi, const double* psio,
                            const double* fx, const double* fy, const double* fz, const double* p,
-                           const double* po, const double* kappa, const double* s, double* duo, double* dvo,
-                           double* dwo, double* uo, double* vo, double* wo) {
-  launch_momentum_t<double>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, duo, dvo, dwo, uo, vo,
+                           const double* po, const double* kappa, const double* s, const SurfSplit* sp,
+                           double* duo, double* dvo, double* dwo, double* uo, double* vo, double* wo) {
+  launch_momentum_t<double>(L, g, ph, sc, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo,
                             wo);
 }
 

@@ -76,6 +76,9 @@ typedef struct cansfz_params {
   int32_t interface_capturing;  /* CANSFZ_ACDI (default) or CANSFZ_VOF_THINC   */
   int32_t sdf_normals;          /* _SDF_NORMALS, default 1                     */
   int32_t brackbill;            /* _CAPILLARY_BRACKBILL_NORMALIZATION, default 1 */
+  int32_t balanced;             /* _BALANCED_CAPILLARY_PRESSURE_SPLIT, default 0:
+                                   the surf?_n/surf?_o histories live in the context
+                                   (cansfz_get_aux "surfx_n" ... "surfz_o")      */
   /* scalar transport: _SCALAR and _BOUSSINESQ_BUOYANCY (compile-time macros
    * of the reference, default 0), &scalar, and ka12/cp12 of &two_fluid    */
   int32_t scalar;               /* transport the scalar s (rk_scal every step) */

@@ -559,14 +559,17 @@ static void mom_xyz_ad(const Dims& D, const double dli[3], const double* dzci, c
       }
 }
 
-// mom_xyz_oth, src/mom.f90:853-1039 (CONSTANT_COEFFS_POISSON on, BALANCED off).
-// s != nullptr: the _SCALAR + _BOUSSINESQ_BUOYANCY term (src/mom.f90:1017-1024)
+// mom_xyz_oth, src/mom.f90:853-1039 (CONSTANT_COEFFS_POISSON on).
+// s != nullptr: the _SCALAR + _BOUSSINESQ_BUOYANCY term (src/mom.f90:1017-1024).
+// surf != nullptr: _BALANCED_CAPILLARY_PRESSURE_SPLIT (src/mom.f90:982-1032),
+// surf[0..2] = surfx_n..surfz_n, surf[3..5] = surfx_o..surfz_o (interior),
+// updated in place as there.
 static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, double dt_r,
                         const double rho12[2], const double beta12[2], const double bforce[3],
                         const double gacc[3], double sigma, double rho0, const double rho_av[3],
                         const double* p, const double* psi, const double* kappa, const double* s,
-                        const double* pn, const double* po, double* dudt, double* dvdt, double* dwdt,
-                        bool brackbill) {
+                        double* const* surf, const double* pn, const double* po, double* dudt, double* dvdt,
+                        double* dwdt, bool brackbill) {
   const double rho = rho12[1], drho = rho12[0] - rho12[1];
   const double rhobeta = rho12[1] * beta12[1], drhobeta = rho12[0] * beta12[0] - rho12[1] * beta12[1];
   const double dxi = dli[0], dyi = dli[1];
@@ -587,7 +590,7 @@ static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, 
         const double c_ccc = psi[ccc], c_pcc = psi[pcc], c_cpc = psi[cpc], c_ccp = psi[ccp];
         const double psixp = 0.5 * (c_pcc + c_ccc), psiyp = 0.5 * (c_cpc + c_ccc), psizp = 0.5 * (c_ccp + c_ccc);
         const double rhoxp = rho + drho * psixp, rhoyp = rho + drho * psiyp, rhozp = rho + drho * psizp;
-        const double dpdx = (p_pcc - p_ccc) * dxi, dpdy = (p_cpc - p_ccc) * dyi, dpdz = (p_ccp - p_ccc) * dzci_c;
+        double dpdx = (p_pcc - p_ccc) * dxi, dpdy = (p_cpc - p_ccc) * dyi, dpdz = (p_ccp - p_ccc) * dzci_c;
         double dudt_aux = bforce[0] + (rhoxp - rhox_av) * gacc[0];
         double dvdt_aux = bforce[1] + (rhoyp - rhoy_av) * gacc[1];
         double dwdt_aux = bforce[2] + (rhozp - rhoz_av) * gacc[2];
@@ -598,10 +601,26 @@ static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, 
         const double surfx = skappaxp * (c_pcc - c_ccc) * dxi;
         const double surfy = skappayp * (c_cpc - c_ccc) * dyi;
         const double surfz = skappazp * (c_ccp - c_ccc) * dzci_c;
-        dudt_aux = dudt_aux + surfx;
-        dvdt_aux = dvdt_aux + surfy;
-        dwdt_aux = dwdt_aux + surfz;
-        const double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
+        const size_t t = D.t(i, j, k);
+        double surfx_e = 0., surfy_e = 0., surfz_e = 0.;
+        if (surf) {
+          surfx_e = (1. + dt_r) * surf[0][t] - dt_r * surf[3][t];
+          surfy_e = (1. + dt_r) * surf[1][t] - dt_r * surf[4][t];
+          surfz_e = (1. + dt_r) * surf[2][t] - dt_r * surf[5][t];
+          dpdx = dpdx - surfx;
+          dpdy = dpdy - surfy;
+          dpdz = dpdz - surfz;
+        } else {
+          dudt_aux = dudt_aux + surfx;
+          dvdt_aux = dvdt_aux + surfy;
+          dwdt_aux = dwdt_aux + surfz;
+        }
+        double dpdx_e = (q_pcc - q_ccc) * dxi, dpdy_e = (q_cpc - q_ccc) * dyi, dpdz_e = (q_ccp - q_ccc) * dzci_c;
+        if (surf) {
+          dpdx_e = dpdx_e - surfx_e;
+          dpdy_e = dpdy_e - surfy_e;
+          dpdz_e = dpdz_e - surfz_e;
+        }
         dudt_aux = dudt_aux - (dpdx_e + rhoxp / rho0 * (dpdx - dpdx_e));
         dvdt_aux = dvdt_aux - (dpdy_e + rhoyp / rho0 * (dpdy - dpdy_e));
         dwdt_aux = dwdt_aux - (dpdz_e + rhozp / rho0 * (dpdz - dpdz_e));
@@ -613,6 +632,10 @@ static void mom_xyz_oth(const Dims& D, const double dli[3], const double* dzci, 
           dudt_aux = dudt_aux - gacc[0] * factorxp * 0.5 * (s_pcc + s_ccc);
           dvdt_aux = dvdt_aux - gacc[1] * factoryp * 0.5 * (s_cpc + s_ccc);
           dwdt_aux = dwdt_aux - gacc[2] * factorzp * 0.5 * (s_ccp + s_ccc);
+        }
+        if (surf) {
+          surf[3][t] = surf[0][t]; surf[4][t] = surf[1][t]; surf[5][t] = surf[2][t];
+          surf[0][t] = surfx; surf[1][t] = surfy; surf[2][t] = surfz;
         }
         dudt[D.t(i, j, k)] = dudt_aux;
         dvdt[D.t(i, j, k)] = dvdt_aux;
@@ -967,6 +990,10 @@ struct Case {
   std::vector<double> du, dv, dw, duo, dvo, dwo, dpsi, dpsio;
   // scalar (_SCALAR): s with ghosts, the dsdtrk/dsdtrko histories of rk_scal
   std::vector<double> s, ds, dso;
+  // balanced capillary split: surfx_n..surfz_n, surfx_o..surfz_o (interior)
+  std::vector<double> surf[6];
+  double* surf_ptrs[6] = {};
+  double* const* split() { return P.balanced ? surf_ptrs : nullptr; }
   bool rk_first = true, rk2_first = true, chkdt_first = true, rks_first = true;
   double dlmin = 0.;
   double time = 0., dt = 0., dto = 0., dt_cfl = 0., gam = 0., divtot = 0., divmax = 0.;
@@ -1079,6 +1106,8 @@ static void setup(Case& C) {
                   &C.normx, &C.normy, &C.normz, &C.fx, &C.fy, &C.fz})
     f->assign(H, 0.);
   for (auto* f : {&C.du, &C.dv, &C.dw, &C.duo, &C.dvo, &C.dwo, &C.dpsi, &C.dpsio}) f->assign(I, 0.);
+  if (P.balanced)
+    for (int q = 0; q < 6; ++q) { C.surf[q].assign(I, 0.); C.surf_ptrs[q] = C.surf[q].data(); }
   if (P.scalar) {
     C.s.assign(H, 0.);
     C.ds.assign(I, 0.);
@@ -1427,8 +1456,8 @@ static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3])
       }
   std::swap(C.du, C.duo); std::swap(C.dv, C.dvo); std::swap(C.dw, C.dwo);
   mom_xyz_oth(D, C.dli, C.dzci.data(), dt_r, P.rho12, P.beta12, P.bforce, P.gacc, P.sigma, C.rho0, rho_av,
-              C.p.data(), C.psi.data(), C.kappa.data(), P.scalar && P.boussinesq ? C.s.data() : nullptr, C.pn.data(),
-              C.po.data(), C.du.data(), C.dv.data(), C.dw.data(), P.brackbill != 0);
+              C.p.data(), C.psi.data(), C.kappa.data(), P.scalar && P.boussinesq ? C.s.data() : nullptr, C.split(),
+              C.pn.data(), C.po.data(), C.du.data(), C.dv.data(), C.dw.data(), P.brackbill != 0);
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= D.n3; ++k)
     for (int j = 1; j <= D.n2; ++j)
@@ -1724,6 +1753,9 @@ static std::vector<double>* field_by_name(Case* C, const char* name) {
   if (s == "dpsidtrko") return &C->dpsio;
   if (s == "s" && C->P.scalar) return &C->s;
   if (s == "dsdtrko" && C->P.scalar) return &C->dso;
+  if (C->P.balanced && s.size() == 7 && s.compare(0, 4, "surf") == 0 && s[5] == '_' && s[4] >= 'x' && s[4] <= 'z' &&
+      (s[6] == 'n' || s[6] == 'o'))
+    return &C->surf[(s[6] == 'o' ? 3 : 0) + (s[4] - 'x')];
   return nullptr;
 }
 
@@ -1835,7 +1867,7 @@ void orc_mom_xyz_oth(void* h, double dt_r, const double* rho_av, const double* p
   Case* C = (Case*)h;
   const double* sb = C->P.scalar && C->P.boussinesq ? s : nullptr;
   mom_xyz_oth(C->D, C->dli, C->dzci.data(), dt_r, C->P.rho12, C->P.beta12, C->P.bforce, C->P.gacc, C->P.sigma,
-              C->rho0, rho_av, p, psi, kappa, sb, pn, po, dudt, dvdt, dwdt, C->P.brackbill != 0);
+              C->rho0, rho_av, p, psi, kappa, sb, C->split(), pn, po, dudt, dvdt, dwdt, C->P.brackbill != 0);
 }
 void orc_scal_ad(void* h, const double* fx, const double* fy, const double* fz, const double* psi, const double* u,
                  const double* v, const double* w, const double* s, double* dsdt) {

@@ -132,7 +132,7 @@ class Case:
         return np.zeros(self.hshape, order="F")
 
     def get(self, name: str) -> np.ndarray:
-        interior = name in ("dudtrko", "dvdtrko", "dwdtrko", "dpsidtrko", "dsdtrko")
+        interior = name in ("dudtrko", "dvdtrko", "dwdtrko", "dpsidtrko", "dsdtrko") or name.startswith("surf")
         a = np.zeros(self.n if interior else self.hshape, order="F")
         rc = lib().orc_get_field(self.h, name.encode(), ptr(a))
         if rc:

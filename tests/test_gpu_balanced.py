@@ -1,0 +1,151 @@
+"""The balanced capillary pressure split (_BALANCED_CAPILLARY_PRESSURE_SPLIT,
+src/mom.f90:982-1032) on the GPU against the oracle: the surface-tension
+force leaves the momentum right-hand side and is subtracted from the
+pressure gradient, its extrapolation (1+dt_r)*surf_n - dt_r*surf_o from the
+extrapolated gradient; the six surf arrays are carried from step to step.
+
+* per procedure: mom_xyz_oth called twice (the second call extrapolates
+  from the first call's force), 1e-12 relative, surf arrays included;
+* whole steps: 3-D droplets (periodic x, y) and a 2-D bubble from rest
+  (ny = 2), 10 steps, 1e-11 relative in u, v, w, p, psi and the surf arrays
+  (for the bubble, whose velocity is a small residual of balanced forces,
+  1e-11 or four times the oracle's own change under a 1e-15 input
+  perturbation, whichever is larger: that change is 8e-11 there); the
+  mixed form within its 1e-6 bound; a batched ensemble bit for bit equal to
+  the cases' own runs.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from cansfz import case as C
+from cansfz import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+SURF = ("surfx_n", "surfy_n", "surfz_n", "surfx_o", "surfy_o", "surfz_o")
+
+
+def _rel(a, b):
+    s = np.abs(b).max()
+    return np.abs(a - b).max() / (s if s > 0 else 1.0)
+
+
+def _droplets(n=32, form=0):
+    p, f = W.droplets((n, n, n), (1.0, 1.0, 1.0), False, count=5, rmin=0.1, rmax=0.15, seed=9)
+    p.balanced = 1
+    p.form = form
+    return p, f
+
+
+def _pair(p, f):
+    q = p.copy()
+    q.form = 0
+    g, o = C.Case(p), O.Case(q)
+    g.set_fields(*f)
+    for nm, a in zip(("u", "v", "w", "p", "psi"), f):
+        o.set(nm, a)
+    g.prepare()
+    o.prepare()
+    return g, o
+
+
+def _check(g, o, tol):
+    errs = {nm: _rel(g.get(nm), o.get(nm)) for nm in ("u", "v", "w", "psi") + SURF}
+    pa, pb = g.get("p")[1:-1, 1:-1, 1:-1], o.get("p")[1:-1, 1:-1, 1:-1]
+    errs["p"] = _rel(pa - pa.mean(), pb - pb.mean())
+    for k, e in errs.items():
+        assert e < tol, f"{k}: rel err {e:.3e} ({errs})"
+    assert np.abs(o.get("surfz_n")).max() > 0  # the split carries a force
+
+
+def test_mom_xyz_oth_split_two_calls():
+    p, _ = _droplets(24)
+    g, o = C.Case(p), O.Case(p)
+    rng = np.random.default_rng(4)
+    shp = tuple(x + 2 for x in p.n)
+    for call, dt_r in enumerate((1.0, 0.8)):
+        pp, pn, po, kap = (np.asfortranarray(rng.standard_normal(shp)) for _ in range(4))
+        psi = np.asfortranarray(np.clip(0.5 + 0.45 * np.tanh(rng.standard_normal(shp)), 0, 1))
+        dev = {k: g.field(a) for k, a in dict(p=pp, pn=pn, po=po, k=kap, psi=psi).items()}
+        outg = [g.interior() for _ in range(3)]
+        outo = [np.zeros(p.n, order="F") for _ in range(3)]
+        g.call("mom_xyz_oth", dt_r, [0.0, 0.0, 0.0], dev["p"], dev["psi"], dev["k"], None, dev["pn"], dev["po"],
+               *outg)
+        o.call("mom_xyz_oth", dt_r, np.zeros(3), pp, psi, kap, None, pn, po, *outo)
+        for a, b in zip(outg, outo):
+            assert _rel(a.get(), b) < 1e-12, call
+        for nm in SURF:
+            assert _rel(g.get(nm), o.get(nm)) < 1e-12, (call, nm)
+
+
+def test_step_droplets_3d():
+    p, f = _droplets()
+    g, o = _pair(p, f)
+    assert g.step(10) == 0 and o.step(10) == 0
+    _check(g, o, 1e-11)
+
+
+def _oracle_sensitivity(p, f, nsteps):
+    """The reference algorithm's own round-off sensitivity: the largest
+    relative change of u, v, w when the oracle's input psi is scaled by
+    (1 - 1e-15)."""
+    runs = []
+    for scale in (1.0, 1.0 - 1e-15):
+        o = O.Case(p)
+        for nm, a in zip(("u", "v", "w", "p", "psi"), f):
+            o.set(nm, a * scale if nm == "psi" else a)
+        o.prepare()
+        assert o.step(nsteps) == 0
+        runs.append([o.get(nm) for nm in ("u", "v", "w")])
+    return max(_rel(a, b) for a, b in zip(runs[1], runs[0]))
+
+
+def test_step_bubble_2d():
+    """A 2-D bubble from rest: the velocity is the small residual of the
+    pressure gradient and the (balanced) surface-tension and gravity forces,
+    so, as for the 3-D bubble of the unsplit step, the bar is 1e-11 or four
+    times the reference algorithm's own change under a 1e-15 perturbation of
+    the input, whichever is larger."""
+    p, f = W._bubble_case(64, 2, 128, 1.0, 2.0 / 64, 2.0, 1000.0, 100.0, 20.0, 0.3, True)
+    p.balanced = 1
+    g, o = _pair(p, f)
+    assert g.step(10) == 0 and o.step(10) == 0
+    _check(g, o, max(1e-11, 4.0 * _oracle_sensitivity(p, f, 10)))
+
+
+def test_step_mixed_form():
+    p, f = _droplets(form=1)
+    g, o = _pair(p, f)
+    assert g.step(10) == 0 and o.step(10) == 0
+    _check(g, o, 1e-6)
+
+
+def test_ensemble_batched():
+    specs = []
+    for seed, sigma in ((1, 1.0), (2, 2.0)):
+        p, f = W.droplets((32, 32, 32), (1.0, 1.0, 1.0), False, count=4, rmin=0.1, rmax=0.15, seed=seed)
+        p.balanced = 1
+        p.sigma = sigma
+        specs.append((p, f))
+
+    def build():
+        out = []
+        for p, f in specs:
+            c = C.Case(p, own_stream=True)
+            c.set_fields(*f)
+            c.prepare()
+            out.append(c)
+        return out
+
+    single = build()
+    for c in single:
+        assert c.step(6) == 0
+    batch = build()
+    ens = C.Ensemble(batch, batch=4)
+    rc, st = ens.step(6)
+    assert rc == 0 and ens.groups() == (1, 2)
+    for a, b in zip(single, batch):
+        for nm in ("u", "v", "w", "p", "psi") + SURF:
+            assert np.array_equal(a.get(nm), b.get(nm)), nm
+    ens.close()

@@ -304,3 +304,30 @@ def test_reference_differentially_heated_cavity(reference_dir):
     txt = open(os.path.join(case, "test.py")).read()
     ref = float(re.search(r"nusselt_ref\s*=\s*([0-9.eE+-]+)", txt).group(1))
     np.testing.assert_allclose([_dhc_nusselt(c)], [ref], rtol=1e-2, atol=1e-2)
+
+
+def test_balanced_split_known_answers():
+    """_BALANCED_CAPILLARY_PRESSURE_SPLIT (src/mom.f90:982-1032): without
+    surface tension the split moves nothing (the same step bit for bit);
+    with it, the surf?_n arrays hold the last step's force and surf?_o the
+    one before, and the step differs from the unsplit one."""
+    from cansfz import workloads as W
+
+    for sigma in (0.0, 1.0):
+        runs = []
+        for bal in (0, 1):
+            p, f = W.droplets((16, 16, 16), (1.0, 1.0, 1.0), False, count=2, rmin=0.15, rmax=0.2, seed=3)
+            p.sigma = sigma
+            p.balanced = bal
+            c = O.Case(p)
+            for nm, a in zip(("u", "v", "w", "p", "psi"), f):
+                c.set(nm, a)
+            c.prepare()
+            assert c.step(4) == 0
+            runs.append(c)
+        same = all(np.array_equal(runs[0].get(nm), runs[1].get(nm)) for nm in ("u", "v", "w", "p", "psi"))
+        assert same == (sigma == 0.0)
+        if sigma > 0:
+            b = runs[1]
+            assert np.abs(b.get("surfz_n")).max() > 0 and np.abs(b.get("surfz_o")).max() > 0
+            assert not np.array_equal(b.get("surfz_n"), b.get("surfz_o"))
