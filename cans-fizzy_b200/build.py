@@ -13,7 +13,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["csrc/k_stencil.cu", "csrc/k_tiles.cu", "csrc/k_momentum.cu", "csrc/k_bc.cu", "csrc/k_poisson.cu",
+SOURCES = ["csrc/k_stencil.cu", "csrc/k_tiles.cu", "csrc/k_momentum.cu", "csrc/k_init.cu", "csrc/k_bc.cu", "csrc/k_poisson.cu",
            "csrc/context.cu", "csrc/noalloc.cu"]
 OUT = os.path.join(HERE, "cansfz", "libcansfz.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -98,6 +98,18 @@ class Case:
                  "cansfz_get_fields")
         return [o.reshape(self.hshape, order="F") for o in outs]
 
+    # initial conditions computed on the device (no host field arrays)
+    def init2fl(self, inipsi: str, spheres=None):
+        sph = np.zeros((0, 4)) if spheres is None else np.ascontiguousarray(spheres, dtype=np.float64).reshape(-1, 4)
+        ptr = sph.ctypes.data_as(ct.c_void_p) if sph.size else None
+        _L.check(self.lib.cansfz_init2fl(self.h, inipsi.encode(), ptr, int(sph.shape[0])), "cansfz_init2fl")
+
+    def initflow(self, inivel: str):
+        _L.check(self.lib.cansfz_initflow(self.h, inivel.encode()), "cansfz_initflow")
+
+    def initscal(self, inisca: str):
+        _L.check(self.lib.cansfz_initscal(self.h, inisca.encode()), "cansfz_initscal")
+
     def set_scalar(self, s):
         """The scalar s of a case built with params.scalar = 1 (halo layout)."""
         a = np.ascontiguousarray(np.asarray(s, dtype=np.float64).reshape(-1, order="F"))

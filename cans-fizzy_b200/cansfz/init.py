@@ -41,6 +41,23 @@ def seps(p: Params) -> float:
     return dlmax * p.psi_thickness_factor
 
 
+def read_spheres(path: str) -> np.ndarray:
+    """read_sphere_file (src/two_fluid.f90:439-471): one sphere per line,
+    x y z r (list-directed); no file: no spheres (init2fl then uses its
+    default sphere).  Returns an (nspheres, 4) array."""
+    import os
+
+    if not os.path.exists(path):
+        return np.zeros((0, 4))
+    rows = []
+    with open(path) as f:
+        for line in f:
+            toks = line.replace(",", " ").split()
+            if toks:
+                rows.append([float(t.replace("d", "e").replace("D", "e")) for t in toks[:4]])
+    return np.array(rows, dtype=np.float64).reshape(-1, 4)
+
+
 def smooth_step_tanh(r, eps):
     return 0.5 * (1.0 + np.tanh(r / (2.0 * eps)))
 

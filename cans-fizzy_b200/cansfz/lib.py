@@ -41,6 +41,9 @@ SIGNATURES = {
     "cansfz_get_fields": (I, [V, V, V, V, V, V, I]),
     "cansfz_get_aux": (I, [V, ct.c_char_p, V, I]),
     "cansfz_set_scalar": (I, [V, V, I]),
+    "cansfz_init2fl": (I, [V, ct.c_char_p, V, I]),
+    "cansfz_initflow": (I, [V, ct.c_char_p]),
+    "cansfz_initscal": (I, [V, ct.c_char_p]),
     "cansfz_prepare": (I, [V]),
     "cansfz_step": (I, [V, I]),
     "cansfz_get_diag": (I, [V, ct.POINTER(Diag)]),

@@ -178,6 +178,14 @@ struct SurfSplit {
   double* out_o[3];
 };
 
+// init2fl's choices (src/two_fluid.f90:275-305) for the device kernel
+struct Init2fl {
+  int zer, flm, sphere, swap;
+  int idir[3], iperiod[3];
+  double l[3], lmax, seps, reach;
+  int nsph;
+};
+
 // optional stage marker of the step profiler (CUDA events between stages)
 struct StageMark {
   void (*fn)(void* arg, const char* name);
@@ -276,6 +284,12 @@ void launch_bulk_mean(const Launch& L, const Geo& g, const Phys& ph, DevScalars*
                       double* partial, int idir, const double* gvr, const double* psi);
 void launch_mass(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                  const double* psi, double vol);
+
+// k_init.cu: initial conditions on the device
+void launch_init2fl(const Launch& L, const Geo& g, const Init2fl& a, const double* sph, const double* zc,
+                    double* psi);
+void launch_fill_zprofile(const Launch& L, const Geo& g, const double* prof, double* f);
+void launch_fill_xprofile(const Launch& L, const Geo& g, double b0, double b1, double lx, double* f);
 
 // step bookkeeping kernels
 void launch_step_begin(const Launch& L, DevScalars* sc, int icheck);

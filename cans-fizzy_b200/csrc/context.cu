@@ -1624,6 +1624,147 @@ int cansfz_set_inivel(cansfz_ctx* c, const char* inivel) {
   return CANSFZ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// initial conditions on the device, into the current slot (cansfz_prepare
+// follows, as the reference's start-up follows its init calls)
+// ---------------------------------------------------------------------------
+// init2fl, src/two_fluid.f90:247-437 (spheres: nspheres rows x, y, z, r as
+// read_sphere_file reads spheres.in; none: the reference's default sphere)
+int cansfz_init2fl(cansfz_ctx* c, const char* inipsi, const double* spheres, int nspheres) {
+  if (!c || !inipsi || nspheres < 0 || (nspheres > 0 && !spheres)) return CANSFZ_ERR_ARG;
+  const cansfz_params& P = c->P;
+  const std::string s(inipsi);
+  Init2fl a{};
+  for (int d = 0; d < 3; ++d) a.idir[d] = 1;
+  if (s == "uni") {
+  } else if (s == "zer") {
+    a.zer = 1;
+  } else if (s == "bub3" || s == "drp3" || s == "dis3") {
+    a.sphere = 1; a.swap = s != "bub3";
+  } else if (s == "bub2" || s == "drp2" || s == "dis2") {
+    a.sphere = 1; a.swap = s != "bub2"; a.idir[1] = 0;
+  } else if (s == "bub1" || s == "drp1" || s == "dis1") {
+    a.sphere = 1; a.swap = s != "bub1"; a.idir[0] = a.idir[1] = 0;
+  } else if (s == "flm") {
+    a.flm = 1;
+  } else {
+    return CANSFZ_ERR_ARG;
+  }
+  std::vector<double> sph;
+  if (a.sphere) {
+    sph.assign(spheres, spheres + 4 * (size_t)nspheres);
+    if (nspheres == 0) {
+      double lmin = 1e300;
+      for (int d = 0; d < 3; ++d)
+        if (a.idir[d]) lmin = std::min(lmin, P.l[d]);
+      sph = {P.l[0] / 2, P.l[1] / 2, P.l[2] / 2, 0.25 * lmin};
+    }
+  }
+  a.nsph = (int)(sph.size() / 4);
+  for (int d = 0; d < 3; ++d) {
+    a.l[d] = P.l[d];
+    a.iperiod[d] = is_pp(P.cbcpsi[d]) ? 1 : 0;
+    a.lmax = std::max(a.lmax, P.l[d] * a.idir[d]);
+  }
+  a.seps = c->seps;
+  a.reach = 40. * c->seps;
+  double* d_sph = nullptr;
+  if (a.nsph > 0) {
+    CK(cudaMalloc(&d_sph, sph.size() * sizeof(double)));
+    CK(cudaMemcpyAsync(d_sph, sph.data(), sph.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  }
+  launch_init2fl(c->L, c->g, a, d_sph, c->d_grid + 6 * (c->g.nz + 2), c->psi[c->cur]);
+  const cudaError_t e1 = cudaGetLastError(), e2 = cudaStreamSynchronize(c->st);
+  if (d_sph) cudaFree(d_sph);
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return CANSFZ_ERR_CUDA;
+  c->prepared = false;
+  return CANSFZ_OK;
+}
+
+// a z profile (nz+2 values, k = 0..nz+1) into a halo field's interior
+static int fill_profile(cansfz_ctx* c, const std::vector<double>& prof, double* f) {
+  CK(cudaMemcpyAsync(c->tpsi, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  launch_fill_zprofile(c->L, c->g, c->tpsi, f);
+  CK(cudaGetLastError());
+  return CANSFZ_OK;
+}
+
+// initflow, src/initflow.f90:16-361: 'zer', 'uni', 'cou', 'poi' (with
+// set_mean, :464-485) from their z profiles, 'voy' and 'vox' at the
+// context's time; v, w, p zero elsewhere
+int cansfz_initflow(cansfz_ctx* c, const char* inivel) {
+  if (!c || !inivel) return CANSFZ_ERR_ARG;
+  const cansfz_params& P = c->P;
+  const Geo& g = c->g;
+  const std::string s(inivel);
+  const int a = c->cur, nz = g.nz;
+  const size_t H = (size_t)g.hsize();
+  for (double* f : {c->v[a], c->w[a], c->p[a]}) launch_fill(c->L, H, 0., f);
+  if (s == "voy" || s == "vox") {
+    launch_fill(c->L, H, 0., c->u[a]);
+    dim3 bb(g.nx >= 128 ? 128 : 64), gg((g.nx + bb.x - 1) / bb.x, g.ny, g.nz);
+    k_prescribed_vel<<<gg, bb, 0, c->st>>>(g, c->sc, s == "voy" ? 1 : 2, P.l[0], P.l[1], P.l[2],
+                                          c->d_grid + 6 * (nz + 2), c->d_grid + 7 * (nz + 2), c->u[a], c->v[a],
+                                          c->w[a], c->p[a]);
+    CK(cudaGetLastError());
+  } else if (s == "zer" || s == "uni" || s == "cou" || s == "poi") {
+    std::vector<double> u1d(nz + 2, 0.);
+    for (int k = 1; k <= nz; ++k) {
+      const double z = c->zc[k] / P.l[2];
+      if (s == "uni") u1d[k] = 1.;
+      else if (s == "cou") u1d[k] = .5 * (1. - 2. * z) * (P.bcvel[0][2][0] - P.bcvel[0][2][1]);
+      else if (s == "poi") u1d[k] = 6. * z * (1. - z) * 1.;
+    }
+    if (s == "poi") {  // set_mean over the interior, in the reference's loop order
+      double meanold = 0.;
+      for (int k = 1; k <= nz; ++k) {
+        const double gk = c->dzf[k] / P.l[2] * (c->dl[0] / P.l[0]) * (c->dl[1] / P.l[1]);
+        for (int j = 1; j <= g.ny; ++j)
+          for (int i = 1; i <= g.nx; ++i) meanold = meanold + u1d[k] * gk;
+      }
+      if (meanold != 0.)
+        for (int k = 1; k <= nz; ++k) u1d[k] = u1d[k] / meanold * 1.;
+    }
+    if (int rc = fill_profile(c, u1d, c->u[a])) return rc;
+  } else {
+    return CANSFZ_ERR_ARG;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->prepared = false;
+  return CANSFZ_OK;
+}
+
+// initscal, src/initflow.f90:363-429 ('cou', 'dhc', 'uni', 'zer')
+int cansfz_initscal(cansfz_ctx* c, const char* inisca) {
+  if (!c || !inisca) return CANSFZ_ERR_ARG;
+  const cansfz_params& P = c->P;
+  if (!P.scalar) return CANSFZ_ERR_UNSUPPORTED;
+  const std::string s(inisca);
+  const int a = c->cur, nz = c->g.nz;
+  if (s == "dhc") {
+    launch_fill_xprofile(c->L, c->g, P.bcsca[0][0], P.bcsca[0][1], P.l[0], c->s[a]);
+    CK(cudaGetLastError());
+  } else if (s == "cou" || s == "uni" || s == "zer") {
+    std::vector<double> s1d(nz + 2, 0.);
+    const double sref = 0.5 * (P.bcsca[2][0] + P.bcsca[2][1]);
+    for (int k = 1; k <= nz; ++k) {
+      if (s == "uni") {
+        s1d[k] = sref;
+      } else if (s == "cou") {
+        double v = .5 * (1. - 2. * (c->zc[k] / P.l[2])) * 1.;
+        v = v + 0.5;
+        s1d[k] = P.bcsca[2][0] * v + P.bcsca[2][1] * (1. - v);
+      }
+    }
+    if (int rc = fill_profile(c, s1d, c->s[a])) return rc;
+  } else {
+    return CANSFZ_ERR_ARG;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->prepared = false;
+  return CANSFZ_OK;
+}
+
 
 // ---------------------------------------------------------------------------
 // library-only measurement helpers (no reference counterpart)

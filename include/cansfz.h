@@ -136,6 +136,21 @@ int cansfz_get_aux(cansfz_ctx* ctx, const char* name, double* out, int on_device
  * without the scalar.                                                     */
 int cansfz_set_scalar(cansfz_ctx* ctx, const double* s, int on_device);
 
+/* Initial conditions computed on the device into the context's fields (no
+ * host field arrays; cansfz_prepare follows):
+ * init2fl (src/two_fluid.f90:247-437): inipsi 'uni', 'zer', 'flm',
+ *   'bub1/2/3', 'drp1/2/3', 'dis1/2/3'; spheres = nspheres rows (x, y, z, r)
+ *   as read_sphere_file reads spheres.in (:439-471), NULL/0 for the
+ *   reference's default sphere;
+ * initflow (src/initflow.f90:16-361): inivel 'zer', 'uni', 'cou', 'poi'
+ *   (with set_mean), 'voy', 'vox' (at the context's time);
+ * initscal (src/initflow.f90:363-429): inisca 'zer', 'uni', 'cou', 'dhc'
+ *   (CANSFZ_ERR_UNSUPPORTED without the scalar).
+ * An unknown name returns CANSFZ_ERR_ARG, where the reference aborts.     */
+int cansfz_init2fl(cansfz_ctx* ctx, const char* inipsi, const double* spheres, int nspheres);
+int cansfz_initflow(cansfz_ctx* ctx, const char* inivel);
+int cansfz_initscal(cansfz_ctx* ctx, const char* inisca);
+
 /* Finish the start-up sequence after set_fields: BCs (the scalar's too),
  * phi, normals, curvature, Gamma and the first chkdt
  * (src/main.f90:337-412).                                                  */

@@ -193,3 +193,16 @@ def test_build_conf_switches(reference_dir, tmp_path):
             raise AssertionError(bad)
         except ValueError:
             pass
+
+
+def test_read_spheres(reference_dir, tmp_path):
+    found = 0
+    for root in ("tests", "examples"):
+        for dirpath, _, files in os.walk(os.path.join(reference_dir, root)):
+            if "spheres.in" in files:
+                path = os.path.join(dirpath, "spheres.in")
+                a = init.read_spheres(path)
+                assert a.shape[1] == 4 and np.allclose(a, np.loadtxt(path, ndmin=2)[:, :4], rtol=0, atol=0)
+                found += 1
+    assert found > 0
+    assert init.read_spheres(str(tmp_path / "none.in")).shape == (0, 4)
