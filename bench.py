@@ -63,6 +63,8 @@ STAGE_BYTES = {
     # correc: phi, u, v, w (r) + u, v, w (w); updatep: p (r) + p_new (w)
     "correc_updatep": 8 * (1 + 6 + 2),
     "gamma_chkdt_chkdiv": 8 * 3,
+    # scalar (_SCALAR): s, psi, psio, u, v, w, fx, fy, fz, history (r) + s_new, history (w)
+    "scalar": 8 * (10 + 2),
 }
 # mixed form: state u, v, w, p, psi FP64; phi, normals, kappa, fluxes, histories
 # and the spectral work buffer FP32
@@ -95,6 +97,8 @@ def parse_args():
                     help="refinement sweeps of the mixed form's FP32 Poisson solve (-1: the solve in FP64)")
     ap.add_argument("--config", default="c3a", choices=["c3a", "c1", "c3b", "c5", "c2"],
                     help="benchmark-matrix configuration (c3a: the metric's 256^3 ACDI case; c2: Poisson only)")
+    ap.add_argument("--scalar-steps", type=int, default=50,
+                    help="steps of the scalar-transport leg (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps per case of the batched-ensemble measurement (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=50,
@@ -234,6 +238,62 @@ def mixed_accuracy(p, fields, nsteps):
     res["steps"] = nsteps
     res["rel_err_max"] = err
     return res
+
+
+def scalar_bench(p0, fields, nsteps, peak):
+    """The same workload with the scalar transport and Boussinesq buoyancy on
+    (_SCALAR, _BOUSSINESQ_BUOYANCY: s Dirichlet 1/0 at the z walls, Couette
+    start, rho*cp and k of both phases unequal): device time per step of
+    the graph-launched step, and the scalar stage (k_scal_step) against its
+    algorithmic bytes (96 B per cell) from the stage profile."""
+    import torch
+
+    from cansfz import case as C
+    from cansfz import lib as _L
+
+    p = p0.copy()
+    p.scalar, p.boussinesq = 1, 1
+    p.cbcsca = b"PPPPDD"
+    p.bcsca[:] = [0.0, 0.0, 0.0, 0.0, 1.0, 0.0]
+    p.ka12[:] = [1e-3, 2e-3]
+    p.cp12[:] = [1.5, 1.0]
+    case = C.Case(p)
+    case.set_fields(*fields)
+    case.initscal("cou")
+    case.prepare()
+    stream = torch.cuda.current_stream()
+    if case.step(3) != 0:
+        raise RuntimeError("scalar warm-up failed")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    rc = case.step(nsteps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"scalar steps failed with status {rc}")
+    ms_step = ev0.elapsed_time(ev1) / nsteps
+    nprof = 3
+    buf = (_L.ct.c_double * 64)()
+    nst = _L.ct.c_int(0)
+    names = _L.ct.create_string_buffer(4096)
+    _L.check(case.lib.cansfz_profile_stages(case.h, nprof, buf, 64, _L.ct.byref(nst), names, 4096), "profile")
+    stage = {nm: buf[q] / nprof for q, nm in enumerate(names.value.decode().split(","))}
+    cells = p.ng[0] * p.ng[1] * p.ng[2]
+    ach = STAGE_BYTES["scalar"] * cells / (stage["scalar"] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        if "scalar" in tj:
+            traffic = tj["scalar"]["bytes_per_cell"] * cells
+    case.close()
+    return {"ms_per_step": ms_step, "steps": nsteps, "scalar_stage_ms": stage["scalar"],
+            "bc_scalar_ms": stage.get("bc_scalar"), "momentum_ms": stage.get("momentum"),
+            "roofline": {"kernel": "k_scal_step", "bound": "hbm", "bytes_per_cell": STAGE_BYTES["scalar"],
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": traffic},
+            "what": "the headline workload with _SCALAR and _BOUSSINESQ_BUOYANCY on; device time, graph-launched"}
 
 
 def ensemble_bench(nsteps, warmup, form):
@@ -408,6 +468,10 @@ def gpu_arm(args):
         "gpu_launches": int(kps.value) * args.steps,
         "clocks": clocks,
     }
+    # ---- the same workload with the scalar transport
+    if world == 1 and args.config == "c3a" and args.form == "fp64" and args.scalar_steps > 0:
+        out["scalar"] = scalar_bench(p, fields, args.scalar_steps, peak)
+        out["scalar"]["overhead"] = out["scalar"]["ms_per_step"] / ms_step - 1.0
     # ---- batched ensemble of independent small cases
     if world == 1 and args.ensemble_steps > 0 and args.config == "c3a":
         out["ensemble"] = ensemble_bench(args.ensemble_steps, 3, 0 if args.form == "fp64" else 1)
