@@ -355,7 +355,7 @@ struct FftXFwd {
     const int l0 = bk.x * L;
     const double dti = FUSED ? sc->dti : 0.;
     const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
-    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+    auto get = [&](int it) -> double {
       const int line = it / n, i = it - line * n;
       const int gl = l0 + line;
       double x = 0.;
@@ -369,9 +369,29 @@ struct FftXFwd {
           x = __ldg(src + c);
         }
       }
+      return x;
+    };
+    auto put = [&](int it, double x) {
+      const int line = it / n, i = it - line * n;
       T xv = (T)x;
       if (pl.kind == 2 && (i & 1)) xv = -xv;  // sine kind: negate odd samples
       str<T>(B, 0, fwd_pos(pl.kind, n, i), line, xv);
+    };
+    constexpr int NB = (LC > 0 && MC > 0) ? (LC * 2 * MC + 255) / 256 : 0;
+    if (NB > 0 && NB <= 16) {
+      double r[NB > 0 ? NB : 1];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        r[q] = it < L * n ? get(it) : 0.;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        if (it < L * n) put(it, r[q]);
+      }
+    } else {
+      for (int it = threadIdx.x; it < L * n; it += blockDim.x) put(it, get(it));
     }
     __syncthreads();
     line_forward<T, false, MC, LC>(pl, B, L, [&](int line, int s, T val) {
@@ -401,10 +421,27 @@ struct FftXBwd {
     const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
     const int nlines = g.ny * g.nz;
     const int l0 = bk.x * L;
-    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
-      const int line = it / n, s = it - line * n;
-      const int gl = l0 + line;
-      str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
+    constexpr int NB = (LC > 0 && MC > 0) ? (LC * 2 * MC + 255) / 256 : 0;
+    if (NB > 0 && NB <= 32) {
+      T r[NB > 0 ? NB : 1];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        const int line = it / n, gl = l0 + line;
+        r[q] = (it < L * n && gl < nlines) ? work[(size_t)gl * n + (it - line * n)] : (T)0;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        const int line = it / n;
+        if (it < L * n) str<T>(B, 1, it - line * n, line, r[q]);
+      }
+    } else {
+      for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+        const int line = it / n, s = it - line * n;
+        const int gl = l0 + line;
+        str<T>(B, 1, s, line, gl < nlines ? work[(size_t)gl * n + s] : (T)0);
+      }
     }
     __syncthreads();
     line_backward<T, false, MC, LC>(pl, B, L, [&](int line, int i, T val) {
@@ -440,16 +477,36 @@ struct FftY {
     const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
     const int i0 = bk.x * L, k = bk.y;
     T* plane = work + (size_t)k * nx * n;
-    for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+    auto put = [&](int it, T x) {
       const int line = it % L, j = it / L;
-      const int i = i0 + line;
-      T x = i < nx ? plane[(size_t)j * nx + i] : (T)0;
       if (DIR > 0) {
         if (pl.kind == 2 && (j & 1)) x = -x;
         str<T>(B, 0, fwd_pos(pl.kind, n, j), line, x);
       } else {
         str<T>(B, 1, j, line, x);
       }
+    };
+    auto get = [&](int it) -> T {
+      const int line = it % L, j = it / L;
+      const int i = i0 + line;
+      return i < nx ? plane[(size_t)j * nx + i] : (T)0;
+    };
+    constexpr int NB = (LC > 0 && MC > 0) ? (LC * 2 * MC + 255) / 256 : 0;
+    if (NB > 0 && NB <= 32) {
+      // the tile's loads issued together, then the shared-memory stores
+      T r[NB > 0 ? NB : 1];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        r[q] = it < L * n ? get(it) : (T)0;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int it = threadIdx.x + 256 * q;
+        if (it < L * n) put(it, r[q]);
+      }
+    } else {
+      for (int it = threadIdx.x; it < L * n; it += blockDim.x) put(it, get(it));
     }
     __syncthreads();
     auto out = [&](int line, int j, T val) {
