@@ -995,7 +995,7 @@ void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool
 template <typename T>
 static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
-  const int tb = 128;
+  const int tb = 64;
   if (zpiv<T>(pl) && zdf<T>(pl)) {
     if (pl.zper)
       kgo<ZSolvePeriodicF<T>, 128, 1>(Lc, k_zsolve_periodic_f<T>, (ncol + tb - 1) / tb, tb, 0, ncol, g.nz, pl.lam,
