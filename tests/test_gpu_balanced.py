@@ -149,3 +149,22 @@ def test_ensemble_batched():
         for nm in ("u", "v", "w", "p", "psi") + SURF:
             assert np.array_equal(a.get(nm), b.get(nm)), nm
     ens.close()
+
+
+def test_step_split_with_scalar_buoyancy():
+    """Both compile-time options of the momentum tile together (balanced split
+    and Boussinesq buoyancy): the two-fluid Rayleigh-Benard-like case of the
+    scalar tests, 10 steps, 1e-11 relative in u, v, w, p, psi, s and the
+    surf arrays."""
+    from test_gpu_scalar import _check as check_scalar
+    from test_gpu_scalar import _pair as pair_scalar
+    from test_gpu_scalar import _rb_fields, _rb_params
+
+    p = _rb_params()
+    p.balanced = 1
+    f, s = _rb_fields(p)
+    g, o = pair_scalar(p, f, s)
+    assert g.step(10) == 0 and o.step(10) == 0
+    check_scalar(g, o, 1e-11)
+    for nm in SURF:
+        assert _rel(g.get(nm), o.get(nm)) < 1e-11, nm
