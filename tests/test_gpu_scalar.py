@@ -313,3 +313,14 @@ def test_ensemble_batched_scalar_cases():
         for nm in ("u", "v", "w", "p", "psi", "s"):
             assert np.array_equal(a.get(nm), b.get(nm)), nm
     ens.close()
+
+
+def test_step_scalar_without_interface_tracking():
+    # is_track_interface = F: the phase fluxes are zero and psi stays as set
+    # (src/main.f90:453-458), so the scalar is advected by rho2*cp2*u only
+    p = _rb_params(24, 16, 20)
+    p.is_track_interface = 0
+    f, s = _rb_fields(p, seed=13)
+    g, o = _pair(p, f, s)
+    assert g.step(10) == 0 and o.step(10) == 0
+    _check(g, o, 1e-11)
