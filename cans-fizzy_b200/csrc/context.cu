@@ -1669,14 +1669,16 @@ int cansfz_init2fl(cansfz_ctx* c, const char* inipsi, const double* spheres, int
   a.seps = c->seps;
   a.reach = 40. * c->seps;
   double* d_sph = nullptr;
-  if (a.nsph > 0) {
-    CK(cudaMalloc(&d_sph, sph.size() * sizeof(double)));
-    CK(cudaMemcpyAsync(d_sph, sph.data(), sph.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  if (a.nsph > 0 && cudaMalloc(&d_sph, sph.size() * sizeof(double)) != cudaSuccess) return CANSFZ_ERR_NOMEM;
+  cudaError_t e = cudaSuccess;
+  if (d_sph) e = cudaMemcpyAsync(d_sph, sph.data(), sph.size() * sizeof(double), cudaMemcpyHostToDevice, c->st);
+  if (e == cudaSuccess) {
+    launch_init2fl(c->L, c->g, a, d_sph, c->d_grid + 6 * (c->g.nz + 2), c->psi[c->cur]);
+    e = cudaGetLastError();
   }
-  launch_init2fl(c->L, c->g, a, d_sph, c->d_grid + 6 * (c->g.nz + 2), c->psi[c->cur]);
-  const cudaError_t e1 = cudaGetLastError(), e2 = cudaStreamSynchronize(c->st);
+  const cudaError_t es = cudaStreamSynchronize(c->st);  // the copy and kernel are done before the free
   if (d_sph) cudaFree(d_sph);
-  if (e1 != cudaSuccess || e2 != cudaSuccess) return CANSFZ_ERR_CUDA;
+  if (e != cudaSuccess || es != cudaSuccess) return CANSFZ_ERR_CUDA;
   c->prepared = false;
   return CANSFZ_OK;
 }
