@@ -763,7 +763,7 @@ void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScala
 // step in one pass: both read the correction phi, and updatep needs none of
 // the velocity ghost fills that follow correc.  32x8 point tiles of the halo
 // array; pout = phi + pp on the interior (the new pressure into the po slot).
-constexpr int kCorrecLevels = 4;  // z levels per thread of k_correc_updatep
+constexpr int kCorrecLevels = 2;  // z levels per thread of k_correc_updatep
 struct CorrecUpdatep {
   // each thread owns one (i, j) column and kCorrecLevels consecutive levels:
   // all loads first (p at level k+1 is the next level's own p), then the
