@@ -1136,7 +1136,7 @@ struct StepReduce {
     const int nrows = g.ny * g.nz;
     if (!chk) {
       // Gamma only (every step): R rows per pass, their loads issued together
-      constexpr int R = 4;
+      constexpr int R = 2;
       for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
         for (int r0 = bk.x; r0 < nrows; r0 += R * bk.nx) {
           double u0[R], u1[R], v0[R], v1[R], w0[R], w1[R];
