@@ -88,7 +88,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cansfz", choices=["cansfz", "reference"])
-    ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of timed CPU work (reference arm)")
+    ap.add_argument("--cpu-budget", type=float, default=240.0,
+                    help="upper bound on the seconds of timed CPU work (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=256, help="cube size of the droplet workload (profiling runs)")
@@ -101,9 +102,45 @@ def parse_args():
                     help="steps of the scalar-transport leg (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps per case of the batched-ensemble measurement (0: skip)")
+    ap.add_argument("--no-mixed-leg", dest="mixed_leg", action="store_false",
+                    help="skip the mixed-form leg of an FP64 run")
     ap.add_argument("--accuracy-steps", type=int, default=50,
                     help="mixed form: steps of the error check against the FP64 form (0: skip)")
     return ap.parse_args()
+
+
+def select_workload(args):
+    """(params, fields, workload description) of the configuration the run
+    measures; the GPU arm and the reference arm build it identically."""
+    from cansfz import workloads as W
+
+    if args.config in CONFIGS:
+        builder, workload = CONFIGS[args.config]
+        p, fields = W.BUILDERS[builder]()
+    elif args.grid == 256:
+        workload = WORKLOAD
+        p, fields = W.droplets_acdi(seed=2026)
+    else:
+        p, fields = W.droplets((args.grid,) * 3, (1.0, 1.0, 1.0), False, seed=2026)
+        workload = f"droplets_acdi at {args.grid}^3 (profiling size)"
+    return p, fields, workload
+
+
+def run_config(args, p, workload, world):
+    """The `config` object of the JSON line: what the workload is, not what a
+    run measured, so that both arms print the same object."""
+    nx, ny, nz = p.n
+    hbytes = 8 * (nx + 2) * (ny + 2) * (nz + 2)
+    return {"workload": workload, "config": args.config, "grid": [nx, ny, nz],
+            "form": "fp64 (drop-in)" if args.form == "fp64" else
+                    ("mixed (FP32 stencils, fluxes, curvature and histories; FP64 state, AB2 accumulation, "
+                     "reductions and Poisson solve)" if args.sweeps < 0 else
+                     f"mixed (FP32 stencils and transforms, FP64 state, AB2 accumulation and reductions, "
+                     f"{args.sweeps} FP64-residual refinement sweeps)"),
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": (f"inputs larger than L2 (each FP64 field {hbytes / 1e6:.0f} MB > 126 MB; ~28 fields resident), "
+                   "no flush needed" if hbytes > 126e6 else
+                   f"profiling size: each FP64 field {hbytes / 1e6:.1f} MB < 126 MB L2, no flush")}
 
 
 def measured_peaks():
@@ -240,6 +277,46 @@ def mixed_accuracy(p, fields, nsteps):
     return res
 
 
+def mixed_leg(args, p0, fields, fp64_ms_step):
+    """The mixed-precision form on the same workload: W warm-up and K timed
+    graph-launched steps (device time, CUDA events on the case's stream),
+    its speed-up over the FP64 step, and its error against the FP64 form
+    after `--accuracy-steps` steps from the same state."""
+    import torch
+
+    from cansfz import case as C
+
+    q = p0.copy()
+    q.form = 1
+    q.refine_sweeps = args.sweeps
+    c = C.Case(q)
+    c.set_fields(*fields)
+    c.prepare()
+    if c.step(args.warmup) != 0:
+        raise RuntimeError("mixed warm-up failed")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(c.stream)
+    rc = c.step(args.steps)
+    ev1.record(c.stream)
+    torch.cuda.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"mixed steps failed with status {rc}")
+    ms = ev0.elapsed_time(ev1) / args.steps
+    c.close()
+    nx, ny, nz = p0.n
+    out = {"value": nx * ny * nz / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms,
+           "steps": args.steps, "warmup": args.warmup, "speedup_vs_fp64": fp64_ms_step / ms,
+           "refine_sweeps": args.sweeps,
+           "form": ("FP32 stencils, fluxes, curvature and AB2 histories; FP64 state, AB2 accumulation, reductions "
+                    "and Poisson solve") if args.sweeps < 0 else
+                   (f"FP32 stencils and transforms, FP64 state, AB2 accumulation and reductions, {args.sweeps} "
+                    "FP64-residual refinement sweeps")}
+    if args.accuracy_steps > 0:
+        out["accuracy_vs_fp64"] = mixed_accuracy(q, fields, args.accuracy_steps)
+    return out
+
+
 def scalar_bench(p0, fields, nsteps, peak):
     """The same workload with the scalar transport and Boussinesq buoyancy on
     (_SCALAR, _BOUSSINESQ_BUOYANCY: s Dirichlet 1/0 at the z walls, Couette
@@ -372,15 +449,7 @@ def gpu_arm(args):
     from cansfz import workloads as W
 
     rank, world, local = dist_setup(args.gpus)
-    workload = WORKLOAD
-    if args.config in CONFIGS:
-        builder, workload = CONFIGS[args.config]
-        p, fields = W.BUILDERS[builder]()
-    elif args.grid == 256:
-        p, fields = W.droplets_acdi(seed=2026)
-    else:
-        p, fields = W.droplets((args.grid,) * 3, (1.0, 1.0, 1.0), False, seed=2026)
-        workload = f"droplets_acdi at {args.grid}^3 (profiling size)"
+    p, fields, workload = select_workload(args)
     if args.form == "mixed":
         p.form = 1
         p.refine_sweeps = args.sweeps
@@ -447,18 +516,8 @@ def gpu_arm(args):
         ("f64 state, momentum and Poisson / f32 phase field" if args.sweeps < 0 else
          "f64 state and momentum / f32 phase field and transforms"),
         "data": DATA,
-        "config": {"workload": workload, "config": args.config,
-                   "grid": [nx, ny, nz],
-                   "form": "fp64 (drop-in)" if args.form == "fp64" else
-                           ("mixed (FP32 phase-field stencils, fluxes, curvature and histories; FP64 state, "
-                            "momentum and Poisson solve)" if args.sweeps < 0 else
-                            f"mixed (FP32 phase field and transforms, FP64 state and momentum, {args.sweeps} "
-                            "refinement sweeps)"),
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": (f"inputs larger than L2 (each FP64 field {8 * (nx + 2) * (ny + 2) * (nz + 2) / 1e6:.0f} MB"
-                          f"{' > ' if 8 * (nx + 2) * (ny + 2) * (nz + 2) > 126e6 else ' < '}126 MB; "
-                          f"{28 if args.form == 'fp64' else 20} fields resident, far above L2)"),
-                   "final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
+        "config": run_config(args, p, workload, world),
+        "run": {"final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "bytes_per_launch": bytes_launch, "traffic": traffic,
@@ -478,6 +537,9 @@ def gpu_arm(args):
     # ---- mixed form: error against the FP64 form after the same steps from the same state
     if args.form == "mixed" and args.accuracy_steps > 0:
         out["accuracy_vs_fp64"] = mixed_accuracy(p, fields, args.accuracy_steps)
+    # ---- the metric's second leg: the mixed form beside the FP64 headline
+    if world == 1 and args.form == "fp64" and args.mixed_leg:
+        out["mixed"] = mixed_leg(args, p, fields, ms_step)
     # ---- end to end through the C ABI with pinned host buffers
     if not args.no_e2e:
         hshape = tuple(x + 2 for x in p.n)
@@ -526,22 +588,35 @@ def gpu_arm(args):
 
 
 def reference_arm(args):
+    """The reference's algorithm on the host cores: the C++ OpenMP restatement
+    in oracle/ (the reference itself is Fortran + MPI + FFTW, which this
+    machine cannot build), W warm-up steps then K timed steps of the same
+    workload and `config` as the GPU arm.  libcansfz is never loaded here:
+    the workload's z grid comes from the oracle's initgrid."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    from cansfz import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from cansfz import init
 
-    p, fields = W.droplets_acdi(seed=2026)
-    v, n, thr, dt = cpu_run(p, fields, budget_s=args.cpu_budget, warmup=min(args.warmup, 1),
-                            max_steps=max(args.steps, 1))
-    out = {"metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": 0, "steps": n, "warmup": min(args.warmup, 1),
+    init.use_initgrid(O.lib().orc_initgrid)
+    if args.config == "c2":
+        print(json.dumps({"impl": "reference", "unavailable": "the Poisson-only configuration has no CPU arm"}))
+        return
+    p, fields, workload = select_workload(args)
+    v, n, thr, dt = cpu_run(p, fields, budget_s=args.cpu_budget, warmup=args.warmup, max_steps=max(args.steps, 1))
+    nx, ny, nz = p.n
+    out = {"metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world, "steps": n, "warmup": args.warmup,
            "ms_per_step": 1e3 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": DATA, "impl": "reference",
-           "config": {"workload": WORKLOAD, "grid": list(p.n), "form": "fp64"},
+           "config": run_config(args, p, workload, world),
            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": thr, "kind": "port",
-                            "sample": f"{n} of the requested {args.steps} steps (time budget {args.cpu_budget:.0f} s)"
-                                      " of the 256^3 workload: the reference is Fortran+MPI+FFTW and cannot be built"
-                                      " here, so its CPU path runs as the C++ OpenMP restatement in oracle/"},
+                            "sample": f"{n} of the requested {args.steps} steps after {args.warmup} warm-up steps "
+                                      f"(time budget {args.cpu_budget:.0f} s) of the {nx}x{ny}x{nz} workload in FP64: "
+                                      "the reference is Fortran+MPI+FFTW and cannot be built here, so its CPU path "
+                                      "runs as the C++ OpenMP restatement in oracle/"},
            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 

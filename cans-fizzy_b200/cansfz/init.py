@@ -23,12 +23,29 @@ from . import lib as _L
 from .params import Params
 
 
+# A host routine with the signature of cansfz_initgrid that replaces the
+# library's (None: the library's).  A process that must not load libcansfz
+# (the timed CPU run of the reference's algorithm) generates its inputs with
+# its own initgrid through this hook.
+_initgrid = None
+
+
+def use_initgrid(fn) -> None:
+    """Route zgrid through `fn(gtype, nz, gr, lz, dzc, dzf, zc, zf) -> int`
+    (ctypes-callable, double* outputs of nz+2 values); None restores the
+    library's cansfz_initgrid."""
+    global _initgrid
+    _initgrid = fn
+
+
 def zgrid(p: Params) -> dict:
-    """initgrid (src/initgrid.f90:14-78) through the library's host routine."""
+    """initgrid (src/initgrid.f90:14-78) through the library's host routine
+    (or the routine set with use_initgrid)."""
     nz = p.ng[2]
     arrs = [np.zeros(nz + 2) for _ in range(4)]
-    _L.check(_L.load().cansfz_initgrid(int(p.gtype), int(nz), float(p.gr), float(p.l[2]),
-                                       *[a.ctypes.data_as(_L.PD) for a in arrs]), "cansfz_initgrid")
+    fn = _initgrid if _initgrid is not None else _L.load().cansfz_initgrid
+    _L.check(fn(int(p.gtype), int(nz), float(p.gr), float(p.l[2]), *[a.ctypes.data_as(_L.PD) for a in arrs]),
+             "initgrid")
     dzc, dzf, zc, zf = arrs
     return {"dzc": dzc, "dzf": dzf, "zc": zc, "zf": zf, "dzci": 1.0 / dzc, "dzfi": 1.0 / dzf}
 

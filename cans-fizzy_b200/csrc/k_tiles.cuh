@@ -60,16 +60,17 @@ inline int rows_of(const Geo& g) { return g.ny <= 2 ? 2 : 8; }
 // z levels per block; `slots`: blocks per SM that the split aims at (the
 // ACDI and Youngs tiles 24, the momentum tile 48, measured at 256^3)
 template <int TYV>
-inline int kz_of(const Geo& g, int batched, int slots = 24) {
+inline int kz_of(const Geo& g, int batched, int nsm, int slots = 24) {
   using S = Shape<TYV>;
   // in an ensemble the other cases keep the GPU busy: 32 levels per block
   // spend 6% on the two extra planes each block loads (25% at 8 levels)
   if (batched) return g.nz < 32 ? g.nz : 32;
-  // several waves of resident blocks on each of 148 SMs, so the last partial
-  // wave costs little; at least 8 levels per block (each block loads two
-  // planes and evaluates one face/vertex plane beyond its own levels)
+  // several waves of resident blocks on each of the device's SMs (148 on a
+  // B200), so the last partial wave costs little; at least 8 levels per
+  // block (each block loads two planes and evaluates one face/vertex plane
+  // beyond its own levels)
   const long long xy = (long long)((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
-  long long kz = (xy * g.nz) / (148LL * slots);
+  long long kz = (xy * g.nz) / ((long long)(nsm > 0 ? nsm : 148) * slots);
   if (kz < 8) kz = 8;
   if (kz > 64) kz = 64;
   return (int)kz;

@@ -34,6 +34,10 @@ namespace {
 
 constexpr size_t kMaxCells = (size_t)128 * 128 * 128;  // 2,097,152 cells of FP64 scratch: 16 MiB
 constexpr int kMaxLine = 1024;                          // longest x or y transform
+// longest z column: the z solve keeps one FP64 pivot checkpoint per 16
+// levels for each of its 64 columns in shared memory (32 bytes per level),
+// which must fit the 48 KiB a kernel gets without opting in
+constexpr int kMaxZ = 1536;
 
 static __device__ __align__(256) double g_scratch[kMaxCells];
 static __device__ __align__(256) double2 g_tw[2][kMaxLine / 2];
@@ -61,7 +65,7 @@ int setup_device(int dev) {
   if (cudaGetSymbolAddress((void**)&s.tw2, g_tw2) != cudaSuccess) return CANSFZ_ERR_CUDA;
   if (cudaGetSymbolAddress((void**)&s.twc, g_twc) != cudaSuccess) return CANSFZ_ERR_CUDA;
   cansfz::poisson_set_attributes();
-  if (cudaGetLastError() != cudaSuccess) return CANSFZ_ERR_CUDA;
+  if (cudaPeekAtLastError() != cudaSuccess) return CANSFZ_ERR_CUDA;
   s.ready = true;
   return CANSFZ_OK;
 }
@@ -106,11 +110,15 @@ extern "C" int cansfz_solver_static(const int n[3], const char cbc[3][2], double
   if (!n || !cbc || !lambdaxy || !a || !b || !c || !p) return CANSFZ_ERR_ARG;
   const int nx = n[0], ny = n[1], nz = n[2];
   if (nx < 2 || ny < 2 || nz < 2 || (nx & 1) || (ny & 1)) return CANSFZ_ERR_ARG;
-  // sizes beyond the static scratch are rejected, not allocated for
-  if ((size_t)nx * ny * nz > kMaxCells || nx > kMaxLine || ny > kMaxLine) return CANSFZ_ERR_ARG;
+  // sizes beyond the static scratch, or beyond what the kernels launch
+  // with, are rejected before anything is launched
+  if ((size_t)nx * ny * nz > kMaxCells || nx > kMaxLine || ny > kMaxLine || nz > kMaxZ) return CANSFZ_ERR_ARG;
   const int kx = kind_of(cbc[0]), ky = kind_of(cbc[1]);
   if (kx < 0 || ky < 0) return CANSFZ_ERR_UNSUPPORTED;
   if (cbc[2][0] == 'P' || cbc[2][1] == 'P') return CANSFZ_ERR_UNSUPPORTED;  // periodic z needs a second buffer
+  // an error left pending by the caller's earlier work is reported before
+  // this call launches anything (and left pending for the caller)
+  if (cudaPeekAtLastError() != cudaSuccess) return CANSFZ_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CANSFZ_ERR_CUDA;
   if (int rc = setup_device(dev)) return rc;
@@ -130,6 +138,7 @@ extern "C" int cansfz_solver_static(const int n[3], const char cbc[3][2], double
     lp.tw2 = s.tw2 + d * (kMaxLine / 2 + 1);
     lp.twc = s.twc + d * (kMaxLine + 1);
     k_twiddles<<<4, 256, 0, st>>>(d, ns[d], s.tw, s.tw2, s.twc);
+    if (cudaGetLastError() != cudaSuccess) return CANSFZ_ERR_CUDA;
   }
   pl.lam = lambdaxy;
   pl.a = a;

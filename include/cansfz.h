@@ -348,9 +348,11 @@ int cansfz_ensemble_info(cansfz_ensemble* ens, int* ngroups, int* grouped_cases)
  * run: the spectral work buffer and the twiddle tables are static device
  * arrays of this library (16 MiB + 64 KiB on every GPU that loads it), so
  * no cudaMalloc or cudaFree runs.  Limits: nx*ny*nz <= 128^3 cells, nx and
- * ny even and <= 1024, x/y pressure BCs PP, NN or DD, z not periodic;
- * beyond them the call returns CANSFZ_ERR_ARG or CANSFZ_ERR_UNSUPPORTED
- * and launches nothing.  n: interior sizes; cbc: cbcpre(0:1,1:3); normfft,
+ * ny even and <= 1024, nz <= 1536, x/y pressure BCs PP, NN or DD, z not
+ * periodic; beyond them the call returns CANSFZ_ERR_ARG or
+ * CANSFZ_ERR_UNSUPPORTED and launches nothing.  A CUDA error already
+ * pending when the call starts is returned as CANSFZ_ERR_CUDA before any
+ * launch, and left pending.  n: interior sizes; cbc: cbcpre(0:1,1:3); normfft,
  * lambdaxy (nx*ny, packed spectral order), a, b, c (nz): initsolver's
  * outputs as cansfz_solver uses them (device pointers); p: halo-layout
  * device field, right-hand side in, solution out (interior).  The first

@@ -1307,7 +1307,7 @@ static double bulk_mean_12_stag(const Dims& D, int idir, const double* gvr, cons
 }
 
 // cmpt_mean_mass, src/output.f90:759-790
-static void cmpt_mean_mass(Case& C, double mass12[2]) {
+static void cmpt_mean_mass(Case& C, const double* psi, double mass12[2]) {
   const Dims& D = C.D;
   std::vector<double> p1(D.n3 + 1, 0.), p2(D.n3 + 1, 0.);
 #pragma omp parallel for schedule(static)
@@ -1316,7 +1316,7 @@ static void cmpt_mean_mass(Case& C, double mass12[2]) {
     const double vcell = C.dl[0] * C.dl[1] * C.dzf[k];
     for (int j = 1; j <= D.n2; ++j)
       for (int i = 1; i <= D.n1; ++i) {
-        const double ps = C.psi[D.h(i, j, k)];
+        const double ps = psi[D.h(i, j, k)];
         m1 = m1 + C.P.rho12[0] * ps * vcell;
         m2 = m2 + C.P.rho12[1] * (1. - ps) * vcell;
       }
@@ -1375,27 +1375,32 @@ static void prepare(Case& C) {
   C.dto = C.dt;
 }
 
-// rk_2fl, src/rk.f90:193-254
-static void rk_2fl(Case& C, const double tm[2]) {
+// rk_2fl, src/rk.f90:193-254, on the given fields; the dpsidtrk/dpsidtrko
+// histories are the case's `save` state
+static void rk_2fl_fields(Case& C, const double tm[2], double dt, double gam, double seps, double beta,
+                          const double* u, const double* v, const double* w, const double* nx, const double* ny,
+                          const double* nz, const double* phi, double* psi, double* fx, double* fy, double* fz) {
   const cansfz_params& P = C.P;
   const Dims& D = C.D;
-  const double factor1 = tm[0] * C.dt, factor2 = tm[1] * C.dt;
+  const double factor1 = tm[0] * dt, factor2 = tm[1] * dt;
   if (P.interface_capturing == CANSFZ_ACDI)
-    acdi_transport_pf(D, C.dli, C.dzci.data(), C.dzfi.data(), C.gam, C.seps, C.u.data(), C.v.data(), C.w.data(),
-                      C.normx.data(), C.normy.data(), C.normz.data(), C.phi.data(), C.psi.data(), C.dpsi.data(),
-                      C.fx.data(), C.fy.data(), C.fz.data(), P.sdf_normals != 0);
+    acdi_transport_pf(D, C.dli, C.dzci.data(), C.dzfi.data(), gam, seps, u, v, w, nx, ny, nz, phi, psi,
+                      C.dpsi.data(), fx, fy, fz, P.sdf_normals != 0);
   else
-    vof_thinc_transport_psi(D, C.dli, C.dzfi.data(), C.vof_beta, C.u.data(), C.v.data(), C.w.data(), C.normx.data(),
-                            C.normy.data(), C.normz.data(), C.phi.data(), C.psi.data(), C.dpsi.data(), C.fx.data(),
-                            C.fy.data(), C.fz.data(), P.sdf_normals != 0);
+    vof_thinc_transport_psi(D, C.dli, C.dzfi.data(), beta, u, v, w, nx, ny, nz, phi, psi, C.dpsi.data(), fx, fy,
+                            fz, P.sdf_normals != 0);
   if (C.rk2_first) { C.dpsio = C.dpsi; C.rk2_first = false; }
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= D.n3; ++k)
     for (int j = 1; j <= D.n2; ++j)
       for (int i = 1; i <= D.n1; ++i)
-        C.psi[D.h(i, j, k)] = C.psi[D.h(i, j, k)] + factor1 * C.dpsi[D.t(i, j, k)] + factor2 * C.dpsio[D.t(i, j, k)];
-  clip_field(D, 0., 1., C.psi.data());
+        psi[D.h(i, j, k)] = psi[D.h(i, j, k)] + factor1 * C.dpsi[D.t(i, j, k)] + factor2 * C.dpsio[D.t(i, j, k)];
+  clip_field(D, 0., 1., psi);
   std::swap(C.dpsi, C.dpsio);
+}
+static void rk_2fl(Case& C, const double tm[2]) {
+  rk_2fl_fields(C, tm, C.dt, C.gam, C.seps, C.vof_beta, C.u.data(), C.v.data(), C.w.data(), C.normx.data(),
+                C.normy.data(), C.normz.data(), C.phi.data(), C.psi.data(), C.fx.data(), C.fy.data(), C.fz.data());
 }
 
 // rk_scal, src/rk.f90:133-191: AB2 of the scalar with the heat-capacity
@@ -1428,17 +1433,19 @@ static void rk_scal(Case& C, const double tm[2]) {
                  C.fy.data(), C.fz.data(), C.s.data());
 }
 
-// rk, src/rk.f90:16-131
-static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3]) {
+// rk, src/rk.f90:16-131, on the given fields; the d?dtrk/d?dtrko histories
+// are the case's `save` state
+static void rk_fields(Case& C, const double tm[2], double dt, double dt_r, const double rho_av[3],
+                      const double* psi, const double* kappa, const double* p, const double* pn, const double* po,
+                      const double* s, const double* psio, const double* fx, const double* fy, const double* fz,
+                      double* u, double* v, double* w) {
   const cansfz_params& P = C.P;
   const Dims& D = C.D;
-  const double factor1 = tm[0] * C.dt, factor2 = tm[1] * C.dt, factor12 = factor1 + factor2;
-  mom_xyz_ad(D, C.dli, C.dzci.data(), C.dzfi.data(), P.rho12, P.mu12, C.fx.data(), C.fy.data(), C.fz.data(),
-             C.u.data(), C.v.data(), C.w.data(), C.psi.data(), C.du.data(), C.dv.data(), C.dw.data());
+  const double factor1 = tm[0] * dt, factor2 = tm[1] * dt, factor12 = factor1 + factor2;
+  mom_xyz_ad(D, C.dli, C.dzci.data(), C.dzfi.data(), P.rho12, P.mu12, fx, fy, fz, u, v, w, psi, C.du.data(),
+             C.dv.data(), C.dw.data());
   if (C.rk_first) { C.duo = C.du; C.dvo = C.dv; C.dwo = C.dw; C.rk_first = false; }
   const double rho = P.rho12[1], drho = P.rho12[0] - P.rho12[1];
-  double *u = C.u.data(), *v = C.v.data(), *w = C.w.data();
-  const double *psi = C.psi.data(), *psio = C.psio.data();
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= D.n3; ++k)
     for (int j = 1; j <= D.n2; ++j)
@@ -1456,8 +1463,8 @@ static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3])
       }
   std::swap(C.du, C.duo); std::swap(C.dv, C.dvo); std::swap(C.dw, C.dwo);
   mom_xyz_oth(D, C.dli, C.dzci.data(), dt_r, P.rho12, P.beta12, P.bforce, P.gacc, P.sigma, C.rho0, rho_av,
-              C.p.data(), C.psi.data(), C.kappa.data(), P.scalar && P.boussinesq ? C.s.data() : nullptr, C.split(),
-              C.pn.data(), C.po.data(), C.du.data(), C.dv.data(), C.dw.data(), P.brackbill != 0);
+              p, psi, kappa, P.scalar && P.boussinesq ? s : nullptr, C.split(), pn, po, C.du.data(), C.dv.data(),
+              C.dw.data(), P.brackbill != 0);
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= D.n3; ++k)
     for (int j = 1; j <= D.n2; ++j)
@@ -1470,6 +1477,10 @@ static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3])
         v[c] = v[c] + factor12 * C.dv[t] / rhoy_p;
         w[c] = w[c] + factor12 * C.dw[t] / rhoz_p;
       }
+}
+static void rk(Case& C, const double tm[2], double dt_r, const double rho_av[3]) {
+  rk_fields(C, tm, C.dt, dt_r, rho_av, C.psi.data(), C.kappa.data(), C.p.data(), C.pn.data(), C.po.data(),
+            C.s.data(), C.psio.data(), C.fx.data(), C.fy.data(), C.fz.data(), C.u.data(), C.v.data(), C.w.data());
 }
 
 // one pass of the loop body of program cans, src/main.f90:414-562
@@ -1813,7 +1824,7 @@ void orc_get_diag(void* h, cansfz_diag* d) {
   std::memset(d, 0, sizeof(*d));
   d->time = C->time; d->istep = C->istep; d->dt = C->dt; d->dto = C->dto; d->dt_cfl = C->dt_cfl;
   d->gam = C->gam; d->seps = C->seps; d->divtot = C->divtot; d->divmax = C->divmax; d->status = C->status;
-  cmpt_mean_mass(*C, d->mass12);
+  cmpt_mean_mass(*C, C->psi.data(), d->mass12);
 }
 void orc_get_grid(void* h, double* dzc, double* dzf, double* zc, double* zf, double* dzci, double* dzfi) {
   Case* C = (Case*)h;
@@ -1892,6 +1903,20 @@ void orc_correc(void* h, double dt, const double* p, double* u, double* v, doubl
 }
 void orc_updatep(void* h, const double* pp, double* p) { updatep(((Case*)h)->D, pp, p); }
 void orc_clip_field(void* h, double rmin, double rmax, double* p) { clip_field(((Case*)h)->D, rmin, rmax, p); }
+// rk_2fl and rk on the given fields, with the case's AB2 histories (the
+// first call of each seeds its history with the current right-hand side)
+void orc_rk_2fl(void* h, const double* rkpar, double dt, double gam, double seps, double beta, const double* u,
+                const double* v, const double* w, const double* nx, const double* ny, const double* nz,
+                const double* phi, double* psi, double* fx, double* fy, double* fz) {
+  rk_2fl_fields(*(Case*)h, rkpar, dt, gam, seps, beta, u, v, w, nx, ny, nz, phi, psi, fx, fy, fz);
+}
+void orc_rk(void* h, const double* rkpar, double dt, double dt_r, const double* rho_av, const double* psi,
+            const double* kappa, const double* p, const double* pn, const double* po, const double* s,
+            const double* psio, const double* fx, const double* fy, const double* fz, double* u, double* v,
+            double* w) {
+  rk_fields(*(Case*)h, rkpar, dt, dt_r, rho_av, psi, kappa, p, pn, po, s, psio, fx, fy, fz, u, v, w);
+}
+void orc_cmpt_mean_mass(void* h, const double* psi, double* mass12) { cmpt_mean_mass(*(Case*)h, psi, mass12); }
 // which: 0 cbcpre, 1 cbcpsi, 2 cbccur, 3..5 cbcnor(:,:,1..3), 6 cbcsca
 void orc_boundp(void* h, int which, double* p) {
   Case* C = (Case*)h;

@@ -75,6 +75,9 @@ def lib():
             "orc_correc": (None, [V, D, P, P, P, P]),
             "orc_updatep": (None, [V, P, P]),
             "orc_clip_field": (None, [V, D, D, P]),
+            "orc_rk_2fl": (None, [V, P, D, D, D, D] + [P] * 10),
+            "orc_rk": (None, [V, P, D, D, P] + [P] * 12),
+            "orc_cmpt_mean_mass": (None, [V, P, P]),
             "orc_boundp": (None, [V, ct.c_int, P]),
             "orc_bounduvw": (None, [V, ct.c_int, P, P, P]),
             "orc_acdi_set_gamma": (D, [V, D, P, P, P]),

@@ -8,7 +8,9 @@ sys.path.insert(0, os.path.join(ROOT, "cans-fizzy_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# the reference checkout (present only in the build container); override
+# with CANSFZ_REFERENCE_DIR
+REFERENCE = os.environ.get("CANSFZ_REFERENCE_DIR", "/root/reference")
 
 
 def pytest_configure(config):

@@ -28,7 +28,10 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 from cansfz import namelist, params  # noqa: E402
 
-CASE = "/root/reference/tests/differentially_heated_cavity"
+# the reference's test case directory (reference checkout from
+# CANSFZ_REFERENCE_DIR, default the build container's read-only copy)
+CASE = os.path.join(os.environ.get("CANSFZ_REFERENCE_DIR", "/root/reference"), "tests",
+                    "differentially_heated_cavity")
 
 
 def nusselt(s_interior, p):

@@ -3,9 +3,9 @@
 * deformation and return of a circle in the reference's serpentine vortex
   ('voy' prescribed velocity, src/initflow.f90:242-258), ACDI transport only:
   after one period the interface must return to its initial position;
-* full-size (256^3) properties of the FP64 step on the droplet workload:
-  max divergence after the projection, phase-mass drift, and the same
-  drift as the oracle over the first steps at a reduced size;
+* the phase-mass change and the divergence after the projection against
+  the oracle's own at 96^3 over 20 steps (the 256^3 benchmark workload is
+  compared with the oracle in test_gpu_configs.py);
 * the reference's abort conditions (src/main.f90:534-561) reported as
   status codes, triggered from the host (a NaN planted in an input field,
   a fixed dt above the stability limit) -- no GPU fault is involved.
@@ -91,27 +91,6 @@ def test_vortex_deformation_and_return():
     assert l1 < 2e-2, l1
     m0 = np.sum(ref)
     assert abs(np.sum(psi) - m0) / m0 < 1e-3
-
-
-@pytest.fixture(scope="module")
-def droplets_full():
-    p, f = workloads.droplets_acdi(seed=2026)
-    return p, f
-
-
-def test_full_size_divergence_and_mass(droplets_full):
-    p, f = droplets_full
-    g = C.Case(p)
-    g.set_fields(*f)
-    g.prepare()
-    m0 = g.diag().mass12
-    assert g.step(20) == 0  # icheck = 10: two divergence checks
-    d = g.diag()
-    # projection to FP64 round-off (the reference aborts above 2.2e-9)
-    assert d.divmax < 1e-10, d.divmax
-    drift = abs(d.mass12[0] - m0[0]) / m0[0]
-    assert drift < 1e-10, drift
-    g.close()
 
 
 def test_mass_drift_matches_oracle():
