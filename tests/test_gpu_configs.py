@@ -49,7 +49,8 @@ def test_c3a_droplets_256cube():
     g.prepare()
     o.prepare()
     mg0, mo0 = g.diag().mass12[0], o.diag().mass12[0]
-    assert abs(mg0 - mo0) <= 1e-14 * mo0
+    # the two reductions sum 16.8M cells in different orders (~3e-14 apart)
+    assert abs(mg0 - mo0) <= 1e-13 * mo0
     assert g.step(10) == 0 and o.step(10) == 0
     errs = _check_step(g, o)
     dg, do = g.diag(), o.diag()
