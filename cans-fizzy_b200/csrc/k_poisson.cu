@@ -768,6 +768,195 @@ __global__ void __launch_bounds__(128) k_zsolve(int ncol, int nz, const double* 
   ZSolve<T>::run(blk_here(), ncol, nz, lam, a, b, c, sc, work, zsing);
 }
 
+// ---------------------------------------------------------------------------
+// z, partitioned: a tile of 32 columns with all nz levels in shared memory,
+// the levels split into P = 8 chunks of CH levels, one warp per chunk and one
+// lane per column.  The spectral buffer is read once and written once (the
+// column solve above reads and writes each level twice), and 256 threads
+// share each column's elimination instead of one.
+//
+//   A  each chunk eliminates its interior rows s+1..e-1 twice with running
+//      scalars only: downwards with x_s as a parameter, which turns row e
+//      into a row in (x_s, x_e, x_{e+1}), and upwards with x_e as a
+//      parameter, which turns row s into a row in (x_{s-1}, x_s, x_e);
+//   B  those 2P rows form a tridiagonal system in the chunks' end values
+//      (x_s0, x_e0, x_s1, x_e1, ...), solved by Thomas in one warp;
+//   C  with x_s and x_e known, each chunk solves its interior rows by Thomas
+//      (forward sweep into shared memory, the c/pivot factors in registers,
+//      back substitution).
+//
+// The order of elimination differs from gaussel's (src/solver.f90:151-177)
+// only by round-off for these diagonally dominant systems (|b + lambda| >=
+// |a| + |c|).  The one singular system, the (0,0) mode of an all-periodic/
+// Neumann problem, whose eps-shifted pivot (src/solver.f90:163-167) fixes
+// the solution's constant, is solved by one thread of block 0 in gaussel's
+// own order (thomas_column's operations) from a copy of its right-hand
+// side, while the rest of the grid runs.
+// ---------------------------------------------------------------------------
+constexpr int ZP_NC = 32;  // columns per tile
+constexpr int ZP_P = 8;    // chunks (warps) per tile
+// the chunk lengths built (nz = 8 * CH)
+#define CANSFZ_FOR_ZCHUNKS(X) X(8) X(12) X(16) X(24) X(32)
+
+__device__ __forceinline__ void cp16_cg(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc));
+}
+
+template <typename T>
+constexpr size_t zpart_smem(int nz) {
+  return sizeof(T) * ((size_t)nz * ZP_NC + (size_t)8 * ZP_P * ZP_NC + (size_t)2 * ZP_P * ZP_NC + 2 * (size_t)nz);
+}
+
+template <typename T, int CH>
+struct ZSolvePart {
+  static __device__ __forceinline__ void run(const Blk& bk, int ncol, int nz, const double* __restrict__ lam,
+      const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+      const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
+    typedef Rn<T> R;
+    if (HALTED(sc)) return;
+    static_assert(CH >= 3, "a chunk needs an interior row");
+    constexpr int NC = ZP_NC, P = ZP_P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* tile = reinterpret_cast<T*>(smraw);        // [nz][NC]
+    T* red = tile + (size_t)nz * NC;               // [2P][4][NC]: sub, diag, sup, rhs of the reduced rows
+    T* xb = red + (size_t)8 * P * NC;              // [2P][NC]: x_s, x_e of every chunk
+    T* s0 = xb + (size_t)2 * P * NC;               // [2][nz]: column 0 of block 0 (serial path)
+    const int col0 = bk.x * NC;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int s = w * CH, e = s + CH - 1;
+    // each warp stages its own chunk's rows (16-byte copies of rows of NC
+    // consecutive columns) and starts on them without waiting for the others
+    constexpr int PER = 16 / (int)sizeof(T), CPR = NC / PER;
+    for (int q = lane; q < CH * CPR; q += 32) {
+      const int l = s + q / CPR, cc = (q % CPR) * PER;
+      cp16_cg(tile + (size_t)l * NC + cc, work + (size_t)l * ncol + col0 + cc);
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    const T lm = (T)__ldg(lam + col0 + lane);
+    const bool serial0 = col0 == 0 && __ldg(lam) == 0.;
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncwarp();
+    // ---- A: the chunk's two reduced rows.  The downward sweep's pivot
+    // reciprocals are those of C's forward sweep (same rows, same first
+    // pivot), so they are kept for it and C needs no reciprocal.
+    T rp[CH - 2];
+    {
+      T D = 0, Y = 0, F = 0, U = 0, Z = 0, G = 0;
+#pragma unroll
+      for (int t = 0; t < CH - 2; ++t) {
+        const int id = s + 1 + t, iu = e - 1 - t;
+        const T ad = (T)__ldg(a + id), cd = (T)__ldg(c + id), bd = (T)__ldg(b + id) + lm;
+        const T au = (T)__ldg(a + iu), cu = (T)__ldg(c + iu), bu = (T)__ldg(b + iu) + lm;
+        const T dd = tile[id * NC + lane], du = tile[iu * NC + lane];
+        const T rd = recip_rn(t == 0 ? bd : bd - ad * D);
+        rp[t] = rd;
+        Y = (t == 0 ? dd : dd - ad * Y) * rd;
+        F = (t == 0 ? -ad : -ad * F) * rd;
+        D = cd * rd;
+        const T ru = recip_rn(t == 0 ? bu : bu - cu * U);
+        Z = (t == 0 ? du : du - cu * Z) * ru;
+        G = (t == 0 ? -cu : -cu * G) * ru;
+        U = au * ru;
+      }
+      T* Rs = red + (size_t)(2 * w) * 4 * NC;
+      T* Re = Rs + 4 * NC;
+      const T as = (T)__ldg(a + s), bs = (T)__ldg(b + s) + lm, cs = (T)__ldg(c + s);
+      const T ae = (T)__ldg(a + e), be = (T)__ldg(b + e) + lm, ce = (T)__ldg(c + e);
+      Rs[0 * NC + lane] = w == 0 ? (T)0 : as;
+      Rs[1 * NC + lane] = bs - cs * U;
+      Rs[2 * NC + lane] = cs * G;
+      Rs[3 * NC + lane] = tile[s * NC + lane] - cs * Z;
+      Re[0 * NC + lane] = ae * F;
+      Re[1 * NC + lane] = be - ae * D;
+      Re[2 * NC + lane] = w == P - 1 ? (T)0 : ce;
+      Re[3 * NC + lane] = tile[e * NC + lane] - ae * Y;
+      if (serial0 && lane == 0)
+        for (int l = s; l <= e; ++l) s0[l] = tile[(size_t)l * NC];  // column 0's right-hand side
+    }
+    __syncthreads();
+    // ---- B: the reduced system of the 2P chunk-end values
+    if (w == 0) {
+      T Dp = 0, Yp = 0;
+      for (int r = 0; r < 2 * P; ++r) {
+        T* Rr = red + (size_t)r * 4 * NC;
+        const T sub = Rr[0 * NC + lane], dg = Rr[1 * NC + lane], sup = Rr[2 * NC + lane], rhs = Rr[3 * NC + lane];
+        const T rr = recip_rn(r == 0 ? dg : dg - sub * Dp);
+        Dp = sup * rr;
+        Yp = (r == 0 ? rhs : rhs - sub * Yp) * rr;
+        Rr[0 * NC + lane] = Dp;
+        Rr[1 * NC + lane] = Yp;
+      }
+      T x = Yp;
+      xb[(2 * P - 1) * NC + lane] = x;
+      for (int r = 2 * P - 2; r >= 0; --r) {
+        const T* Rr = red + (size_t)r * 4 * NC;
+        x = Rr[1 * NC + lane] - Rr[0 * NC + lane] * x;
+        xb[r * NC + lane] = x;
+      }
+    }
+    __syncthreads();
+    // ---- C: the chunk's interior rows with x_s and x_e known, then its rows
+    // out (column 0 of block 0 waits for the serial solve)
+    {
+      const T xs = xb[(2 * w) * NC + lane], xe = xb[(2 * w + 1) * NC + lane];
+      T Y = 0;
+#pragma unroll
+      for (int t = 0; t < CH - 2; ++t) {
+        const int i = s + 1 + t;
+        const T ai = (T)__ldg(a + i), ci = (T)__ldg(c + i);
+        T rhs = tile[i * NC + lane];
+        if (t == 0) rhs -= ai * xs;
+        if (t == CH - 3) rhs -= ci * xe;  // row e-1: x_e is known, no super-diagonal left
+        Y = (t == 0 ? rhs : rhs - ai * Y) * rp[t];
+        tile[i * NC + lane] = Y;
+      }
+      T* out = work + col0 + lane;
+      const bool keep = !(serial0 && lane == 0);
+      if (keep) {
+        out[(size_t)s * ncol] = xs;
+        out[(size_t)e * ncol] = xe;
+        out[(size_t)(e - 1) * ncol] = Y;
+      }
+      T x = Y;
+#pragma unroll
+      for (int t = CH - 4; t >= 0; --t) {
+        const int i = s + 1 + t;
+        x = tile[i * NC + lane] - ((T)__ldg(c + i) * rp[t]) * x;
+        if (keep) out[(size_t)i * ncol] = x;
+      }
+    }
+    if (serial0 && threadIdx.x == 0) {
+      // gaussel's elimination order and rounding for the singular mode
+      T* pv = s0;
+      T* dd = s0 + nz;
+      const bool pin = sizeof(T) == 4 && zsing;
+      T dprev = 0, pprev = 0;
+      for (int l = 0; l < nz; ++l) {
+        const T z = piv_inv<T>(l, nz, (T)__ldg(b + l), (T)0, (T)__ldg(a + l), dprev, pin);
+        const T d = R::mul((T)__ldg(c + l), z);
+        const T pn = l == 0 ? R::mul(pv[l], z) : R::mul(R::sub(pv[l], R::mul((T)__ldg(a + l), pprev)), z);
+        dd[l] = d;
+        pv[l] = pn;
+        dprev = d;
+        pprev = pn;
+      }
+      T pnext = 0;
+      for (int l = nz - 1; l >= 0; --l) {
+        if (l < nz - 1) pv[l] = R::sub(pv[l], R::mul(dd[l], pnext));
+        pnext = pv[l];
+        work[(size_t)l * ncol] = pv[l];
+      }
+    }
+  }
+};
+template <typename T, int CH>
+__global__ void __launch_bounds__(256, 2) k_zsolve_part(int ncol, int nz, const double* __restrict__ lam,
+    const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+    const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
+  ZSolvePart<T, CH>::run(blk_here(), ncol, nz, lam, a, b, c, sc, work, zsing);
+}
+
 // periodic z: gaussel_periodic (src/solver.f90:107-149)
 template <typename T>
 struct ZSolvePeriodic {
@@ -906,7 +1095,16 @@ static void set_attr_len() {
 }
 
 // opt the transform kernels into > 48 KB of dynamic shared memory (once)
+template <typename T, int CH>
+static void set_attr_zpart() {
+  cudaFuncSetAttribute(k_zsolve_part<T, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)zpart_smem<T>(CH * ZP_P));
+}
+
 void poisson_set_attributes() {
+#define X(C) set_attr_zpart<double, C>(); set_attr_zpart<float, C>();
+  CANSFZ_FOR_ZCHUNKS(X)
+#undef X
   set_attr_len<double, 0>();
   set_attr_len<float, 0>();
 #define X(M) set_attr_len<double, M>(); set_attr_len<float, M>();
@@ -992,10 +1190,39 @@ void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool
                                                               static_cast<double*>(piv), static_cast<double*>(df));
 }
 
+template <typename T, int CH>
+static void z_part_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
+  const int ncol = g.nx * g.ny;
+  kgo<ZSolvePart<T, CH>, 256, 2>(Lc, k_zsolve_part<T, CH>, ncol / ZP_NC, 32 * ZP_P, zpart_smem<T>(g.nz), ncol,
+                                 g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl), pl.zsing);
+}
+
+// the partitioned solve serves non-periodic z with nz = 8 * CH and whole
+// tiles of columns; few-column grids keep the factored solve
+static bool z_part_ok(const Geo& g, const PoissonPlan& pl) {
+  const int ncol = g.nx * g.ny;
+  if (pl.zper || ncol % ZP_NC != 0 || g.nz % ZP_P != 0) return false;
+  switch (g.nz / ZP_P) {
+#define X(C) case C:
+    CANSFZ_FOR_ZCHUNKS(X)
+#undef X
+    return true;
+    default: return false;
+  }
+}
+
 template <typename T>
 static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
   const int tb = 64;
+  if (!(zpiv<T>(pl) && zdf<T>(pl)) && z_part_ok(g, pl)) {
+    switch (g.nz / ZP_P) {
+#define X(C) case C: z_part_len<T, C>(Lc, g, pl, sc); return;
+      CANSFZ_FOR_ZCHUNKS(X)
+#undef X
+      default: break;
+    }
+  }
   if (zpiv<T>(pl) && zdf<T>(pl)) {
     if (pl.zper)
       kgo<ZSolvePeriodicF<T>, 128, 1>(Lc, k_zsolve_periodic_f<T>, (ncol + tb - 1) / tb, tb, 0, ncol, g.nz, pl.lam,

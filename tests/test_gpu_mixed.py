@@ -23,12 +23,20 @@ def _poisson_pair(n=64, seed=2026, cbc="PPPPNN"):
     p, rhs = workloads.poisson_rhs(n, seed)
     if cbc != "PPPPNN":
         p.cbcpre = cbc.encode()
+    # compatible with the discrete Neumann/periodic operator: zero mean under
+    # the cell-height weights dzf, which vary at the 1e-8 level where initgrid's
+    # single-precision z0 quotient does not divide evenly (nz = 192); the plain
+    # mean leaves a residue no solve can remove
+    dzf = init.zgrid(p)["dzf"][1:-1]
+    r = rhs[1:-1, 1:-1, 1:-1]
+    r -= (r * dzf[None, None, :]).sum() / (dzf.sum() * r.shape[0] * r.shape[1])
     return p, rhs
 
 
-@pytest.mark.parametrize("cbc", ["PPPPNN", "NNPPNN", "PPPPPP"])
-def test_refinement_converges(cbc):
-    p, rhs = _poisson_pair(64, 2026, cbc)
+@pytest.mark.parametrize("cbc,n", [("PPPPNN", 64), ("NNPPNN", 64), ("PPPPPP", 64),
+                                   ("PPPPNN", 192)])  # 192^3: the partitioned z solve
+def test_refinement_converges(cbc, n):
+    p, rhs = _poisson_pair(n, 2026, cbc)
     g = C.Case(p)
     ref = g.field(rhs)
     g.call("solver", ref)
@@ -47,10 +55,10 @@ def test_refinement_converges(cbc):
         g.call("poisson_residual", src, out, r)
         rr = r.get()[1:-1, 1:-1, 1:-1]
         res_norms.append(np.abs(rr).max() / np.abs(rhs).max())
-    assert errs[0] < 1e-4, errs
-    assert errs[1] < errs[0] * 1e-2, errs
-    assert errs[2] < 1e-11 or errs[2] < errs[1] * 1e-2, errs
-    assert res_norms[3] < 1e-11, res_norms
+    assert errs[0] < 1e-4, (errs, res_norms)
+    assert errs[1] < errs[0] * 1e-2, (errs, res_norms)
+    assert errs[2] < 1e-11 or errs[2] < errs[1] * 1e-2, (errs, res_norms)
+    assert res_norms[3] < 1e-11, (errs, res_norms)
 
 
 def _step_params(n=32, mixed=True, sweeps=2):

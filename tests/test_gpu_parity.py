@@ -178,7 +178,13 @@ def test_projection_procedures(small):
 @pytest.mark.parametrize("cbcpre,ng", [("PPPPNN", (24, 16, 20)), ("NNPPNN", (24, 16, 20)), ("DDPPNN", (24, 16, 20)),
                                         ("PPNNNN", (24, 16, 20)), ("PPPPPP", (24, 16, 20)), ("NNNNNN", (24, 16, 20)),
                                         # nx*ny >= 32768: the z solve evaluates its pivots on the fly
-                                        ("PPPPNN", (256, 128, 8)), ("PPPPPP", (256, 128, 8))])
+                                        ("PPPPNN", (256, 128, 8)), ("PPPPPP", (256, 128, 8)),
+                                        # ... in the partitioned form (nz = 8 * chunk, whole tiles of 32 columns)
+                                        ("PPPPNN", (256, 128, 64)), ("NNPPNN", (256, 128, 96)),
+                                        ("DDNNDD", (128, 256, 64)), ("PPPPDD", (256, 128, 128)),
+                                        ("NNNNNN", (256, 128, 64)),
+                                        # lines of 192 points (radix 4, 4, 2, 3); a z chunk of 24 levels
+                                        ("PPPPNN", (192, 192, 64)), ("PPPPNN", (256, 128, 192))])
 def test_poisson_bcs(cbcpre, ng):
     p = _nml(*ng, cbcpre, l=(1.0, 0.75, 1.2))
     g, o = C.Case(p), O.Case(p)
