@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCES = ["csrc/k_stencil.cu", "csrc/k_tiles.cu", "csrc/k_momentum.cu", "csrc/k_init.cu", "csrc/k_bc.cu", "csrc/k_poisson.cu",
-           "csrc/context.cu", "csrc/noalloc.cu"]
+           "csrc/context.cu", "csrc/noalloc.cu", "csrc/k_xform_gemm.cu"]
 OUT = os.path.join(HERE, "cansfz", "libcansfz.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -81,6 +81,7 @@ SIGNATURES = {
     "cansfz_profile_stages": (I, [V, I, PD, I, ct.POINTER(I), ct.c_char_p, I]),
     "cansfz_solver_refined": (I, [V, V, V, I]),
     "cansfz_poisson_residual": (I, [V, V, V, V]),
+    "cansfz_xform_matrix": (I, [I, I, I, PD]),
     "cansfz_ensemble_create": (I, [V, I, V, V]),
     "cansfz_ensemble_step": (I, [V, I, V]),
     "cansfz_ensemble_destroy": (I, [V]),

@@ -108,6 +108,9 @@ SCHEMA = {
         "acdi_gam_min": Var("r", (), (), _sp(1.0e-12)),
         "form": Var("s", (), (), "fp64"),
         "refine_sweeps": Var("i", (), (), -1),
+        # the FP32 solve's x/y transforms: 'gemm' (tensor cores where the
+        # line lengths allow) or 'fft'
+        "fp32_transforms": Var("s", (), (), "gemm"),
     },
     "cudecomp": {},
 }

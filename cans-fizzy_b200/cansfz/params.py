@@ -54,7 +54,8 @@ class Params(ct.Structure):
         ("cp12", ct.c_double * 2),
         ("form", ct.c_int32),
         ("refine_sweeps", ct.c_int32),
-        ("reserved", ct.c_int32 * 8),
+        ("fp32_transforms", ct.c_int32),
+        ("reserved", ct.c_int32 * 7),
     ]
 
     # -- convenience views -------------------------------------------------
@@ -130,6 +131,7 @@ def from_namelist(nl: _nml.Namelist) -> Params:
     p.cp12[:] = _dbls(nl["cp12"])
     p.form = FORM_MIXED if str(nl["form"]).lower().startswith("mix") else FORM_FP64
     p.refine_sweeps = int(nl["refine_sweeps"])
+    p.fp32_transforms = 1 if str(nl["fp32_transforms"]).lower().startswith("fft") else 0
     return p
 
 

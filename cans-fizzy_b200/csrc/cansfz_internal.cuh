@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/cansfz.h"
 
 #define CANSFZ_EPS 2.220446049250313e-16  // epsilon(1._rp), src/param.f90:18
@@ -149,6 +151,10 @@ struct PoissonPlan {
   double* zdf;
   float* zpivf;
   float* zdff;
+  // the FP32 solve's x and y transforms as tensor-core GEMMs (k_xform_gemm.cu):
+  // split-BF16 matrices [0] forward, [1] backward; null: the FFT kernels
+  const uint16_t* gx[2];
+  const uint16_t* gy[2];
 };
 
 // ---------------------------------------------------------------------------
@@ -303,6 +309,13 @@ void launch_updt_rhs_b(const Launch& L, const Geo& g, const int is_bound[3][2],
 
 // k_poisson.cu
 void poisson_set_attributes();
+// tensor-core line transforms of the FP32 solve (k_xform_gemm.cu)
+double xform_coef(int kind, int dir, int n, int j, int k);
+std::vector<uint16_t> xform_bmat(int kind, int dir, int n);
+bool xform_gemm_length(int n);
+int xform_gemm_set_attributes();
+void launch_xform_gemm(const Launch& L, const Geo& g, int mode, bool add, const uint16_t* bmat, int n,
+                       const void* src, void* dst, double normfft, DevScalars* sc);
 // the z systems' elimination factors of `pl` (FP64, or FP32 for the mixed
 // form) into piv/df, evaluated exactly as the solve's forward sweep does
 void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool f32, void* piv, void* df);

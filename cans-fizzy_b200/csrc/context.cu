@@ -284,9 +284,37 @@ bool factorize(int m, int radix[FFT_MAXSTAGES], int* nst) {
 bool zsolve_factored(const cansfz_ctx* c) { return (long long)c->g.nx * c->g.ny < 32768; }
 
 // FP32 spectral buffers and z factors of the mixed-form solve (once)
+// the split-BF16 matrices of the tensor-core transforms (once), for the
+// line lengths and kinds they serve
+int alloc_xform_gemm(cansfz_ctx* c) {
+  const cansfz_params& P = c->P;
+  if (P.fp32_transforms != 0 || c->pl.gx[0] || c->pl.gy[0]) return CANSFZ_OK;
+  static bool attrs = false;
+  if (!attrs) {
+    if (xform_gemm_set_attributes()) return CANSFZ_ERR_CUDA;
+    attrs = true;
+  }
+  const int kinds[2] = {line_kind(P.cbcpre[0]), line_kind(P.cbcpre[1])};
+  const int ns[2] = {c->n[0], c->n[1]};
+  for (int d = 0; d < 2; ++d) {
+    if (!xform_gemm_length(ns[d])) continue;
+    for (int dir = 0; dir < 2; ++dir) {
+      const std::vector<uint16_t> m = xform_bmat(kinds[d], dir == 0 ? 1 : -1, ns[d]);
+      uint16_t* dm = nullptr;
+      int rc;
+      if ((rc = dalloc(c, &dm, m.size()))) return rc;
+      CK(cudaMemcpyAsync(dm, m.data(), m.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      (d == 0 ? c->pl.gx : c->pl.gy)[dir] = dm;
+    }
+  }
+  return CANSFZ_OK;
+}
+
 int alloc_f32_solver(cansfz_ctx* c) {
   const size_t nint = (size_t)c->g.tsize();
   int rc;
+  if ((rc = alloc_xform_gemm(c))) return rc;
   if (!c->pl.workf && (rc = dalloc(c, &c->pl.workf, nint))) return rc;
   if (c->pl.zper && !c->pl.work2f && (rc = dalloc(c, &c->pl.work2f, nint))) return rc;
   if (!c->pl.zpivf && zsolve_factored(c)) {

@@ -1299,11 +1299,16 @@ void launch_poisson_fused_rhs(const Launch& L, const Geo& g, const PoissonPlan& 
 // FP32 spectral solve of the mixed form: dst = S(src), or dst += S(src) (add)
 void launch_poisson_f32(const Launch& L, const Geo& g, const PoissonPlan& pl, const DevScalars* sc,
                         const double* src, double* dst, bool add, const StageMark* mk) {
-  x_forward<float>(L, g, pl, sc, src, nullptr, nullptr, nullptr, nullptr, false);
-  y_pass<float>(L, g, pl, sc, +1);
+  DevScalars* scw = const_cast<DevScalars*>(sc);  // the tensor-core passes report a timed-out wait there
+  if (pl.gx[0]) launch_xform_gemm(L, g, 0, false, pl.gx[0], g.nx, src, pl.workf, 1., scw);
+  else x_forward<float>(L, g, pl, sc, src, nullptr, nullptr, nullptr, nullptr, false);
+  if (pl.gy[0]) launch_xform_gemm(L, g, 1, false, pl.gy[0], g.ny, pl.workf, pl.workf, 1., scw);
+  else y_pass<float>(L, g, pl, sc, +1);
   z_pass<float>(L, g, pl, sc);
-  y_pass<float>(L, g, pl, sc, -1);
-  if (add) x_backward<float, true>(L, g, pl, sc, dst);
+  if (pl.gy[1]) launch_xform_gemm(L, g, 1, false, pl.gy[1], g.ny, pl.workf, pl.workf, 1., scw);
+  else y_pass<float>(L, g, pl, sc, -1);
+  if (pl.gx[1]) launch_xform_gemm(L, g, 2, add, pl.gx[1], g.nx, pl.workf, dst, pl.normfft, scw);
+  else if (add) x_backward<float, true>(L, g, pl, sc, dst);
   else x_backward<float, false>(L, g, pl, sc, dst);
   if (mk) mk->mark(add ? "poisson_f32_correction" : "poisson_f32");
 }

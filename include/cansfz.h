@@ -91,7 +91,11 @@ typedef struct cansfz_params {
   int32_t form;                 /* CANSFZ_FORM_FP64 (drop-in) or CANSFZ_FORM_MIXED */
   int32_t refine_sweeps;        /* mixed form: FP64-residual refinement sweeps of the
                                    FP32 Poisson solve; -1: the Poisson solve in FP64 */
-  int32_t reserved[8];
+  int32_t fp32_transforms;      /* mixed form, FP32 solve: 0 = x/y line transforms as
+                                   split-BF16 GEMMs on the tensor cores (tcgen05) where
+                                   the line lengths are 64, 128 or 256, shared-memory FFTs
+                                   otherwise; 1 = shared-memory FFTs always          */
+  int32_t reserved[7];
 } cansfz_params;
 
 /* Per-step diagnostics, mirrored from the device (main.f90 prints). */
@@ -315,6 +319,12 @@ int cansfz_profile_stages(cansfz_ctx* ctx, int nsteps, double* ms, int maxstages
 int cansfz_solver_refined(cansfz_ctx* ctx, const double* rhs, double* p, int sweeps);
 /* FP64 residual res = rhs - L(p) of that operator (p's ghosts are filled). */
 int cansfz_poisson_residual(cansfz_ctx* ctx, const double* rhs, double* p, double* res);
+/* The dense matrix F (row-major n x n, host array, out[j] = sum_k F[j*n+k]
+ * in[k]) of one line transform of the FP32 solve's tensor-core path: kind 0
+ * the packed real DFT (r0, r_{n/2}, r1, i1, ...) and its unnormalised
+ * inverse, kind 1 DCT-II / DCT-III, kind 2 DST-II / DST-III (FFTW's REDFT10,
+ * REDFT01, RODFT10, RODFT01); dir > 0 forward, dir < 0 backward.          */
+int cansfz_xform_matrix(int kind, int dir, int n, double* F);
 
 /* ---- batched ensemble (no reference counterpart: the reference runs one
  * case per program) -----------------------------------------------------

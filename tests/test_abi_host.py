@@ -206,3 +206,33 @@ def test_read_spheres(reference_dir, tmp_path):
                 found += 1
     assert found > 0
     assert init.read_spheres(str(tmp_path / "none.in")).shape == (0, 4)
+
+
+def test_xform_matrices_match_the_r2r_kinds():
+    """The dense matrices of the FP32 solve's tensor-core transforms against
+    the oracle's restatement of FFTW's kinds (R2HC/HC2R in the packed order
+    (r0, r_{n/2}, r1, i1, ...), REDFT10/01, RODFT10/01)."""
+    L = lib.load()
+    R2HC, HC2R, REDFT01, REDFT10, RODFT01, RODFT10 = 0, 1, 4, 5, 8, 9
+    rng = np.random.default_rng(11)
+    for n in (64, 128, 256, 96):
+        x = rng.standard_normal((3, n))
+
+        def mat(kind, d):
+            F = np.zeros(n * n)
+            assert L.cansfz_xform_matrix(kind, d, n, F.ctypes.data_as(lib.PD)) == 0
+            return F.reshape(n, n)
+
+        # periodic: FFTW's half-complex order -> the packed order
+        hc = O.r2r(R2HC, x)
+        h = n // 2
+        packed = np.zeros_like(hc)
+        packed[:, 0], packed[:, 1] = hc[:, 0], hc[:, h]
+        for k in range(1, h):
+            packed[:, 2 * k], packed[:, 2 * k + 1] = hc[:, k], hc[:, n - k]
+        tol = 1e-12 * n
+        assert np.abs(x @ mat(0, 1).T - packed).max() <= tol * np.abs(packed).max()
+        assert np.abs(packed @ mat(0, -1).T - O.r2r(HC2R, hc)).max() <= tol * n * np.abs(x).max()
+        for kind, fw, bw in ((1, REDFT10, REDFT01), (2, RODFT10, RODFT01)):
+            assert np.abs(x @ mat(kind, 1).T - O.r2r(fw, x)).max() <= tol * np.abs(O.r2r(fw, x)).max()
+            assert np.abs(x @ mat(kind, -1).T - O.r2r(bw, x)).max() <= tol * np.abs(O.r2r(bw, x)).max()
