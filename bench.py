@@ -102,6 +102,8 @@ def parse_args():
                     help="steps of the scalar-transport leg (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps per case of the batched-ensemble measurement (0: skip)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default launch plan instead of the autotuned one")
     ap.add_argument("--no-mixed-leg", dest="mixed_leg", action="store_false",
                     help="skip the mixed-form leg of an FP64 run")
     ap.add_argument("--accuracy-steps", type=int, default=50,
@@ -141,6 +143,20 @@ def run_config(args, p, workload, world):
             "l2": (f"inputs larger than L2 (each FP64 field {hbytes / 1e6:.0f} MB > 126 MB; ~28 fields resident), "
                    "no flush needed" if hbytes > 126e6 else
                    f"profiling size: each FP64 field {hbytes / 1e6:.1f} MB < 126 MB L2, no flush")}
+
+
+def plan_cache():
+    """The autotuner's cache file (one line per grid/form/GPU key)."""
+    d = os.environ.get("CANSFZ_PLAN_CACHE_DIR", os.path.join(os.path.expanduser("~"), ".cache", "cansfz"))
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, "plans.txt")
+
+
+def plan_dict(q, report):
+    return {"phase_slots": q.phase_slots, "momentum_slots": q.momentum_slots,
+            "zsolve": "partitioned tiles" if q.zsolve == 0 else "one column per thread",
+            "fp32_transforms": "tcgen05 GEMM" if q.fp32_transforms == 0 else "FFT",
+            "tuned_ms_per_step": q.ms_per_step, "report": report}
 
 
 def measured_peaks():
@@ -292,6 +308,7 @@ def mixed_leg(args, p0, fields, fp64_ms_step):
     c = C.Case(q)
     c.set_fields(*fields)
     c.prepare()
+    plan, plan_report = c.autotune(plan_cache()) if args.autotune else (c.plan(), "default plan")
     if c.step(args.warmup) != 0:
         raise RuntimeError("mixed warm-up failed")
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -307,7 +324,7 @@ def mixed_leg(args, p0, fields, fp64_ms_step):
     nx, ny, nz = p0.n
     out = {"value": nx * ny * nz / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms,
            "steps": args.steps, "warmup": args.warmup, "speedup_vs_fp64": fp64_ms_step / ms,
-           "refine_sweeps": args.sweeps,
+           "refine_sweeps": args.sweeps, "plan": plan_dict(plan, plan_report),
            "form": ("FP32 stencils, fluxes, curvature and AB2 histories; FP64 state, AB2 accumulation, reductions "
                     "and Poisson solve") if args.sweeps < 0 else
                    (f"FP32 stencils and transforms, FP64 state, AB2 accumulation and reductions, {args.sweeps} "
@@ -373,7 +390,7 @@ def scalar_bench(p0, fields, nsteps, peak):
             "what": "the headline workload with _SCALAR and _BOUSSINESQ_BUOYANCY on; device time, graph-launched"}
 
 
-def ensemble_bench(nsteps, warmup, form):
+def ensemble_bench(nsteps, warmup, form, tune=True):
     """The batched-ensemble configuration: 64 independent rising-bubble cases,
     `nsteps` steps each, run (a) one case at a time (each case's own graph,
     cansfz_step) and (b) batched (cansfz_ensemble_step: one graph launch per
@@ -386,6 +403,8 @@ def ensemble_bench(nsteps, warmup, form):
 
     specs = W.ensemble_cases(seed=4)
 
+    reports = {}
+
     def build():
         cs = []
         for p, f in specs:
@@ -394,6 +413,10 @@ def ensemble_bench(nsteps, warmup, form):
             c = C.Case(q, own_stream=True)
             c.set_fields(*f)
             c.prepare()
+            if tune:
+                # one timing per grid shape (the cache holds the rest)
+                pl, rep = c.autotune(plan_cache())
+                reports.setdefault(f"{q.ng[0]}x{q.ng[1]}x{q.ng[2]}", plan_dict(pl, rep))
             cs.append(c)
         return cs
 
@@ -436,6 +459,7 @@ def ensemble_bench(nsteps, warmup, form):
             "cases_per_s_batched": n / t_bat, "cases_per_s_sequential": n / t_seq,
             "speedup": t_seq / t_bat, "cell_steps_per_s_batched": cells * nsteps / t_bat,
             "batched_equals_sequential": bool(same),
+            "plans": reports,
             "what": "64 rising-bubble cases (seed 4; 32 2-D 64x128..256x512, 32 3-D 32^3..96x96x192); "
                     "wall clock around synchronised work"}
 
@@ -458,6 +482,8 @@ def gpu_arm(args):
     case = C.Case(p)
     case.set_fields(*fields)
     case.prepare()
+    # launch plan: timed on a copy of the case, cached per grid/form/GPU
+    plan, plan_report = case.autotune(plan_cache()) if args.autotune else (case.plan(), "default plan")
     rc = case.step(args.warmup)
     if rc != 0:
         raise RuntimeError(f"warm-up step failed with status {rc}")
@@ -526,6 +552,7 @@ def gpu_arm(args):
         "stage_share": {k: round(v / tot, 4) for k, v in stage_ms.items()},
         "gpu_launches": int(kps.value) * args.steps,
         "clocks": clocks,
+        "plan": plan_dict(plan, plan_report),
     }
     # ---- the same workload with the scalar transport
     if world == 1 and args.config == "c3a" and args.form == "fp64" and args.scalar_steps > 0:
@@ -533,7 +560,7 @@ def gpu_arm(args):
         out["scalar"]["overhead"] = out["scalar"]["ms_per_step"] / ms_step - 1.0
     # ---- batched ensemble of independent small cases
     if world == 1 and args.ensemble_steps > 0 and args.config == "c3a":
-        out["ensemble"] = ensemble_bench(args.ensemble_steps, 3, 0 if args.form == "fp64" else 1)
+        out["ensemble"] = ensemble_bench(args.ensemble_steps, 3, 0 if args.form == "fp64" else 1, args.autotune)
     # ---- mixed form: error against the FP64 form after the same steps from the same state
     if args.form == "mixed" and args.accuracy_steps > 0:
         out["accuracy_vs_fp64"] = mixed_accuracy(p, fields, args.accuracy_steps)
@@ -548,6 +575,8 @@ def gpu_arm(args):
             t.copy_(torch.from_numpy(np.ascontiguousarray(a.reshape(-1, order="F"))))
         ptrs = [_L.ct.c_void_p(t.data_ptr()) for t in pin]
         e2e_case = C.Case(p)
+        if args.autotune:
+            e2e_case.autotune(plan_cache())  # the headline case's cached plan
         ksteps = args.steps
         diag = _L.Diag()
         barrier(world)
@@ -661,13 +690,33 @@ def poisson_arm(args):
     out = g.field()
     rin = rhs[1:-1, 1:-1, 1:-1]
     res = {}
+    # the FP32 solve with its x/y transforms as split-BF16 GEMMs on the tensor
+    # cores, and with the shared-memory FFTs (fp32_transforms = 1)
+    pf = p.copy()
+    pf.fp32_transforms = 1
+    gf = C.Case(pf)
+    srcf, outf = gf.field(rhs), gf.field()
+
+    def timed_f(fn):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(gf.stream)
+        for _ in range(k):
+            fn()
+        e1.record(gf.stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
     for sw in range(4):
+        ms_fft = timed_f(lambda: gf.call("solver_refined", srcf, outf, sw))
         ms = timed(lambda: g.call("solver_refined", src, out, sw))
         b = out.get()[1:-1, 1:-1, 1:-1]
         b = b - b.mean()
         g.call("poisson_residual", src, out, r)
         rr = r.get()[1:-1, 1:-1, 1:-1]
-        res[str(sw)] = {"ms_per_solve": ms, "solves_per_s": 1e3 / ms,
+        res[str(sw)] = {"ms_per_solve": ms, "solves_per_s": 1e3 / ms, "ms_per_solve_fft_transforms": ms_fft,
                         "residual_l2_rel": float(np.linalg.norm(rr) / np.linalg.norm(rin)),
                         "residual_linf_rel": float(np.abs(rr).max() / np.abs(rin).max()),
                         "err_vs_fp64_rel": float(np.abs(b - a64).max() / np.abs(a64).max())}
@@ -676,8 +725,11 @@ def poisson_arm(args):
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
                       "config": {"workload": "poisson_256: 256^3 uniform, periodic x,y, Neumann z, RHS ~ N(0,1) "
                                              "(seed 2026), mean removed", "config": "c2"},
-                      "fp32_refined": res}), flush=True)
+                      "fp32_refined": res,
+                      "fp32_transforms": "x/y as split-BF16 GEMMs on tcgen05 (ms_per_solve); shared-memory FFTs "
+                                         "(ms_per_solve_fft_transforms)"}), flush=True)
     g.close()
+    gf.close()
 
 
 def main():

@@ -147,6 +147,23 @@ class Case:
         _L.check(self.lib.cansfz_get_status(self.h, ct.byref(d)), "cansfz_get_status")
         return d
 
+    def plan(self) -> _L.Plan:
+        q = _L.Plan()
+        _L.check(self.lib.cansfz_get_plan(self.h, ct.byref(q)), "cansfz_get_plan")
+        return q
+
+    def set_plan(self, q: _L.Plan):
+        _L.check(self.lib.cansfz_set_plan(self.h, ct.byref(q)), "cansfz_set_plan")
+
+    def autotune(self, cache_file: str | None = None):
+        """Time candidate launch plans on a copy of this case and apply the
+        fastest (cansfz_autotune); returns (plan, one-line report)."""
+        q = _L.Plan()
+        rep = ct.create_string_buffer(256)
+        _L.check(self.lib.cansfz_autotune(self.h, cache_file.encode() if cache_file else None, ct.byref(q), rep, 256),
+                 "cansfz_autotune")
+        return q, rep.value.decode()
+
     def grid(self):
         nz = self.n[2]
         arrs = [np.zeros(nz + 2) for _ in range(6)]

@@ -31,6 +31,12 @@ class Diag(ct.Structure):
                 ("status", ct.c_int32), ("reserved", ct.c_int32 * 7)]
 
 
+class Plan(ct.Structure):
+    """cansfz_plan: the launch shapes the autotuner chooses."""
+    _fields_ = [("phase_slots", ct.c_int32), ("momentum_slots", ct.c_int32), ("zsolve", ct.c_int32),
+                ("fp32_transforms", ct.c_int32), ("ms_per_step", D), ("reserved", ct.c_int32 * 6)]
+
+
 SIGNATURES = {
     "cansfz_version": (I, []),
     "cansfz_status_string": (ct.c_char_p, [I]),
@@ -82,6 +88,9 @@ SIGNATURES = {
     "cansfz_solver_refined": (I, [V, V, V, I]),
     "cansfz_poisson_residual": (I, [V, V, V, V]),
     "cansfz_xform_matrix": (I, [I, I, I, PD]),
+    "cansfz_get_plan": (I, [V, ct.POINTER(Plan)]),
+    "cansfz_set_plan": (I, [V, ct.POINTER(Plan)]),
+    "cansfz_autotune": (I, [V, ct.c_char_p, ct.POINTER(Plan), ct.c_char_p, I]),
     "cansfz_ensemble_create": (I, [V, I, V, V]),
     "cansfz_ensemble_step": (I, [V, I, V]),
     "cansfz_ensemble_destroy": (I, [V]),

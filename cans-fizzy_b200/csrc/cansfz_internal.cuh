@@ -155,6 +155,9 @@ struct PoissonPlan {
   // split-BF16 matrices [0] forward, [1] backward; null: the FFT kernels
   const uint16_t* gx[2];
   const uint16_t* gy[2];
+  // z solve of grids with many columns: 0 the partitioned tile solve where
+  // it applies, 1 one column per thread (cansfz_plan.zsolve)
+  int zmode;
 };
 
 // ---------------------------------------------------------------------------
@@ -169,6 +172,10 @@ struct Launch {
   int batched;
   // set: launches are recorded for a batched replay instead of issued
   Recorder* rec = nullptr;
+  // tunable launch shapes (cansfz_plan): blocks per SM that the z split of
+  // the phase-field tiles (ACDI/THINC, Youngs) and of the momentum tile aim at
+  int phase_slots = 24;
+  int mom_slots = 48;
 };
 
 // the surface-tension histories surf?_n, surf?_o of the balanced capillary
@@ -313,6 +320,7 @@ void poisson_set_attributes();
 double xform_coef(int kind, int dir, int n, int j, int k);
 std::vector<uint16_t> xform_bmat(int kind, int dir, int n);
 bool xform_gemm_length(int n);
+bool z_part_ok(const Geo& g, const PoissonPlan& pl);
 int xform_gemm_set_attributes();
 void launch_xform_gemm(const Launch& L, const Geo& g, int mode, bool add, const uint16_t* bmat, int n,
                        const void* src, void* dst, double normfft, DevScalars* sc);

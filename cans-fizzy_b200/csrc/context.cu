@@ -116,6 +116,8 @@ struct cansfz_ctx {
   DevScalars* sc_call = nullptr;  // scalars of a per-procedure call (device)
   DevScalars* sc_host = nullptr;  // pinned mirror
   bool first_rk_call = true, first_rk2fl_call = true, first_rkscal_call = true;
+  // the tensor-core transform matrices while a plan selects the FFTs
+  const uint16_t* gsave[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool prepared = false;
@@ -1917,4 +1919,184 @@ int cansfz_poisson_residual(cansfz_ctx* c, const double* rhs, double* p, double*
   CK(cudaGetLastError());
   return CANSFZ_OK;
 }
+// ---------------------------------------------------------------------------
+// launch plans and the autotuner (no reference counterpart)
+// ---------------------------------------------------------------------------
+static void drop_graphs(cansfz_ctx* c) {
+  for (auto& ge : c->gexec)
+    if (ge) {
+      cudaGraphExecDestroy(ge);
+      ge = nullptr;
+    }
+}
+
+int cansfz_get_plan(cansfz_ctx* c, cansfz_plan* plan) {
+  if (!c || !plan) return CANSFZ_ERR_ARG;
+  std::memset(plan, 0, sizeof(*plan));
+  plan->phase_slots = c->L.phase_slots;
+  plan->momentum_slots = c->L.mom_slots;
+  plan->zsolve = c->pl.zmode;
+  plan->fp32_transforms = c->P.fp32_transforms;
+  return CANSFZ_OK;
+}
+
+int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
+  if (!c || !plan) return CANSFZ_ERR_ARG;
+  if (plan->phase_slots < 1 || plan->phase_slots > 1024 || plan->momentum_slots < 1 ||
+      plan->momentum_slots > 1024 || plan->zsolve < 0 || plan->zsolve > 1 || plan->fp32_transforms < 0 ||
+      plan->fp32_transforms > 1)
+    return CANSFZ_ERR_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  c->L.phase_slots = plan->phase_slots;
+  c->L.mom_slots = plan->momentum_slots;
+  c->pl.zmode = plan->zsolve;
+  if (plan->fp32_transforms != c->P.fp32_transforms) {
+    if (plan->fp32_transforms == 1) {
+      for (int d = 0; d < 2; ++d) {
+        c->gsave[0][d] = c->pl.gx[d];
+        c->gsave[1][d] = c->pl.gy[d];
+        c->pl.gx[d] = c->pl.gy[d] = nullptr;
+      }
+      c->P.fp32_transforms = 1;
+    } else {
+      c->P.fp32_transforms = 0;
+      if (c->gsave[0][0] || c->gsave[1][0]) {
+        for (int d = 0; d < 2; ++d) {
+          c->pl.gx[d] = c->gsave[0][d];
+          c->pl.gy[d] = c->gsave[1][d];
+        }
+      } else if (c->pl.workf) {
+        if (int rc = alloc_xform_gemm(c)) return rc;
+      }
+    }
+  }
+  drop_graphs(c);
+  return CANSFZ_OK;
+}
+
+namespace {
+std::string plan_key(const cansfz_ctx* c) {
+  cudaDeviceProp prop{};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaGetDeviceProperties(&prop, dev);
+  std::string name(prop.name);
+  for (auto& ch : name)
+    if (ch == ' ') ch = '_';
+  char buf[256];
+  std::snprintf(buf, sizeof buf, "grid=%dx%dx%d form=%d sweeps=%d vof=%d scalar=%d balanced=%d gpu=%s", c->n[0],
+                c->n[1], c->n[2], c->P.form, c->mixed ? c->sweeps : -1, c->P.interface_capturing, c->P.scalar,
+                c->P.balanced, name.c_str());
+  return buf;
+}
+
+// device time per step of `k` with `pl`, after two steps that capture the
+// graphs; a huge value when the copy's run stops
+double time_plan(cansfz_ctx* k, const cansfz_plan& pl, int nsteps) {
+  if (cansfz_set_plan(k, &pl) != CANSFZ_OK) return 1e30;
+  if (cansfz_step(k, 2) != CANSFZ_OK) return 1e30;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, k->st);
+  const int rc = cansfz_step(k, nsteps);
+  cudaEventRecord(e1, k->st);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc == CANSFZ_OK ? (double)ms / nsteps : 1e30;
+}
+}  // namespace
+
+int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, char* report, int cap) {
+  if (!c) return CANSFZ_ERR_ARG;
+  const std::string key = plan_key(c);
+  cansfz_plan best{};
+  cansfz_get_plan(c, &best);
+  // a cached choice
+  if (cache_file) {
+    if (FILE* f = std::fopen(cache_file, "r")) {
+      char line[512];
+      bool found = false;
+      while (std::fgets(line, sizeof line, f)) {
+        const std::string ln(line);
+        if (ln.compare(0, key.size(), key) != 0 || ln.size() <= key.size() || ln[key.size()] != ' ') continue;
+        cansfz_plan q = best;
+        double ms = 0.;
+        if (std::sscanf(ln.c_str() + key.size(), " | phase=%d mom=%d z=%d xf=%d ms=%lf", &q.phase_slots,
+                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &ms) == 5) {
+          q.ms_per_step = ms;
+          best = q;
+          found = true;
+        }
+      }
+      std::fclose(f);
+      if (found) {
+        if (int rc = cansfz_set_plan(c, &best)) return rc;
+        if (chosen) *chosen = best;
+        if (report && cap > 0)
+          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d ms=%.4f", best.phase_slots,
+                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+        return CANSFZ_OK;
+      }
+    }
+  }
+  // a copy of the case to time on (from the case's current fields)
+  if (!c->prepared) {
+    if (int rc = cansfz_prepare(c)) return rc;
+  }
+  cansfz_ctx* k = nullptr;
+  int rc = cansfz_create(&c->P, c->st, &k);
+  if (rc) return rc;
+  const int a = c->cur;
+  rc = cansfz_set_fields(k, c->u[a], c->v[a], c->w[a], c->p[a], c->psi[a], 1);
+  if (!rc && c->P.scalar) rc = cansfz_set_scalar(k, c->s[a], 1);
+  if (!rc) rc = cansfz_prepare(k);
+  if (rc) {
+    cansfz_destroy(k);
+    return rc;
+  }
+  const double cells = (double)c->n[0] * c->n[1] * c->n[2];
+  const int nt = cells >= 8e6 ? 4 : (cells >= 1e6 ? 8 : 20);
+  int evals = 0;
+  double tbest = time_plan(k, best, nt);
+  ++evals;
+  auto try_knob = [&](int cansfz_plan::*knob, std::initializer_list<int> vals) {
+    const int keep = best.*knob;
+    for (int v : vals) {
+      if (v == keep) continue;
+      cansfz_plan q = best;
+      q.*knob = v;
+      const double t = time_plan(k, q, nt);
+      ++evals;
+      if (t < tbest) {
+        tbest = t;
+        best = q;
+      }
+    }
+  };
+  try_knob(&cansfz_plan::phase_slots, {12, 24, 48});
+  try_knob(&cansfz_plan::momentum_slots, {24, 48, 96});
+  if (z_part_ok(c->g, c->pl) && !c->pl.zpiv) try_knob(&cansfz_plan::zsolve, {0, 1});
+  if (c->mixed && c->sweeps >= 0 && (xform_gemm_length(c->n[0]) || xform_gemm_length(c->n[1])))
+    try_knob(&cansfz_plan::fp32_transforms, {0, 1});
+  cansfz_destroy(k);
+  best.ms_per_step = tbest;
+  if ((rc = cansfz_set_plan(c, &best))) return rc;
+  if (chosen) *chosen = best;
+  if (cache_file) {
+    if (FILE* f = std::fopen(cache_file, "a")) {
+      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d ms=%.6f\n", key.c_str(), best.phase_slots,
+                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+      std::fclose(f);
+    }
+  }
+  if (report && cap > 0)
+    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d ms=%.4f", evals, best.phase_slots,
+                  best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+  return CANSFZ_OK;
+}
+
 }  // extern "C"

@@ -357,7 +357,7 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
                         const double* s, const SurfSplit& sp, TI* duo, TI* dvo, TI* dwo, double* uo, double* vo,
                         double* wo) {
   using S = tile::Shape<TYV>;
-  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, kMomSlots);
+  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.mom_slots > 0 ? L.mom_slots : kMomSlots);
   kgo<MomentumTile<TI, TYV, OPT>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT>, tile::grid_of<TYV>(g, kz),
                                        dim3(S::TX, S::TY), mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
                                        fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo);

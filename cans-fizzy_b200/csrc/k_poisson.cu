@@ -951,7 +951,7 @@ struct ZSolvePart {
   }
 };
 template <typename T, int CH>
-__global__ void __launch_bounds__(256, 2) k_zsolve_part(int ncol, int nz, const double* __restrict__ lam,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zsolve_part(int ncol, int nz, const double* __restrict__ lam,
     const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
     const DevScalars* __restrict__ sc, T* __restrict__ work, int zsing) {
   ZSolvePart<T, CH>::run(blk_here(), ncol, nz, lam, a, b, c, sc, work, zsing);
@@ -1099,6 +1099,9 @@ template <typename T, int CH>
 static void set_attr_zpart() {
   cudaFuncSetAttribute(k_zsolve_part<T, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)zpart_smem<T>(CH * ZP_P));
+  // all of the unified L1/shared storage as shared memory: 2 FP64 or 4 FP32
+  // tiles per SM
+  cudaFuncSetAttribute(k_zsolve_part<T, CH>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 void poisson_set_attributes() {
@@ -1193,13 +1196,13 @@ void launch_z_factors(const Launch& L, const Geo& g, const PoissonPlan& pl, bool
 template <typename T, int CH>
 static void z_part_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
-  kgo<ZSolvePart<T, CH>, 256, 2>(Lc, k_zsolve_part<T, CH>, ncol / ZP_NC, 32 * ZP_P, zpart_smem<T>(g.nz), ncol,
+  kgo<ZSolvePart<T, CH>, 256, sizeof(T) == 4 ? 4 : 2>(Lc, k_zsolve_part<T, CH>, ncol / ZP_NC, 32 * ZP_P, zpart_smem<T>(g.nz), ncol,
                                  g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl), pl.zsing);
 }
 
 // the partitioned solve serves non-periodic z with nz = 8 * CH and whole
 // tiles of columns; few-column grids keep the factored solve
-static bool z_part_ok(const Geo& g, const PoissonPlan& pl) {
+bool z_part_ok(const Geo& g, const PoissonPlan& pl) {
   const int ncol = g.nx * g.ny;
   if (pl.zper || ncol % ZP_NC != 0 || g.nz % ZP_P != 0) return false;
   switch (g.nz / ZP_P) {
@@ -1215,7 +1218,7 @@ template <typename T>
 static void z_pass(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc) {
   const int ncol = g.nx * g.ny;
   const int tb = 64;
-  if (!(zpiv<T>(pl) && zdf<T>(pl)) && z_part_ok(g, pl)) {
+  if (pl.zmode != 1 && !(zpiv<T>(pl) && zdf<T>(pl)) && z_part_ok(g, pl)) {
     switch (g.nz / ZP_P) {
 #define X(C) case C: z_part_len<T, C>(Lc, g, pl, sc); return;
       CANSFZ_FOR_ZCHUNKS(X)

@@ -372,7 +372,7 @@ template <typename TI, int TYV>
 static void youngs_go(const Launch& L, const Geo& g, const DevScalars* sc, const TI* phi, TI* nx, TI* ny, TI* nz,
                       TI* kappa) {
   using S = tile::Shape<TYV>;
-  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm);
+  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.phase_slots > 0 ? L.phase_slots : 24);
   kgo<YoungsTile<TI, TYV>, S::NT, 3>(L, k_youngs_tile<TI, TYV>, tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), 0, g,
                                      sc, kz, phi, nx, ny, nz, kappa);
 }
@@ -389,7 +389,7 @@ static void acdi_go(const Launch& L, const Geo& g, const DevScalars* sc, const d
                     const double* w, const TI* nx, const TI* ny, const TI* nz, const TI* phi, const double* psi,
                     double* psi_out, TI* hist, TI* fx, TI* fy, TI* fz) {
   using S = tile::Shape<TYV>;
-  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm);
+  const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.phase_slots > 0 ? L.phase_slots : 24);
   kgo<AcdiTile<TI, SDF, UPD, TYV>, S::TX * (S::TY + 1), 3>(L, k_acdi_tile<TI, SDF, UPD, TYV>,
                                              tile::grid_of<TYV>(g, kz),
                                              dim3(S::TX, S::TY + 1), acdi_smem<TI, SDF, TYV>(), g, sc, kz, u, v, w, nx,

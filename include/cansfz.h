@@ -326,6 +326,33 @@ int cansfz_poisson_residual(cansfz_ctx* ctx, const double* rhs, double* p, doubl
  * REDFT01, RODFT10, RODFT01); dir > 0 forward, dir < 0 backward.          */
 int cansfz_xform_matrix(int kind, int dir, int n, double* F);
 
+/* ---- launch plans and the autotuner (no reference counterpart) ----------
+ * The launch shapes that suit a grid and a GPU, chosen by measurement.    */
+typedef struct cansfz_plan {
+  int32_t phase_slots;      /* blocks per SM that the z split of the ACDI/THINC
+                               and Youngs tiles aims at (default 24)          */
+  int32_t momentum_slots;   /* the same for the momentum tile (default 48)   */
+  int32_t zsolve;           /* Poisson z solve of grids with >= 32768 columns:
+                               0 the partitioned 32-column tiles where nz is
+                               8 x (8, 12, 16, 24 or 32), 1 one column per
+                               thread                                         */
+  int32_t fp32_transforms;  /* mixed form's FP32 solve: 0 tensor-core GEMMs
+                               where the line lengths allow, 1 FFTs           */
+  double  ms_per_step;      /* step time measured with the plan by
+                               cansfz_autotune (0: not measured)              */
+  int32_t reserved[6];
+} cansfz_plan;
+int cansfz_get_plan(cansfz_ctx* ctx, cansfz_plan* plan);
+/* Takes effect at the next step (the step graphs are captured again).    */
+int cansfz_set_plan(cansfz_ctx* ctx, const cansfz_plan* plan);
+/* Time candidate plans on a copy of the case (same parameters, the case's
+ * current fields; the case itself does not advance) by a coordinate search
+ * over the four knobs, and apply the fastest.  cache_file (NULL: none): a
+ * text file with one line per key (grid, form, refinement sweeps, options,
+ * GPU name); a key found there is applied without timing, a new one is
+ * appended.  report (NULL or cap bytes): a one-line account of the choice. */
+int cansfz_autotune(cansfz_ctx* ctx, const char* cache_file, cansfz_plan* chosen, char* report, int cap);
+
 /* ---- batched ensemble (no reference counterpart: the reference runs one
  * case per program) -----------------------------------------------------
  * Groups independent, prepared contexts (any grid sizes and parameters, all

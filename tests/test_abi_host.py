@@ -46,7 +46,7 @@ def _c_layout(tmp_path, struct, fields):
 
 
 def test_params_layout_matches_c(tmp_path):
-    for cls, struct in ((params.Params, "cansfz_params"), (lib.Diag, "cansfz_diag")):
+    for cls, struct in ((params.Params, "cansfz_params"), (lib.Diag, "cansfz_diag"), (lib.Plan, "cansfz_plan")):
         names = [f[0] for f in cls._fields_]
         got = _c_layout(tmp_path, struct, names)
         assert got[0] == ct.sizeof(cls), struct
