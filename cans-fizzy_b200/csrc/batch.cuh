@@ -121,6 +121,7 @@ int batch_launch(const RecEntry& e, int n, const void* tab, cudaStream_t st) {
 template <class F, int NT, int MINB, class K, class... V>
 inline void kgo(const Launch& L, K k, dim3 grid, dim3 block, size_t smem, V&&... v) {
   using P = typename RunArgs<decltype(&F::run)>::type;
+  static_assert(alignof(P) <= 128, "argument tables align their entries to at most 128 bytes");
   if (L.rec) {
     P p;
     fill_pack(p, std::forward<V>(v)...);

@@ -176,6 +176,9 @@ struct Launch {
   // the phase-field tiles (ACDI/THINC, Youngs) and of the momentum tile aim at
   int phase_slots = 24;
   int mom_slots = 48;
+  // 1: the momentum tile stages its FP64 planes by TMA (tensor maps built
+  // per launch), 0: by element-wise cp.async (cansfz_plan.tma)
+  int tma = 1;
 };
 
 // the surface-tension histories surf?_n, surf?_o of the balanced capillary

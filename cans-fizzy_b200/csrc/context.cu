@@ -1159,7 +1159,8 @@ int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
       e->ngroups = (int)groups.size();
       e->grouped = 0;
       // argument tables: per group and launch, the cases' argument lists in
-      // case order, 16-byte aligned, in one device buffer
+      // case order, in one device buffer; each table starts on a 128-byte
+      // boundary (argument lists that hold tensor maps need 64)
       std::vector<std::vector<size_t>> off(groups.size());
       size_t total = 0;
       for (size_t gi = 0; gi < groups.size(); ++gi) {
@@ -1169,7 +1170,7 @@ int cansfz_ensemble_step(cansfz_ensemble* e, int nsteps, int* status_out) {
         for (const RecEntry& en : rec[gr[0]].e) {
           if (en.prepare(en)) return CANSFZ_ERR_CUDA;
           off[gi].push_back(total);
-          total += (gr.size() * en.args.size() + 15) / 16 * 16;
+          total += (gr.size() * en.args.size() + 127) / 128 * 128;
         }
       }
       if (e->argtab[par]) {
@@ -1937,6 +1938,7 @@ int cansfz_get_plan(cansfz_ctx* c, cansfz_plan* plan) {
   plan->momentum_slots = c->L.mom_slots;
   plan->zsolve = c->pl.zmode;
   plan->fp32_transforms = c->P.fp32_transforms;
+  plan->tile_tma = c->L.tma;
   return CANSFZ_OK;
 }
 
@@ -1944,9 +1946,10 @@ int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
   if (!c || !plan) return CANSFZ_ERR_ARG;
   if (plan->phase_slots < 1 || plan->phase_slots > 1024 || plan->momentum_slots < 1 ||
       plan->momentum_slots > 1024 || plan->zsolve < 0 || plan->zsolve > 1 || plan->fp32_transforms < 0 ||
-      plan->fp32_transforms > 1)
+      plan->fp32_transforms > 1 || plan->tile_tma < 0 || plan->tile_tma > 1)
     return CANSFZ_ERR_ARG;
   CK(cudaStreamSynchronize(c->st));
+  c->L.tma = plan->tile_tma;
   c->L.phase_slots = plan->phase_slots;
   c->L.mom_slots = plan->momentum_slots;
   c->pl.zmode = plan->zsolve;
@@ -2025,8 +2028,8 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         if (ln.compare(0, key.size(), key) != 0 || ln.size() <= key.size() || ln[key.size()] != ' ') continue;
         cansfz_plan q = best;
         double ms = 0.;
-        if (std::sscanf(ln.c_str() + key.size(), " | phase=%d mom=%d z=%d xf=%d ms=%lf", &q.phase_slots,
-                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &ms) == 5) {
+        if (std::sscanf(ln.c_str() + key.size(), " | phase=%d mom=%d z=%d xf=%d tma=%d ms=%lf", &q.phase_slots,
+                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &q.tile_tma, &ms) == 6) {
           q.ms_per_step = ms;
           best = q;
           found = true;
@@ -2037,8 +2040,8 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         if (int rc = cansfz_set_plan(c, &best)) return rc;
         if (chosen) *chosen = best;
         if (report && cap > 0)
-          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d ms=%.4f", best.phase_slots,
-                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d tma=%d ms=%.4f", best.phase_slots,
+                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ms_per_step);
         return CANSFZ_OK;
       }
     }
@@ -2079,6 +2082,7 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   };
   try_knob(&cansfz_plan::phase_slots, {12, 24, 48});
   try_knob(&cansfz_plan::momentum_slots, {24, 48, 96});
+  if (c->P.form == CANSFZ_FORM_FP64) try_knob(&cansfz_plan::tile_tma, {1, 0});
   if (z_part_ok(c->g, c->pl) && !c->pl.zpiv) try_knob(&cansfz_plan::zsolve, {0, 1});
   if (c->mixed && c->sweeps >= 0 && (xform_gemm_length(c->n[0]) || xform_gemm_length(c->n[1])))
     try_knob(&cansfz_plan::fp32_transforms, {0, 1});
@@ -2088,14 +2092,15 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   if (chosen) *chosen = best;
   if (cache_file) {
     if (FILE* f = std::fopen(cache_file, "a")) {
-      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d ms=%.6f\n", key.c_str(), best.phase_slots,
-                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d tma=%d ms=%.6f\n", key.c_str(), best.phase_slots,
+                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ms_per_step);
       std::fclose(f);
     }
   }
   if (report && cap > 0)
-    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d ms=%.4f", evals, best.phase_slots,
-                  best.momentum_slots, best.zsolve, best.fp32_transforms, best.ms_per_step);
+    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d tma=%d ms=%.4f", evals,
+                  best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
+                  best.ms_per_step);
   return CANSFZ_OK;
 }
 

@@ -2,8 +2,11 @@
 // in one pass per step, with its compile-time variants (Boussinesq buoyancy,
 // balanced capillary split).  It shares the tile helpers of k_tiles.cuh with
 // the phase-field tiles of k_tiles.cu.
+#include <cstring>
+
 #include "batch.cuh"
 #include "k_tiles.cuh"
+#include "tma.cuh"
 
 namespace cansfz {
 
@@ -38,12 +41,19 @@ namespace cansfz {
 // from the extrapolated one, and the new force goes to the history slot.
 // ---------------------------------------------------------------------------
 namespace {
+// the plane slot pitch: for the FP64 drop-in the ring slots start on 128-byte
+// boundaries, where the TMA plane copies land
+template <typename TI, int TYV>
+constexpr int mom_pitch() {
+  using SH = tile::Shape<TYV>;
+  return sizeof(TI) == 8 ? (SH::PXY + 15) / 16 * 16 : SH::PXY;
+}
 template <typename TI, int TYV>
 constexpr size_t mom_smem() {
   using namespace tile;
   using SH = Shape<TYV>;
-  constexpr int PXY = SH::PXY, NSLOT = SH::NSLOT;
-  return (size_t)NSLOT * PXY * (4 * sizeof(double) + 3 * sizeof(TI));
+  constexpr int SP = mom_pitch<TI, TYV>(), NSLOT = SH::NSLOT;
+  return (size_t)NSLOT * SP * (4 * sizeof(double) + 3 * sizeof(TI)) + NSLOT * sizeof(uint64_t);
 }
 }  // namespace
 
@@ -60,29 +70,59 @@ struct MomentumTile {
       const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
       const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s,
       const SurfSplit& sp, TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-      double* __restrict__ vo, double* __restrict__ wo) {
+      double* __restrict__ vo, double* __restrict__ wo, const HaloMaps& maps, int use_tma) {
     constexpr bool BUOY = (OPT & kMomBuoy) != 0, BAL = (OPT & kMomBal) != 0;
     using namespace tile;
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
+    constexpr int SP = mom_pitch<TI, TYV>();
+    // TMA plane copies for the FP64 drop-in's seven staged fields; the
+    // element copies otherwise (and for the FP32 fluxes of the mixed form)
+    // (a tensor map must sit on a 64-byte boundary; a misplaced one falls back)
+    const bool tmaon = sizeof(TI) == 8 && use_tma != 0 && (reinterpret_cast<uintptr_t>(&maps) & 63) == 0;
     (void)TY;
     typedef double T;  // the RHS in FP64 for both storage types
-    extern __shared__ __align__(16) unsigned char smem[];
-    double* s_u = reinterpret_cast<double*>(smem);  // each [NSLOT][PXY]
-    double* s_v = s_u + NSLOT * PXY;
-    double* s_w = s_v + NSLOT * PXY;
-    double* s_c = s_w + NSLOT * PXY;
-    TI* s_fx = reinterpret_cast<TI*>(s_c + NSLOT * PXY);
-    TI* s_fy = s_fx + NSLOT * PXY;
-    TI* s_fz = s_fy + NSLOT * PXY;
+    extern __shared__ __align__(128) unsigned char smem[];
+    double* s_u = reinterpret_cast<double*>(smem);  // each [NSLOT][SP]
+    double* s_v = s_u + NSLOT * SP;
+    double* s_w = s_v + NSLOT * SP;
+    double* s_c = s_w + NSLOT * SP;
+    TI* s_fx = reinterpret_cast<TI*>(s_c + NSLOT * SP);
+    TI* s_fy = s_fx + NSLOT * SP;
+    TI* s_fz = s_fy + NSLOT * SP;
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_fz + NSLOT * SP);  // [NSLOT]
     if (HALTED(sc)) return;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
     const int i0 = bk.x * TX + 1, j0 = bk.y * TY + 1;
     const int kb = bk.z * kz + 1, ke = min(kb + kz - 1, g.nz);
     const int sx = g.sx, sxy = g.sxy;
+    if (tmaon) {
+      if (tid == 0) {
+        for (int q = 0; q < NSLOT; ++q) tma::bar_init(s_bar + q, 1);
+        tma::bar_init_fence();
+      }
+      __syncthreads();
+    }
+    // plane kk lives in ring slot (kk - kb) % NSLOT; its TMA fill is that
+    // slot's ((kk - kb) / NSLOT)-th, which fixes the mbarrier phase
+    auto slot = [&](int kk) { return (kk - kb) % NSLOT; };
+    auto phase = [&](int kk) { return (uint32_t)(((kk - kb) / NSLOT) & 1); };
 
+    int issued = kb - 1;  // the last plane whose copies were issued
     auto issue = [&](int kk) {
-      const int o = (kk % NSLOT) * PXY;
+      const int o = slot(kk) * SP;
+      if (tmaon) {
+        issued = kk;
+        if (tid == 0) {
+          uint64_t* bar = s_bar + slot(kk);
+          tma::bar_expect_tx(bar, 7u * PXY * 8u);
+          double* dst[7] = {s_u + o, s_v + o, s_w + o, s_c + o, reinterpret_cast<double*>(s_fx + o),
+                            reinterpret_cast<double*>(s_fy + o), reinterpret_cast<double*>(s_fz + o)};
+#pragma unroll
+          for (int f = 0; f < 7; ++f) tma::load_3d(dst[f], &maps.m[f], i0 - 1, j0 - 1, kk, bar);
+        }
+        return;
+      }
       for (int q = tid; q < PXY; q += NT) {
         int h;
         const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
@@ -135,13 +175,20 @@ struct MomentumTile {
 
     issue(kb);
     issue(kb + 1);
+    bool fail = false;
     for (int k = kb; k <= ke; ++k) {
       if (k + 2 <= ke + 1) issue(k + 2);
-      else cp_commit();
-      cp_wait<1>();
-      __syncthreads();  // planes k and k+1 are in; every thread is done with level k-1
-      if (act) {
-        const int o0 = (k % NSLOT) * PXY + qc, o1 = ((k + 1) % NSLOT) * PXY + qc;
+      else if (!tmaon) cp_commit();
+      if (tmaon) {
+        // planes k and k+1 are in (each thread waits for the copies itself)
+        if (!tma::bar_wait(s_bar + slot(k), phase(k)) || !tma::bar_wait(s_bar + slot(k + 1), phase(k + 1)))
+          fail = true;
+      } else {
+        cp_wait<1>();
+        __syncthreads();  // planes k and k+1 are in; every thread is done with level k-1
+      }
+      if (act && !fail) {
+        const int o0 = slot(k) * SP + qc, o1 = slot(k + 1) * SP + qc;
 #define PU(s, a, b) ((T)s_u[o##s + (a) + PX * (b)])
 #define PV(s, a, b) ((T)s_v[o##s + (a) + PX * (b)])
 #define PW(s, a, b) ((T)s_w[o##s + (a) + PX * (b)])
@@ -329,7 +376,16 @@ struct MomentumTile {
 #undef FLZ
         p_c = p_z; po_c = po_z; pso_c = pso_z; k_c = k_z;
       }
-      __syncthreads();  // plane k's slot is refilled at the next level
+      // plane k's slot is refilled at the next level; a plane copy that
+      // never completed stops the block
+      if (__syncthreads_or(fail)) break;
+    }
+    if (fail && tid == 0) {
+      // the copies still in flight land before the block exits
+      for (int kk = max(kb, issued - NSLOT + 1); kk <= issued; ++kk) tma::bar_wait(s_bar + slot(kk), phase(kk));
+      DevScalars* scw = const_cast<DevScalars*>(sc);
+      atomicCAS(&scw->status, CANSFZ_OK, CANSFZ_ERR_TIMEOUT);
+      scw->halted = 1;
     }
     (void)sxy;
   }
@@ -341,11 +397,46 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 512 / tile::Shape<TYV>::
     const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
     const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s, const SurfSplit sp,
     TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-    double* __restrict__ vo, double* __restrict__ wo) {
+    double* __restrict__ vo, double* __restrict__ wo, const __grid_constant__ HaloMaps maps, int use_tma) {
   MomentumTile<TI, TYV, OPT>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, sp, duo,
-      dvo, dwo, uo, vo, wo);
+      dvo, dwo, uo, vo, wo, maps, use_tma);
 }
 
+
+// ---------------------------------------------------------------------------
+// tensor maps of halo-layout fields (cuTensorMapEncodeTiled through the
+// runtime's driver entry point, so the library needs no libcuda link)
+// ---------------------------------------------------------------------------
+namespace {
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(f);
+  }
+  return fn;
+}
+}  // namespace
+
+bool make_halo_map(CUtensorMap* m, const void* base, const Geo& g, int bx, int by) {
+  EncodeTiled fn = encode_fn();
+  if (!fn || !base || ((uintptr_t)base & 15) || (g.sx * 8) % 16 || (bx * 8) % 16) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.sx, (cuuint64_t)(g.ny + 2), (cuuint64_t)(g.nz + 2)};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.sx * 8, (cuuint64_t)g.sxy * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // ---------------------------------------------------------------------------
 // launchers
@@ -358,9 +449,19 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
                         double* wo) {
   using S = tile::Shape<TYV>;
   const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.mom_slots > 0 ? L.mom_slots : kMomSlots);
+  // the staged fields' tensor maps (FP64 drop-in only)
+  HaloMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  int use_tma = 0;
+  if (sizeof(TI) == 8 && L.tma) {
+    const void* f[7] = {u, v, w, psi, fx, fy, fz};
+    use_tma = 1;
+    for (int q = 0; q < 7; ++q)
+      if (!make_halo_map(&maps.m[q], f[q], g, S::PX, S::TY + 2)) use_tma = 0;
+  }
   kgo<MomentumTile<TI, TYV, OPT>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT>, tile::grid_of<TYV>(g, kz),
                                        dim3(S::TX, S::TY), mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
-                                       fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo);
+                                       fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, use_tma);
 }
 
 template <typename TI, int TYV>

@@ -248,13 +248,20 @@ def _check_step(g, o, tol=1e-11):
     return errs
 
 
-def _oracle_sensitivity(p, u, v, w, pr, psi, nsteps, names=("u", "v", "w")):
+def _oracle_sensitivity(p, u, v, w, pr, psi, nsteps, names=("u", "v", "w"), mode="scale"):
     """The reference algorithm's own round-off sensitivity: the oracle rerun
-    with psi scaled by (1 - 1e-15); the largest relative change of a field."""
+    with psi scaled by (1 - 1e-15) (mode "scale"), or moved by one ulp up or
+    down at random in every cell (mode "ulp", seeded); the largest relative
+    change of a field."""
+    if mode == "ulp":
+        sgn = np.random.default_rng(0).choice([-1.0, 1.0], size=psi.shape)
+        pert = np.clip(np.where(sgn > 0, np.nextafter(psi, 2.0), np.nextafter(psi, -1.0)), 0.0, 1.0)
+    else:
+        pert = psi * (1.0 - 1e-15)
     runs = []
-    for scale in (1.0, 1.0 - 1e-15):
+    for ps in (psi, np.asfortranarray(pert)):
         o = O.Case(p)
-        for name, a in zip(("u", "v", "w", "p", "psi"), (u, v, w, pr, psi * scale)):
+        for name, a in zip(("u", "v", "w", "p", "psi"), (u, v, w, pr, ps)):
             o.set(name, a)
         o.prepare()
         assert o.step(nsteps) == 0

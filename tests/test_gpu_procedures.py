@@ -21,7 +21,7 @@ import oracle as O
 from cansfz import case as C
 from cansfz import init, namelist, params
 
-from test_gpu_parity import _check_step, _nml, _rand_fields, _rel, _run_pair
+from test_gpu_parity import _check_step, _nml, _oracle_sensitivity, _rand_fields, _rel, _run_pair
 
 pytestmark = pytest.mark.gpu
 
@@ -157,16 +157,30 @@ def test_updt_rhs_b_nonzero_dirichlet():
 
 def test_step_dirichlet_pressure():
     """10 steps with a non-zero Dirichlet pressure BC in x: the step's
-    fillps + updt_rhs_b + unfused solve path."""
+    fillps + updt_rhs_b + unfused solve path.  After one step the GPU
+    matches the oracle to 1e-12.  Over ten steps the case amplifies
+    round-off in the reference algorithm itself: far from the bubble psi
+    lies within ~1e-12 of 1, where the SDF phi = eps*log((psi+e)/(1-psi+e))
+    turns a one-ulp change of psi into a ~1e-4 change of phi, and through
+    the normals and curvature into the velocity; moving psi by one ulp at
+    random changes the oracle's own u, v, w by ~1e-6 after 10 steps (the
+    GPU's FMA-rounded transport differs from the oracle by one ulp in some
+    cells).  The bar is 1e-11 or four times that self-sensitivity."""
     p = params.from_namelist(namelist.parse(_DIRICHLET))
     psi = init.init2fl(p, "bub3", np.array([[0.5, 0.375, 0.5, 0.2]]))
     u, v, w, pr = init.initflow(p, "zer")
+    g1, o1, rg, ro = _run_pair(p, u, v, w, pr, psi, 1)
+    assert rg == 0 and ro == 0
+    for nm in ("u", "v", "w", "p", "psi"):
+        assert _rel(g1.get(nm), o1.get(nm)) < 1e-12, nm
     g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
     assert rg == 0 and ro == 0
+    sens = _oracle_sensitivity(p, u, v, w, pr, psi, 10, names=("u", "v", "w", "p"), mode="ulp")
+    tol = max(1e-11, 4.0 * sens)
+    errs = _check_step(g, o, tol=tol)
     # the Dirichlet BC fixes the pressure level: compare p itself as well
-    errs = _check_step(g, o)
     pa, pb = g.get("p")[1:-1, 1:-1, 1:-1], o.get("p")[1:-1, 1:-1, 1:-1]
-    assert _rel(pa, pb) < 1e-11, errs
+    assert _rel(pa, pb) < tol, (errs, sens)
 
 
 def test_step_gravity_along_periodic_x():
