@@ -196,3 +196,55 @@ def test_step_gravity_along_periodic_x():
     g, o, rg, ro = _run_pair(p, u, v, w, np.zeros_like(u), psi, 10)
     assert rg == 0 and ro == 0
     _check_step(g, o)
+
+
+_WALLS = """
+&dns
+ng(1:3) = 20, 18, 16
+l(1:3) = 1., 0.9, 0.8
+gtype = 1, gr = 1.2
+cbcvel(0:1,1:3,1) = 'D','D', 'D','N', 'D','D'
+cbcvel(0:1,1:3,2) = 'N','D', 'D','D', 'N','D'
+cbcvel(0:1,1:3,3) = 'D','N', 'N','D', 'D','D'
+bcvel(0:1,1:3,1)  = 0.3, -0.2, 0.1, 0.05, 0., 0.7
+bcvel(0:1,1:3,2)  = 0.2, 0.4, -0.1, 0.3, 0.6, -0.5
+bcvel(0:1,1:3,3)  = 0.1, 0.25, 0.35, -0.45, 0.15, 0.
+cbcpre(0:1,1:3)   = 'N','N', 'D','D', 'N','N'
+bcpre(0:1,1:3)    = 0.5, -0.25, 1.5, -0.5, 0.75, 0.
+/
+&two_fluid
+cbcpsi(0:1,1:3)   = 'N','D', 'D','N', 'N','N'
+bcpsi(0:1,1:3)    = 0.1, 0.9, 0.2, 0.3, 0.4, 0.5
+cbcnor(0:1,1:3,1) = 'D','D', 'N','N', 'N','N'
+cbcnor(0:1,1:3,2) = 'N','N', 'D','D', 'N','N'
+cbcnor(0:1,1:3,3) = 'N','N', 'N','N', 'D','D'
+rho12(1:2) = 1000., 100.
+mu12(1:2) = 10., 1.
+/
+"""
+
+
+@pytest.mark.parametrize("text", [_DIRICHLET, _WALLS], ids=["x-walls", "all-walls"])
+def test_boundary_fills_with_walls(text):
+    """boundp for every field kind and bounduvw (after momentum and after
+    correc) against the oracle, bit for bit, with walls in x (and y, z),
+    centered and non-centered Dirichlet and Neumann faces with non-zero
+    values, and periodic y: every ghost cell's value depends on the order of
+    the fills (src/bound.f90:15-124), which the one-launch fill composes."""
+    p = params.from_namelist(namelist.parse(text))
+    g, o = C.Case(p), O.Case(p)
+    rng = np.random.default_rng(31)
+    shp = tuple(x + 2 for x in p.n)
+    for which in range(6):
+        a = np.asfortranarray(rng.standard_normal(shp))
+        ag = g.field(a)
+        g.call("boundp", which, ag)
+        o.call("boundp", which, a)
+        assert np.array_equal(ag.get(), a), which
+    for is_correc in (0, 1):
+        fs = [np.asfortranarray(rng.standard_normal(shp)) for _ in range(3)]
+        gs = [g.field(a) for a in fs]
+        g.call("bounduvw", is_correc, *gs)
+        o.call("bounduvw", is_correc, *fs)
+        for q, (a, b) in enumerate(zip(gs, fs)):
+            assert np.array_equal(a.get(), b), (is_correc, q)
