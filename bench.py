@@ -156,6 +156,8 @@ def plan_dict(q, report):
     return {"phase_slots": q.phase_slots, "momentum_slots": q.momentum_slots,
             "zsolve": "partitioned tiles" if q.zsolve == 0 else "one column per thread",
             "fp32_transforms": "tcgen05 GEMM" if q.fp32_transforms == 0 else "FFT",
+            "tile_staging": "TMA" if q.tile_tma else "cp.async",
+            "ghost_images": "written by the producing kernels" if q.ghost_images else "fill stages",
             "tuned_ms_per_step": q.ms_per_step, "report": report}
 
 

@@ -39,6 +39,43 @@ struct Geo {
   __host__ __device__ inline int tsize() const { return nx * ny * nz; }
 };
 
+// Periodic ghost images written by the kernel that produces a field.  A
+// periodic ghost fill copies a(n) into a(0) and a(1) into a(n+1) along each
+// periodic direction (src/bound.f90:126-293 for x, updthalo for y and z);
+// the kernel that computes interior point (i,j,k) can store the same value
+// into those images itself, edges and corners included (every combination
+// of the directions in which the point is a first or last interior one).
+// wrap: bit d set when direction d is periodic and the images along it are
+// to be written (never for n = 1, where both images come from one point).
+// The ghost fill that follows then skips those directions: the values match
+// the reference's fill order, because its later stages (the non-periodic
+// faces) read the same images.
+#ifdef __CUDACC__
+// the image offsets of (i,j,k) along x, y and z (0: none)
+__device__ __forceinline__ int wrap_ox(const Geo& g, int wrap, int i) {
+  return (wrap & 1) ? (i == 1 ? g.nx : (i == g.nx ? -g.nx : 0)) : 0;
+}
+__device__ __forceinline__ int wrap_oy(const Geo& g, int wrap, int j) {
+  return (wrap & 2) ? (j == 1 ? g.ny * g.sx : (j == g.ny ? -g.ny * g.sx : 0)) : 0;
+}
+__device__ __forceinline__ int wrap_oz(const Geo& g, int wrap, int k) {
+  return (wrap & 4) ? (k == 1 ? g.nz * g.sxy : (k == g.nz ? -g.nz * g.sxy : 0)) : 0;
+}
+// st(h) for every image c + (a combination of the non-zero offsets)
+template <typename F>
+__device__ __forceinline__ void store_images(int c, int ox, int oy, int oz, F st) {
+  const int m = (ox != 0 ? 1 : 0) | (oy != 0 ? 2 : 0) | (oz != 0 ? 4 : 0);
+  if (m == 0) return;
+#pragma unroll 1
+  for (int s = m; s != 0; s = (s - 1) & m)  // every non-empty combination of the image directions
+    st(c + ((s & 1) ? ox : 0) + ((s & 2) ? oy : 0) + ((s & 4) ? oz : 0));
+}
+template <typename F>
+__device__ __forceinline__ void store_wraps(const Geo& g, int wrap, int i, int j, int k, F st) {
+  store_images(g.h(i, j, k), wrap_ox(g, wrap, i), wrap_oy(g, wrap, j), wrap_oz(g, wrap, k), st);
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // per-step scalars kept on the device so a whole step is graph-capturable.
 // Names follow program cans (src/main.f90:414-562).
@@ -106,6 +143,7 @@ struct BcField {
   int f32;
   BcFace face[3][2];     // [idir][ibound]
   int halo_periodic[3];  // y/z periodic self-exchange (updthalo)
+  int wrapped;           // directions (bit d) whose periodic images the producing kernel wrote (store_wraps)
 };
 #define BC_MAXF 6
 struct BcGroup {
@@ -179,6 +217,9 @@ struct Launch {
   // 1: the momentum tile stages its FP64 planes by TMA (tensor maps built
   // per launch), 0: by element-wise cp.async (cansfz_plan.tma)
   int tma = 1;
+  // periodic images that the producing kernels of the whole step write
+  // (store_wraps); 0 for the per-procedure entries
+  int wrap = 0;
 };
 
 // the surface-tension histories surf?_n, surf?_o of the balanced capillary

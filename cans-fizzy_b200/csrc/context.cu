@@ -80,6 +80,11 @@ struct cansfz_ctx {
   double* d_grid = nullptr;  // dzc,dzf,dzci,dzfi,gvr_c,gvr_f on the device
   int is_bound[3][2]{};
   int halo_periodic[3]{};
+  // directions whose periodic ghost images the step's producing kernels write
+  // themselves (store_wraps), so that the ghost fills after them skip those
+  // copies: bit d when every field is periodic along d and n_d >= 2
+  int wrap = 0;
+  int images = 1;  // launch plan: 1 the producers write those images (cansfz_plan.ghost_images)
   char cbccur[3][2]{};
   double bccur[3][2]{};
   double seps = 0., beta = 1.;
@@ -217,26 +222,29 @@ void scalar_bc_spec(const cansfz_ctx* c, int which, const char (**cbc)[2], const
   else if (which == 6) { *cbc = P.cbcsca; *bc = P.bcsca; }
 }
 
-void run_bc(cansfz_ctx* c, std::initializer_list<BcField> fields, const DevScalars* sc) {
+// wrapped: the periodic images the producing kernel already wrote (BcField::wrapped)
+void run_bc(cansfz_ctx* c, std::initializer_list<BcField> fields, const DevScalars* sc, int wrapped = 0) {
   BcGroup grp{};
   for (const BcField& f : fields) {
     if (grp.nf == BC_MAXF) { launch_bc_group(c->L, c->g, grp, sc); grp.nf = 0; }
-    grp.f[grp.nf++] = f;
+    grp.f[grp.nf] = f;
+    grp.f[grp.nf++].wrapped = wrapped;
   }
   launch_bc_group(c->L, c->g, grp, sc);
 }
 
-void run_bcp(cansfz_ctx* c, int which, double* p, const DevScalars* sc) {
+void run_bcp(cansfz_ctx* c, int which, double* p, const DevScalars* sc, int wrapped = 0) {
   const char(*cbc)[2];
   const double(*bc)[2];
   scalar_bc_spec(c, which, &cbc, &bc);
-  run_bc(c, {bc_scalar(c, cbc, bc, p)}, sc);
+  run_bc(c, {bc_scalar(c, cbc, bc, p)}, sc, wrapped);
 }
 
-void run_bcuvw(cansfz_ctx* c, bool is_correc, double* u, double* v, double* w, const DevScalars* sc) {
+void run_bcuvw(cansfz_ctx* c, bool is_correc, double* u, double* v, double* w, const DevScalars* sc,
+               int wrapped = 0) {
   BcField F[3];
   bc_vel(c, is_correc, u, v, w, F);
-  run_bc(c, {F[0], F[1], F[2]}, sc);
+  run_bc(c, {F[0], F[1], F[2]}, sc, wrapped);
 }
 
 // ---------------------------------------------------------------------------
@@ -531,16 +539,20 @@ __global__ void k_prescribed_vel(Geo g, const DevScalars* __restrict__ sc, int w
   p[c] = 0.;
 }
 
-// phi, Youngs normals and curvature and their ghost fills in FP32 (mixed form)
-void normals_f32(cansfz_ctx* c, const double* psi, const DevScalars* sc, const StageMark* mk = nullptr) {
+// phi, Youngs normals and curvature and their ghost fills in FP32 (mixed
+// form); wrap: the periodic images the Youngs tile writes itself
+void normals_f32(cansfz_ctx* c, const double* psi, const DevScalars* sc, const StageMark* mk = nullptr,
+                 int wrap = 0) {
   const cansfz_params& P = c->P;
+  Launch Lw = c->L;
+  Lw.wrap = wrap;
   launch_cmpt_phi_f32(c->L, c->g, sc, c->ph.acdi != 0, psi, c->phif, c->ph.sdf == 0);
   if (mk) mk->mark("cmpt_phi");
-  launch_youngs_t<float>(c->L, c->g, sc, c->phif, c->nxf, c->nyf, c->nzf, c->kappaf);
+  launch_youngs_t<float>(Lw, c->g, sc, c->phif, c->nxf, c->nyf, c->nzf, c->kappaf);
   if (mk) mk->mark("youngs");
   run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappaf), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nxf),
              bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->nyf), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nzf)},
-         sc);
+         sc, wrap);
   if (mk) mk->mark("bc_normals");
 }
 
@@ -554,13 +566,18 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
   const Geo& g = c->g;
   const int a = c->cur, b = a ^ 1;
   DevScalars* sc = c->sc;
+  // the producing kernels below also write the periodic ghost images
+  // (c->wrap), and the ghost fills after them skip those copies
+  const int wr = c->images ? c->wrap : 0;
+  Launch Lw = L;
+  Lw.wrap = wr;
   launch_step_begin(L, sc, P.icheck);
   MARK("step_begin");
   // phase field: rk_2fl + boundary fills + phi + normals/curvature
   if (P.is_track_interface && c->mixed) {
     const bool sdf = c->ph.sdf != 0;
     if (c->ph.acdi)
-      launch_acdi_t<float>(L, g, sc, sdf, true, c->u[a], c->v[a], c->w[a], c->nxf, c->nyf, c->nzf, c->phif,
+      launch_acdi_t<float>(Lw, g, sc, sdf, true, c->u[a], c->v[a], c->w[a], c->nxf, c->nyf, c->nzf, c->phif,
                            c->psi[a], c->psi[b], c->hpsif, c->fxf, c->fyf, c->fzf);
     else
       launch_thinc_step_t<float>(L, g, sc, sdf, c->u[a], c->v[a], c->w[a], c->nxf, c->nyf, c->nzf, c->phif,
@@ -568,12 +585,12 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     MARK("phase_transport");
     BcField F[3];
     bc_vel(c, false, c->fxf, c->fyf, c->fzf, F);
-    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc);
+    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc, c->ph.acdi ? wr : 0);
     MARK("bc_phase");
-    normals_f32(c, c->psi[b], sc, mk);
+    normals_f32(c, c->psi[b], sc, mk, wr);
   } else if (P.is_track_interface) {
     if (c->ph.acdi)
-      launch_acdi_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
+      launch_acdi_step(Lw, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
                        c->psi[a], c->psi[b], c->hpsi, c->fx, c->fy, c->fz);
     else
       launch_thinc_step(L, g, sc, c->ph.sdf != 0, c->u[a], c->v[a], c->w[a], c->nx, c->ny, c->nz, c->phi,
@@ -581,15 +598,15 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
     MARK("phase_transport");
     BcField F[3];
     bc_vel(c, false, c->fx, c->fy, c->fz, F);
-    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc);
+    run_bc(c, {F[0], F[1], F[2], bc_scalar(c, P.cbcpsi, P.bcpsi, c->psi[b])}, sc, c->ph.acdi ? wr : 0);
     MARK("bc_phase");
     if (c->ph.sdf) launch_cmpt_phi(L, g, sc, c->ph.acdi != 0, c->psi[b], c->phi);
     MARK("cmpt_phi");
-    launch_youngs(L, g, sc, c->ph.sdf ? c->phi : c->psi[b], c->nx, c->ny, c->nz, c->kappa);
+    launch_youngs(Lw, g, sc, c->ph.sdf ? c->phi : c->psi[b], c->nx, c->ny, c->nz, c->kappa);
     MARK("youngs");
     run_bc(c, {bc_scalar(c, c->cbccur, c->bccur, c->kappa), bc_scalar(c, P.cbcnor[0], P.bcnor[0], c->nx),
                bc_scalar(c, P.cbcnor[1], P.bcnor[1], c->ny), bc_scalar(c, P.cbcnor[2], P.bcnor[2], c->nz)},
-           sc);
+           sc, wr);
     MARK("bc_normals");
   } else {
     launch_copy(L, (size_t)g.hsize(), c->psi[a], c->psi[b]);
@@ -636,15 +653,15 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
       for (int d = 0; d < 3; ++d) { split.n[d] = c->surf[a][d]; split.o[d] = c->surf[b][d]; split.out_n[d] = c->surf[b][d]; }
     const SurfSplit* sp = c->ph.balanced ? &split : nullptr;
     if (c->mixed)
-      launch_momentum_t<float>(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fxf, c->fyf,
+      launch_momentum_t<float>(Lw, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fxf, c->fyf,
                                c->fzf, c->p[a], c->p[b], c->kappaf, sb, sp, c->huf, c->hvf, c->hwf, c->u[b], c->v[b],
                                c->w[b]);
     else
-      launch_momentum_fused(L, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy,
+      launch_momentum_fused(Lw, g, c->ph, sc, c->u[a], c->v[a], c->w[a], c->psi[b], c->psi[a], c->fx, c->fy,
                             c->fz, c->p[a], c->p[b], c->kappa, sb, sp, c->hu, c->hv, c->hw, c->u[b], c->v[b],
                             c->w[b]);
     MARK("momentum");
-    run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc);
+    run_bcuvw(c, false, c->u[b], c->v[b], c->w[b], sc, wr);
     MARK("bc_uvw");
     // fillps + updt_rhs_b + solver
     if (c->mixed && c->sweeps >= 0) {
@@ -659,17 +676,18 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
         launch_poisson_f32(L, g, c->pl, sc, c->res64, c->phip, true, mk);
       }
     } else if (c->rhsb_zero) {
-      launch_poisson_fused_rhs(L, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip, mk);
+      launch_poisson_fused_rhs(Lw, g, c->pl, c->ph, sc, c->u[b], c->v[b], c->w[b], nullptr, c->phip, mk);
     } else {
       launch_fillps(L, g, c->ph, sc, c->u[b], c->v[b], c->w[b], c->phip);
       launch_updt_rhs_b(L, g, c->is_bound, c->rhsbx, c->rhsby, c->rhsbz, c->phip);
-      launch_poisson(L, g, c->pl, sc, c->phip, mk);
+      launch_poisson(Lw, g, c->pl, sc, c->phip, mk);
     }
-    run_bcp(c, 0, c->phip, sc);
+    // the FP64 solve's inverse x pass wrote the periodic images
+    run_bcp(c, 0, c->phip, sc, (c->mixed && c->sweeps >= 0) ? 0 : wr);
     MARK("bc_pcorr");
     // correc, and updatep (p_new = phi + p into the po slot, then po <- p by
     // the parity flip), in one pass over phi
-    launch_correc_updatep(L, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b], c->p[a], c->p[b]);
+    launch_correc_updatep(Lw, g, c->ph, sc, c->phip, c->u[b], c->v[b], c->w[b], c->p[a], c->p[b]);
     MARK("correc_updatep");
     {
       // bounduvw after correc and boundp of the new pressure: independent
@@ -679,7 +697,7 @@ void enqueue_step(cansfz_ctx* c, const StageMark* mk = nullptr) {
       const char(*cbc)[2];
       const double(*bcv)[2];
       scalar_bc_spec(c, 0, &cbc, &bcv);
-      run_bc(c, {F[0], F[1], F[2], bc_scalar(c, cbc, bcv, c->p[b])}, sc);
+      run_bc(c, {F[0], F[1], F[2], bc_scalar(c, cbc, bcv, c->p[b])}, sc, wr);
     }
     MARK("bc_uvw_p");
   }
@@ -807,6 +825,12 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   }
   for (int d = 0; d < 3; ++d)
     for (int ib = 0; ib < 2; ++ib) { c->cbccur[d][ib] = P.cbcpsi[d][ib]; c->bccur[d][ib] = P.bcpre[d][ib]; }
+  {
+    bool xp = is_pp(P.cbcpre[0]) && is_pp(P.cbcpsi[0]) && (!P.scalar || is_pp(P.cbcsca[0]));
+    for (int q = 0; q < 3; ++q) xp = xp && is_pp(P.cbcvel[q][0]) && is_pp(P.cbcnor[q][0]);
+    c->wrap = (xp && nx >= 2 ? 1 : 0) | (c->halo_periodic[1] && ny >= 2 ? 2 : 0) |
+              (c->halo_periodic[2] && nz >= 2 ? 4 : 0);
+  }
   // physics constants (src/param.f90:170-178)
   Phys& ph = c->ph;
   for (int q = 0; q < 2; ++q) { ph.rho12[q] = P.rho12[q]; ph.mu12[q] = P.mu12[q]; }
@@ -1939,6 +1963,7 @@ int cansfz_get_plan(cansfz_ctx* c, cansfz_plan* plan) {
   plan->zsolve = c->pl.zmode;
   plan->fp32_transforms = c->P.fp32_transforms;
   plan->tile_tma = c->L.tma;
+  plan->ghost_images = c->images;
   return CANSFZ_OK;
 }
 
@@ -1946,10 +1971,12 @@ int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
   if (!c || !plan) return CANSFZ_ERR_ARG;
   if (plan->phase_slots < 1 || plan->phase_slots > 1024 || plan->momentum_slots < 1 ||
       plan->momentum_slots > 1024 || plan->zsolve < 0 || plan->zsolve > 1 || plan->fp32_transforms < 0 ||
-      plan->fp32_transforms > 1 || plan->tile_tma < 0 || plan->tile_tma > 1)
+      plan->fp32_transforms > 1 || plan->tile_tma < 0 || plan->tile_tma > 1 || plan->ghost_images < 0 ||
+      plan->ghost_images > 1)
     return CANSFZ_ERR_ARG;
   CK(cudaStreamSynchronize(c->st));
   c->L.tma = plan->tile_tma;
+  c->images = plan->ghost_images;
   c->L.phase_slots = plan->phase_slots;
   c->L.mom_slots = plan->momentum_slots;
   c->pl.zmode = plan->zsolve;
@@ -2028,8 +2055,11 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         if (ln.compare(0, key.size(), key) != 0 || ln.size() <= key.size() || ln[key.size()] != ' ') continue;
         cansfz_plan q = best;
         double ms = 0.;
-        if (std::sscanf(ln.c_str() + key.size(), " | phase=%d mom=%d z=%d xf=%d tma=%d ms=%lf", &q.phase_slots,
-                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &q.tile_tma, &ms) == 6) {
+        const char* rest = ln.c_str() + key.size();
+        if (std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%lf", &q.phase_slots,
+                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &q.tile_tma, &q.ghost_images, &ms) == 7 ||
+            std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d ms=%lf", &q.phase_slots, &q.momentum_slots,
+                        &q.zsolve, &q.fp32_transforms, &q.tile_tma, &ms) == 6) {
           q.ms_per_step = ms;
           best = q;
           found = true;
@@ -2040,8 +2070,9 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         if (int rc = cansfz_set_plan(c, &best)) return rc;
         if (chosen) *chosen = best;
         if (report && cap > 0)
-          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d tma=%d ms=%.4f", best.phase_slots,
-                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ms_per_step);
+          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.4f", best.phase_slots,
+                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ghost_images,
+                        best.ms_per_step);
         return CANSFZ_OK;
       }
     }
@@ -2083,6 +2114,7 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   try_knob(&cansfz_plan::phase_slots, {12, 24, 48});
   try_knob(&cansfz_plan::momentum_slots, {24, 48, 96});
   if (c->P.form == CANSFZ_FORM_FP64) try_knob(&cansfz_plan::tile_tma, {1, 0});
+  if (c->wrap) try_knob(&cansfz_plan::ghost_images, {1, 0});
   if (z_part_ok(c->g, c->pl) && !c->pl.zpiv) try_knob(&cansfz_plan::zsolve, {0, 1});
   if (c->mixed && c->sweeps >= 0 && (xform_gemm_length(c->n[0]) || xform_gemm_length(c->n[1])))
     try_knob(&cansfz_plan::fp32_transforms, {0, 1});
@@ -2092,15 +2124,16 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   if (chosen) *chosen = best;
   if (cache_file) {
     if (FILE* f = std::fopen(cache_file, "a")) {
-      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d tma=%d ms=%.6f\n", key.c_str(), best.phase_slots,
-                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ms_per_step);
+      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.6f\n", key.c_str(), best.phase_slots,
+                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ghost_images,
+                   best.ms_per_step);
       std::fclose(f);
     }
   }
   if (report && cap > 0)
-    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d tma=%d ms=%.4f", evals,
+    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.4f", evals,
                   best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
-                  best.ms_per_step);
+                  best.ghost_images, best.ms_per_step);
   return CANSFZ_OK;
 }
 

@@ -6,7 +6,10 @@
 //   4. set_bc on the z faces when z is not periodic
 // Each stage is one launch over every field of a BcGroup; within a stage a
 // thread owns one point of the face plane and applies face 0 then face 1,
-// exactly as set_bc (src/bound.f90:126-293) writes them.
+// exactly as set_bc (src/bound.f90:126-293) writes them.  A field whose
+// producing kernel already wrote its periodic images (BcField::wrapped)
+// skips the periodic copies of those directions; the stages of its
+// non-periodic faces run as before and read those images.
 #include "batch.cuh"
 
 namespace cansfz {
@@ -41,7 +44,7 @@ template <int STAGE, typename E>
 __device__ __forceinline__ void bc_stage_point(const Geo& g, const BcField& F, E* __restrict__ p, int q) {
   const int NX = g.nx + 2, NY = g.ny + 2, NZ = g.nz + 2;
   if (STAGE == ST_PER) {
-    const bool py = F.halo_periodic[1], pz = F.halo_periodic[2];
+    const bool py = F.halo_periodic[1] && !(F.wrapped & 2), pz = F.halo_periodic[2] && !(F.wrapped & 4);
     const int nyp = py ? 2 * NX * NZ : 0, nzp = pz ? 2 * NX * NY : 0;
     int i, j, k;
     if (q < nyp) {
@@ -57,7 +60,7 @@ __device__ __forceinline__ void bc_stage_point(const Geo& g, const BcField& F, E
     if (pz) { if (k == 0) ks = g.nz; else if (k == g.nz + 1) ks = 1; }
     p[g.h(i, j, k)] = p[g.h(i, js, ks)];
   } else if (STAGE == ST_X) {
-    if (q >= NY * NZ) return;
+    if (q >= NY * NZ || (F.wrapped & 1)) return;
     const int j = q % NY, k = q / NY;
     const int base = g.sx * j + g.sxy * k;
     auto at = [=](int m) { return base + m; };
@@ -103,8 +106,8 @@ void launch_bc_group(const Launch& L, const Geo& g, const BcGroup& grp, const De
   bool any_per = false, any_x = false, any_y = false, any_z = false;
   for (int f = 0; f < grp.nf; ++f) {
     const BcField& F = grp.f[f];
-    any_per |= F.halo_periodic[1] || F.halo_periodic[2];
-    any_x |= F.face[0][0].type != BC_NONE || F.face[0][1].type != BC_NONE;
+    any_per |= (F.halo_periodic[1] && !(F.wrapped & 2)) || (F.halo_periodic[2] && !(F.wrapped & 4));
+    any_x |= (F.face[0][0].type != BC_NONE || F.face[0][1].type != BC_NONE) && !(F.wrapped & 1);
     any_y |= F.face[1][0].type != BC_NONE || F.face[1][1].type != BC_NONE;
     any_z |= F.face[2][0].type != BC_NONE || F.face[2][1].type != BC_NONE;
   }

@@ -70,7 +70,7 @@ struct MomentumTile {
       const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
       const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s,
       const SurfSplit& sp, TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-      double* __restrict__ vo, double* __restrict__ wo, const HaloMaps& maps, int use_tma) {
+      double* __restrict__ vo, double* __restrict__ wo, const HaloMaps& maps, int use_tma, int wrap) {
     constexpr bool BUOY = (OPT & kMomBuoy) != 0, BAL = (OPT & kMomBal) != 0;
     using namespace tile;
     using SH = Shape<TYV>;
@@ -360,9 +360,17 @@ struct MomentumTile {
           sdv = sdv - ph.gacc[1] * factoryp * 0.5 * (s_y + s_c);
           sdw = sdw - ph.gacc[2] * factorzp * 0.5 * (s_z + s_c);
         }
-        uo[c] = un + f12 * sdu * irx;
-        vo[c] = vn + f12 * sdv * iry;
-        wo[c] = wn + f12 * sdw * irz;
+        {
+          const double ua = un + f12 * sdu * irx, va = vn + f12 * sdv * iry, wa = wn + f12 * sdw * irz;
+          uo[c] = ua;
+          vo[c] = va;
+          wo[c] = wa;
+          store_wraps(g, wrap, i, j, k, [&](int h) {
+            uo[h] = ua;
+            vo[h] = va;
+            wo[h] = wa;
+          });
+        }
         // carry upwards
         u_ccm = PU(0, 0, 0); v_ccm = PV(0, 0, 0); w_ccm = PW(0, 0, 0); w_pcm = PW(0, 1, 0); w_cpm = PW(0, 0, 1);
         c_ccm = PC(0, 0, 0); c_pcm = PC(0, 1, 0); c_cpm = PC(0, 0, 1);
@@ -397,9 +405,9 @@ __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 512 / tile::Shape<TYV>::
     const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
     const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s, const SurfSplit sp,
     TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-    double* __restrict__ vo, double* __restrict__ wo, const __grid_constant__ HaloMaps maps, int use_tma) {
+    double* __restrict__ vo, double* __restrict__ wo, const __grid_constant__ HaloMaps maps, int use_tma, int wrap) {
   MomentumTile<TI, TYV, OPT>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, sp, duo,
-      dvo, dwo, uo, vo, wo, maps, use_tma);
+      dvo, dwo, uo, vo, wo, maps, use_tma, wrap);
 }
 
 
@@ -461,7 +469,7 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
   }
   kgo<MomentumTile<TI, TYV, OPT>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT>, tile::grid_of<TYV>(g, kz),
                                        dim3(S::TX, S::TY), mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
-                                       fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, use_tma);
+                                       fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, use_tma, L.wrap);
 }
 
 template <typename TI, int TYV>

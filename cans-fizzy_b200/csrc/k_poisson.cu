@@ -408,11 +408,12 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, LinePlan pl, const Dev
 }
 
 // ADD: dst += normfft * x (refinement correction) instead of dst = normfft * x
+// wrap: periodic images of dst written as well (store_wraps; not with ADD)
 template <typename T, bool ADD, int MC, int LC>
 struct FftXBwd {
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
       const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
-      int Lrt) {
+      int Lrt, int wrap) {
     if (HALTED(sc)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
@@ -449,16 +450,21 @@ struct FftXBwd {
       if (gl < nlines) {
         const int j = gl % g.ny + 1, k = gl / g.ny + 1;
         const int c = g.h(i + 1, j, k);
-        if (ADD) dst[c] = dst[c] + (double)val * normfft;
-        else dst[c] = (double)val * normfft;
+        if (ADD) {
+          dst[c] = dst[c] + (double)val * normfft;
+        } else {
+          const double o = (double)val * normfft;
+          dst[c] = o;
+          store_wraps(g, wrap, i + 1, j, k, [&](int h) { dst[h] = o; });
+        }
       }
     });
   }
 };
 template <typename T, bool ADD, int MC, int LC>
 __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
-    const T* __restrict__ work, double normfft, double* __restrict__ dst, int Lrt) {
-  FftXBwd<T, ADD, MC, LC>::run(blk_here(), g, pl, sc, work, normfft, dst, Lrt);
+    const T* __restrict__ work, double normfft, double* __restrict__ dst, int Lrt, int wrap) {
+  FftXBwd<T, ADD, MC, LC>::run(blk_here(), g, pl, sc, work, normfft, dst, Lrt, wrap);
 }
 
 // ---------------------------------------------------------------------------
@@ -1253,7 +1259,8 @@ static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
   kgo<FftXBwd<T, ADD, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_bwd<T, ADD, MC, xL<T, MC>()>, (nlines + L - 1) / L, 256,
-                                                smem, g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L);
+                                                smem, g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L,
+                                                ADD ? 0 : Lc.wrap);
 }
 
 template <typename T, bool ADD>

@@ -763,6 +763,17 @@ void launch_correc(const Launch& L, const Geo& g, const Phys& ph, const DevScala
 // step in one pass: both read the correction phi, and updatep needs none of
 // the velocity ghost fills that follow correc.  32x8 point tiles of the halo
 // array; pout = phi + pp on the interior (the new pressure into the po slot).
+//
+// wrap (bit d: direction d periodic, its images written here).  correc
+// already updates the whole halo range but u at i = nx+1, v at j = ny+1 and
+// w at k = nz+1, and with periodic ghosts of its operands (phi, and the
+// predicted velocity, both filled before) the values it computes at a ghost
+// point equal those at the point's periodic image, operation for operation
+// (w at k = 0 takes dzci(nz), the metric of its image).
+// So the periodic fill after correc only has to supply those three planes:
+// the thread of u(1), v(1) or w(1) stores its value there (no thread reads
+// them here).  pout is also evaluated at the ghost points of the wrapped
+// directions, from the periodic ghosts of phi and pp.
 constexpr int kCorrecLevels = 2;  // z levels per thread of k_correc_updatep
 struct CorrecUpdatep {
   // each thread owns one (i, j) column and kCorrecLevels consecutive levels:
@@ -770,7 +781,8 @@ struct CorrecUpdatep {
   // updates, so that a warp has many independent loads in flight
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
       const DevScalars* __restrict__ sc, const double* __restrict__ p, double* __restrict__ u,
-      double* __restrict__ v, double* __restrict__ w, const double* __restrict__ pp, double* __restrict__ pout) {
+      double* __restrict__ v, double* __restrict__ w, const double* __restrict__ pp, double* __restrict__ pout,
+      int wrap) {
     constexpr int KC = kCorrecLevels;
     if (HALTED(sc)) return;
     const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k0 = bk.z * KC;
@@ -778,6 +790,9 @@ struct CorrecUpdatep {
     const double dt = sc->dt, rhop = ph.rho0;
     const int c0 = g.h(i, j, k0);
     const bool xin = i <= g.nx, yin = j <= g.ny, ij_int = i >= 1 && xin && j >= 1 && yin;
+    // pout at (i,j): interior, or a ghost of a wrapped direction
+    const bool ij_p = (((wrap & 1) != 0) || (i >= 1 && xin)) && (((wrap & 2) != 0) || (j >= 1 && yin));
+    auto k_p = [&](int k) { return ((wrap & 4) != 0) || (k >= 1 && k <= g.nz); };
     double pc[KC + 1], px[KC], py[KC], uo[KC], vo[KC], wo[KC], pq[KC];
 #pragma unroll
     for (int q = 0; q < KC; ++q) {
@@ -789,7 +804,7 @@ struct CorrecUpdatep {
         uo[q] = xin ? u[c] : 0.;
         vo[q] = yin ? v[c] : 0.;
         wo[q] = k <= g.nz ? w[c] : 0.;
-        pq[q] = (ij_int && k >= 1 && k <= g.nz) ? LD(pp, c) : 0.;
+        pq[q] = (ij_p && k_p(k)) ? LD(pp, c) : 0.;
       }
     }
     pc[KC] = (k0 + KC - 1 <= g.nz) ? LD(p, c0 + KC * g.sxy) : 0.;
@@ -797,23 +812,39 @@ struct CorrecUpdatep {
     for (int q = 0; q < KC; ++q) {
       const int k = k0 + q, c = c0 + q * g.sxy;
       if (k > g.nz + 1) break;
-      if (xin) u[c] = uo[q] - dt * g.dxi * (px[q] - pc[q]) / rhop;
-      if (yin) v[c] = vo[q] - dt * g.dyi * (py[q] - pc[q]) / rhop;
-      if (k <= g.nz) w[c] = wo[q] - dt * g.dzci[k] * (pc[q + 1] - pc[q]) / rhop;
-      if (ij_int && k >= 1 && k <= g.nz) pout[c] = pc[q] + pq[q];
+      if (xin) {
+        const double un = uo[q] - dt * g.dxi * (px[q] - pc[q]) / rhop;
+        u[c] = un;
+        if ((wrap & 1) && i == 1) u[c + g.nx] = un;
+      }
+      if (yin) {
+        const double vn = vo[q] - dt * g.dyi * (py[q] - pc[q]) / rhop;
+        v[c] = vn;
+        if ((wrap & 2) && j == 1) v[c + g.ny * g.sx] = vn;
+      }
+      if (k <= g.nz) {
+        // with periodic z, w(0) is w(nz)'s image: the same operands, and
+        // dzci(nz), which may differ from dzci(0) in its last bits
+        const double dzk = ((wrap & 4) && k == 0) ? g.dzci[g.nz] : g.dzci[k];
+        const double wn = wo[q] - dt * dzk * (pc[q + 1] - pc[q]) / rhop;
+        w[c] = wn;
+        if ((wrap & 4) && k == 1) w[c + g.nz * g.sxy] = wn;
+      }
+      if (ij_p && k_p(k)) pout[c] = pc[q] + pq[q];
     }
   }
 };
 __global__ void __launch_bounds__(256) k_correc_updatep(Geo g, Phys ph, const DevScalars* __restrict__ sc,
                                                         const double* __restrict__ p, double* __restrict__ u,
                                                         double* __restrict__ v, double* __restrict__ w,
-                                                        const double* __restrict__ pp, double* __restrict__ pout) {
-  CorrecUpdatep::run(blk_here(), g, ph, sc, p, u, v, w, pp, pout);
+                                                        const double* __restrict__ pp, double* __restrict__ pout,
+                                                        int wrap) {
+  CorrecUpdatep::run(blk_here(), g, ph, sc, p, u, v, w, pp, pout, wrap);
 }
 void launch_correc_updatep(const Launch& L, const Geo& g, const Phys& ph, const DevScalars* sc, const double* p,
                            double* u, double* v, double* w, const double* pp, double* pout) {
   const dim3 b(32, 8), gr((g.nx + 2 + 31) / 32, (g.ny + 2 + 7) / 8, (g.nz + 2 + kCorrecLevels - 1) / kCorrecLevels);
-  kgo<CorrecUpdatep, 256, 1>(L, k_correc_updatep, gr, b, 0, g, ph, sc, p, u, v, w, pp, pout);
+  kgo<CorrecUpdatep, 256, 1>(L, k_correc_updatep, gr, b, 0, g, ph, sc, p, u, v, w, pp, pout, L.wrap);
 }
 
 // updatep, src/updatep.f90:13-24
@@ -922,6 +953,12 @@ __device__ __forceinline__ double block_sum(double v) {
   if (wid == 0) v = warp_sum(v);
   return v;
 }
+// |u_c|^2 of acdi_set_gamma (src/acdi.f90:52-55): (uc^2 + vc^2) + wc^2,
+// rounded at each operation as the reference evaluates it (no contraction
+// into FMAs), the same bits in every kernel that forms it
+__device__ __forceinline__ double vel2(double uc, double vc, double wc) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(uc, uc), __dmul_rn(vc, vc)), __dmul_rn(wc, wc));
+}
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, double v) {
   atomicMax(slot, (unsigned long long)__double_as_longlong(v));
 }
@@ -938,7 +975,7 @@ __global__ void k_gamma_max(Geo g, DevScalars* __restrict__ sc, double* __restri
     const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
     const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
     const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
-    vel = uc * uc + vc * vc + wc * wc;
+    vel = vel2(uc, vc, wc);
   }
   vel = block_max(vel);
   if (threadIdx.x == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = vel;
@@ -1159,7 +1196,7 @@ struct StepReduce {
             const double uc = 0.5 * (u0[q] + u1[q]);
             const double vc = 0.5 * (v0[q] + v1[q]);
             const double wc = 0.5 * (w0[q] + w1[q]);
-            velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+            velmax = fmax(velmax, vel2(uc, vc, wc));
           }
         }
       }
@@ -1172,7 +1209,7 @@ struct StepReduce {
             const double uc = 0.5 * (LD(u, c) + LD(u, c - 1));
             const double vc = 0.5 * (LD(v, c) + LD(v, c - g.sx));
             const double wc = 0.5 * (LD(w, c) + LD(w, c - g.sxy));
-            velmax = fmax(velmax, uc * uc + vc * vc + wc * wc);
+            velmax = fmax(velmax, vel2(uc, vc, wc));
           }
           dtimax = fmax(dtimax, chkdt_cell(g, i, j, k, u, v, w));
           const double div = (LD(w, c) - LD(w, c - g.sxy)) * g.dzfi[k] + (LD(v, c) - LD(v, c - g.sx)) * g.dyi +

@@ -16,7 +16,11 @@
 // reference evaluates from another cell may differ in the last bit (sums of
 // the same four terms in another order).  The vertex plane of level k+1 and
 // the cells of level k are evaluated in the same pass (three vertex planes,
-// four cell planes in the ring), so each level needs one barrier.
+// four cell planes in the ring), so each level needs one barrier.  A vertex
+// plane has (TX+1)(TY+1) vertices, TX+TY+1 more than the tile's cells; a
+// ninth warp takes those, so that per level every thread evaluates at most
+// two normalisations (one vertex and one cell, or two vertices) and no cell
+// warp waits at the barrier for a third.
 //
 // ACDI: each face flux (advective part and regularisation part) is shared by
 // the two cells on either side.  Each thread evaluates its cell's +x, +y and
@@ -50,13 +54,16 @@ template <typename TI, int TYV>
 struct YoungsTile {
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const DevScalars* __restrict__ sc, int kz,
       const TI* __restrict__ phi, TI* __restrict__ normx, TI* __restrict__ normy, TI* __restrict__ normz,
-      TI* __restrict__ kappa) {
+      TI* __restrict__ kappa, int wrap) {
     using namespace tile;
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY;
-    (void)TY;
     typedef TI T;
     constexpr int VX = TX + 1, VY = TY + 1, VXY = VX * VY;  // vertices of the tile's cells in one plane
+    // threads: TY cell rows plus the vertex warp; each thread's first vertex
+    // is its own index, and the vertex warp's lanes 0..TY take the rest
+    constexpr int NTT = NT + TX;
+    static_assert(NTT <= VXY && VXY - NTT <= TX, "one vertex per thread plus the vertex warp's second");
     // cell planes m-1 .. m+2 around the level m being gathered (m+3 in
     // flight), and three vertex planes: the two the cells of level m gather
     // from and the one evaluated for level m+1 in the same pass
@@ -73,7 +80,7 @@ struct YoungsTile {
     auto issue = [&](int kk) {
       if (kk <= ke + 1) {
         T* dst = pl[kk % NCP];
-        for (int q = tid; q < PXY; q += NT) {
+        for (int q = tid; q < PXY; q += NTT) {
           int h;
           const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
           cp_async(dst + q, phi + (ok ? h : 0), ok);
@@ -89,7 +96,7 @@ struct YoungsTile {
       T* oy = vn[(kk + NVP) % NVP][1];
       T* oz = vn[(kk + NVP) % NVP][2];
       const T d1 = (T)g.dxi, d2 = (T)g.dyi, dz = (T)g.dzci[kk];
-      for (int q = tid; q < VXY; q += NT) {
+      auto vertex = [&](int q) {
         const int a = q % VX, b = q / VX, s = a + PX * b;
         const T ccc = lo[s], pcc = lo[s + 1], cpc = lo[s + PX], ppc = lo[s + PX + 1];
         const T ccp = hi[s], pcp = hi[s + 1], cpp = hi[s + PX], ppp = hi[s + PX + 1];
@@ -100,7 +107,9 @@ struct YoungsTile {
         ox[q] = mx * inv;
         oy[q] = my * inv;
         oz[q] = mz * inv;
-      }
+      };
+      vertex(tid);  // tid < NTT <= VXY
+      if (tid >= NT && tid - NT + NTT < VXY) vertex(tid - NT + NTT);
     };
 
     issue(kb - 1);
@@ -114,8 +123,9 @@ struct YoungsTile {
     __syncthreads();  // plane kb-1's slot is refilled at the first level
 
     const int i = i0 + tx, j = j0 + ty;
-    const bool act = i <= g.nx && j <= g.ny;
+    const bool act = ty < TY && i <= g.nx && j <= g.ny;
     const T d1 = (T)g.dxi, d2 = (T)g.dyi;
+    const int wox = wrap_ox(g, wrap, i), woy = wrap_oy(g, wrap, j);  // the column's x and y images
     for (int k = kb; k <= ke; ++k) {
       // plane k+3 goes into the slot of plane k-1, last read for vertex plane
       // k-1/2 before the previous barrier
@@ -144,22 +154,30 @@ struct YoungsTile {
         const T norm_z = T(.125) * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
         const T inv = recip_rn(sqrt(sqr(norm_x) + sqr(norm_y) + sqr(norm_z)) + T(CANSFZ_EPS));
         const int c = g.h(i, j, k);
-        normx[c] = norm_x * inv;
-        normy[c] = norm_y * inv;
-        normz[c] = norm_z * inv;
-        kappa[c] = -(T(0.25) * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
-                     T(0.25) * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
-                     T(0.25) * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * (T)g.dzfi[k]);
+        const T ox = norm_x * inv, oy = norm_y * inv, oz = norm_z * inv;
+        const T kap = -(T(0.25) * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
+                        T(0.25) * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
+                        T(0.25) * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * (T)g.dzfi[k]);
+        normx[c] = ox;
+        normy[c] = oy;
+        normz[c] = oz;
+        kappa[c] = kap;
+        store_images(c, wox, woy, wrap_oz(g, wrap, k), [&](int h) {
+          normx[h] = ox;
+          normy[h] = oy;
+          normz[h] = oz;
+          kappa[h] = kap;
+        });
       }
     }
   }
 };
 template <typename TI, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::NT) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT + tile::Shape<TYV>::TX, 3) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
                                                           const TI* __restrict__ phi, TI* __restrict__ normx,
                                                           TI* __restrict__ normy, TI* __restrict__ normz,
-                                                          TI* __restrict__ kappa) {
-  YoungsTile<TI, TYV>::run(blk_here(), g, sc, kz, phi, normx, normy, normz, kappa);
+                                                          TI* __restrict__ kappa, int wrap) {
+  YoungsTile<TI, TYV>::run(blk_here(), g, sc, kz, phi, normx, normy, normz, kappa, wrap);
 }
 
 // ---------------------------------------------------------------------------
@@ -213,7 +231,7 @@ struct AcdiTile {
       const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
       const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
       const TI* __restrict__ phi, const double* __restrict__ psi, TI* __restrict__ dpsidt, TI* __restrict__ fx,
-      TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out) {
+      TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out, int wrap) {
     using namespace tile;
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
@@ -340,14 +358,23 @@ struct AcdiTile {
         const T rglr = (rgxp - rgxm) * dxi + (rgyp - rgym) * dyi + (rg_zp - rg_zm) * dzfi_c;
         const T d = -adv + rglr;
         const int c = g.h(i, j, k), t = g.t(i, j, k);
+        double pn = 0.;
         if (UPD) {
           const T dO = first2 ? d : dO_pre;
-          psi_out[c] = fmin(fmax(0., psi_c + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
+          pn = fmin(fmax(0., psi_c + sc->f1 * (double)d + sc->f2 * (double)dO), 1.);
+          psi_out[c] = pn;
         }
         dpsidt[t] = d;
-        fx[c] = upxp - rgxp;
-        fy[c] = upyp - rgyp;
-        fz[c] = up_zp - rg_zp;
+        const T ex = upxp - rgxp, ey = upyp - rgyp, ez = up_zp - rg_zp;
+        fx[c] = ex;
+        fy[c] = ey;
+        fz[c] = ez;
+        store_wraps(g, wrap, i, j, k, [&](int h) {
+          if (UPD) psi_out[h] = pn;
+          fx[h] = ex;
+          fy[h] = ey;
+          fz[h] = ez;
+        });
       }
       up_zm = up_zp;
       rg_zm = rg_zp;
@@ -356,13 +383,13 @@ struct AcdiTile {
   }
 };
 template <typename TI, bool SDF, bool UPD, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::TX * (tile::Shape<TYV>::TY + 1)) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+__global__ void __launch_bounds__(tile::Shape<TYV>::TX * (tile::Shape<TYV>::TY + 1), 3) k_acdi_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
     const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
     const TI* __restrict__ nx_, const TI* __restrict__ ny_, const TI* __restrict__ nz_,
     const TI* __restrict__ phi, const double* __restrict__ psi, TI* __restrict__ dpsidt,
-    TI* __restrict__ fx, TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out) {
+    TI* __restrict__ fx, TI* __restrict__ fy, TI* __restrict__ fz, double* __restrict__ psi_out, int wrap) {
   AcdiTile<TI, SDF, UPD, TYV>::run(blk_here(), g, sc, kz, u, v, w, nx_, ny_, nz_, phi, psi, dpsidt, fx, fy, fz,
-      psi_out);
+      psi_out, wrap);
 }
 
 // ---------------------------------------------------------------------------
@@ -373,8 +400,8 @@ static void youngs_go(const Launch& L, const Geo& g, const DevScalars* sc, const
                       TI* kappa) {
   using S = tile::Shape<TYV>;
   const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.phase_slots > 0 ? L.phase_slots : 24);
-  kgo<YoungsTile<TI, TYV>, S::NT, 3>(L, k_youngs_tile<TI, TYV>, tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), 0, g,
-                                     sc, kz, phi, nx, ny, nz, kappa);
+  kgo<YoungsTile<TI, TYV>, S::NT + S::TX, 3>(L, k_youngs_tile<TI, TYV>, tile::grid_of<TYV>(g, kz),
+                                              dim3(S::TX, S::TY + 1), 0, g, sc, kz, phi, nx, ny, nz, kappa, L.wrap);
 }
 
 template <typename TI>
@@ -393,7 +420,7 @@ static void acdi_go(const Launch& L, const Geo& g, const DevScalars* sc, const d
   kgo<AcdiTile<TI, SDF, UPD, TYV>, S::TX * (S::TY + 1), 3>(L, k_acdi_tile<TI, SDF, UPD, TYV>,
                                              tile::grid_of<TYV>(g, kz),
                                              dim3(S::TX, S::TY + 1), acdi_smem<TI, SDF, TYV>(), g, sc, kz, u, v, w, nx,
-                                             ny, nz, phi, psi, hist, fx, fy, fz, psi_out);
+                                             ny, nz, phi, psi, hist, fx, fy, fz, psi_out, L.wrap);
 }
 
 template <typename TI, int TYV>

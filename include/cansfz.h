@@ -343,14 +343,19 @@ typedef struct cansfz_plan {
   int32_t tile_tma;         /* FP64 drop-in momentum tile: 1 stages its planes
                                with TMA tensor copies (default), 0 with
                                element-wise cp.async                          */
-  int32_t reserved[5];
+  int32_t ghost_images;     /* periodic directions: 1 the kernels that produce
+                               a field in the step also write its periodic
+                               ghost images, so the ghost fills after them
+                               skip those copies (default); 0 the fills copy
+                               them.  The ghost values are the same bits     */
+  int32_t reserved[4];
 } cansfz_plan;
 int cansfz_get_plan(cansfz_ctx* ctx, cansfz_plan* plan);
 /* Takes effect at the next step (the step graphs are captured again).    */
 int cansfz_set_plan(cansfz_ctx* ctx, const cansfz_plan* plan);
 /* Time candidate plans on a copy of the case (same parameters, the case's
  * current fields; the case itself does not advance) by a coordinate search
- * over the five knobs, and apply the fastest.  cache_file (NULL: none): a
+ * over the six knobs, and apply the fastest.  cache_file (NULL: none): a
  * text file with one line per key (grid, form, refinement sweeps, options,
  * GPU name); a key found there is applied without timing, a new one is
  * appended.  report (NULL or cap bytes): a one-line account of the choice. */

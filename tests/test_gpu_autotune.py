@@ -44,6 +44,32 @@ def test_tile_splits_are_bit_equal():
         assert np.array_equal(x, y)
 
 
+_AUX = ("phi", "kappa", "normx", "normy", "normz", "psiflx_x", "psiflx_y", "psiflx_z", "pn", "po", "pcorr")
+
+
+@pytest.mark.parametrize("kind", ["walls-z", "periodic", "mixed", "thinc"])
+def test_ghost_images_are_bit_equal(kind):
+    """The producing kernels' periodic ghost images (ghost_images = 1) and
+    the fill stages (0) leave the same bits in every field, ghosts included."""
+    kw = {}
+    if kind == "mixed":
+        kw["form"] = 1
+    if kind == "thinc":
+        kw["interface_capturing"] = 1
+    if kind == "periodic":
+        kw.update(cbcvel=b"P" * 18, cbcpre=b"P" * 6, cbcpsi=b"P" * 6, cbcnor=b"P" * 18)
+    a, b = _case((64, 32, 48), **kw), _case((64, 32, 48), **kw)
+    q = b.plan()
+    assert q.ghost_images == 1
+    q.ghost_images = 0
+    b.set_plan(q)
+    assert a.step(5) == 0 and b.step(5) == 0
+    for nm, x, y in zip(("u", "v", "w", "p", "psi"), _state(a), _state(b)):
+        assert np.array_equal(x, y), nm
+    for nm in _AUX:
+        assert np.array_equal(a.get(nm), b.get(nm)), nm
+
+
 def test_zsolve_variants_agree():
     # 256 x 128 columns: the partitioned z solve applies (nz = 64 = 8 x 8)
     a, b = _case((256, 128, 64)), _case((256, 128, 64))
