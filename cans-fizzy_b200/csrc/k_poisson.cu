@@ -340,6 +340,9 @@ __device__ __forceinline__ Bufs<T> smem_bufs(T* sm, int m, int L) {
 // fillps right-hand side rho0*div(u)/dt computed on the fly in FP64
 // (src/fillps.f90:39-50).
 // ---------------------------------------------------------------------------
+// the most lines an x-transform CTA holds (lines_per_cta with x_maxL)
+constexpr int kXLinesMax = 16;
+
 template <typename T, bool FUSED, int MC, int LC>
 struct FftXFwd {
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
@@ -355,15 +358,24 @@ struct FftXFwd {
     const int l0 = bk.x * L;
     const double dti = FUSED ? sc->dti : 0.;
     const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
+    // per line: the halo index of its point i = 0 (-1 past the last line)
+    // and dti*dzfi(k), so that the per-point work needs no division by ny
+    __shared__ int lbase[kXLinesMax];
+    __shared__ double ldz[kXLinesMax];
+    if (threadIdx.x < L) {
+      const int gl = l0 + threadIdx.x, k = gl / g.ny + 1;
+      lbase[threadIdx.x] = gl < nlines ? g.h(0, gl % g.ny + 1, k) : -1;
+      ldz[threadIdx.x] = gl < nlines ? dti * g.dzfi[k] : 0.;
+    }
+    __syncthreads();
     auto get = [&](int it) -> double {
       const int line = it / n, i = it - line * n;
-      const int gl = l0 + line;
+      const int cb = lbase[line];
       double x = 0.;
-      if (gl < nlines) {
-        const int j = gl % g.ny + 1, k = gl / g.ny + 1;
-        const int c = g.h(i + 1, j, k);
+      if (cb >= 0) {
+        const int c = cb + i + 1;
         if (FUSED) {
-          x = ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * dti * g.dzfi[k] +
+          x = ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * ldz[line] +
                          (__ldg(v + c) - __ldg(v + c - g.sx)) * dtidyi + (__ldg(u + c) - __ldg(u + c - 1)) * dtidxi);
         } else {
           x = __ldg(src + c);
@@ -422,6 +434,15 @@ struct FftXBwd {
     const Bufs<T> B = smem_bufs<T>(sm, m < 1 ? 1 : m, L);
     const int nlines = g.ny * g.nz;
     const int l0 = bk.x * L;
+    // per line: the halo index of its point i = 0 (-1 past the last line)
+    // and the offsets of its y and z images
+    __shared__ int lbase[kXLinesMax], loy[kXLinesMax], loz[kXLinesMax];
+    if (threadIdx.x < L) {
+      const int gl = l0 + threadIdx.x, j = gl % g.ny + 1, k = gl / g.ny + 1;
+      lbase[threadIdx.x] = gl < nlines ? g.h(0, j, k) : -1;
+      loy[threadIdx.x] = ADD ? 0 : wrap_oy(g, wrap, j);
+      loz[threadIdx.x] = ADD ? 0 : wrap_oz(g, wrap, k);
+    }
     constexpr int NB = (LC > 0 && MC > 0) ? (LC * 2 * MC + 255) / 256 : 0;
     if (NB > 0 && NB <= 32) {
       T r[NB > 0 ? NB : 1];
@@ -446,16 +467,15 @@ struct FftXBwd {
     }
     __syncthreads();
     line_backward<T, false, MC, LC>(pl, B, L, [&](int line, int i, T val) {
-      const int gl = l0 + line;
-      if (gl < nlines) {
-        const int j = gl % g.ny + 1, k = gl / g.ny + 1;
-        const int c = g.h(i + 1, j, k);
+      const int cb = lbase[line];
+      if (cb >= 0) {
+        const int c = cb + i + 1;
         if (ADD) {
           dst[c] = dst[c] + (double)val * normfft;
         } else {
           const double o = (double)val * normfft;
           dst[c] = o;
-          store_wraps(g, wrap, i + 1, j, k, [&](int h) { dst[h] = o; });
+          store_images(c, ADD ? 0 : wrap_ox(g, wrap, i + 1), loy[line], loz[line], [&](int h) { dst[h] = o; });
         }
       }
     });
