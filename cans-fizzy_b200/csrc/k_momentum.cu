@@ -48,12 +48,19 @@ constexpr int mom_pitch() {
   using SH = tile::Shape<TYV>;
   return sizeof(TI) == 8 ? (SH::PXY + 15) / 16 * 16 : SH::PXY;
 }
-template <typename TI, int TYV>
+// STG: the FP64 drop-in's planes are staged by TMA, and then psio, p, po
+// and kappa as well, so that their +x, +y, +z neighbours come from shared
+// memory; otherwise seven fields by element copies and those four through
+// the read-only cache
+template <typename TI, int STG>
+constexpr int mom_extra() { return (STG && sizeof(TI) == 8) ? 4 : 0; }
+template <typename TI, int TYV, int STG>
 constexpr size_t mom_smem() {
   using namespace tile;
   using SH = Shape<TYV>;
   constexpr int SP = mom_pitch<TI, TYV>(), NSLOT = SH::NSLOT;
-  return (size_t)NSLOT * SP * (4 * sizeof(double) + 3 * sizeof(TI)) + NSLOT * sizeof(uint64_t);
+  return (size_t)NSLOT * SP * ((4 + mom_extra<TI, STG>()) * sizeof(double) + 3 * sizeof(TI)) +
+         NSLOT * sizeof(uint64_t);
 }
 }  // namespace
 
@@ -62,7 +69,7 @@ enum { kMomBuoy = 1, kMomBal = 2 };
 // the phase-field tiles' (0.711 -> 0.683 ms at 256^3 against 24)
 constexpr int kMomSlots = 48;
 
-template <typename TI, int TYV, int OPT>
+template <typename TI, int TYV, int OPT, int STG>
 struct MomentumTile {
   static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const Phys& ph,
       const DevScalars* __restrict__ sc, int kz, const double* __restrict__ u, const double* __restrict__ v,
@@ -70,7 +77,7 @@ struct MomentumTile {
       const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
       const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s,
       const SurfSplit& sp, TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-      double* __restrict__ vo, double* __restrict__ wo, const HaloMaps& maps, int use_tma, int wrap) {
+      double* __restrict__ vo, double* __restrict__ wo, const HaloMaps& maps, int wrap) {
     constexpr bool BUOY = (OPT & kMomBuoy) != 0, BAL = (OPT & kMomBal) != 0;
     using namespace tile;
     using SH = Shape<TYV>;
@@ -79,7 +86,7 @@ struct MomentumTile {
     // TMA plane copies for the FP64 drop-in's seven staged fields; the
     // element copies otherwise (and for the FP32 fluxes of the mixed form)
     // (a tensor map must sit on a 64-byte boundary; a misplaced one falls back)
-    const bool tmaon = sizeof(TI) == 8 && use_tma != 0 && (reinterpret_cast<uintptr_t>(&maps) & 63) == 0;
+    constexpr bool tmaon = STG != 0 && sizeof(TI) == 8;
     (void)TY;
     typedef double T;  // the RHS in FP64 for both storage types
     extern __shared__ __align__(128) unsigned char smem[];
@@ -90,8 +97,19 @@ struct MomentumTile {
     TI* s_fx = reinterpret_cast<TI*>(s_c + NSLOT * SP);
     TI* s_fy = s_fx + NSLOT * SP;
     TI* s_fz = s_fy + NSLOT * SP;
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_fz + NSLOT * SP);  // [NSLOT]
+    constexpr int NX4 = mom_extra<TI, STG>();  // staged psio, p, po, kappa (FP64 drop-in)
+    double* s_ps = reinterpret_cast<double*>(s_fz + NSLOT * SP);  // [NX4][NSLOT][SP]
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_ps + NX4 * NSLOT * SP);  // [NSLOT]
     if (HALTED(sc)) return;
+    if (tmaon && (reinterpret_cast<uintptr_t>(&maps) & 63) != 0) {
+      // a tensor map must sit on a 64-byte boundary (the host aligns them)
+      if (threadIdx.x == 0 && threadIdx.y == 0) {
+        DevScalars* scw = const_cast<DevScalars*>(sc);
+        atomicCAS(&scw->status, CANSFZ_OK, CANSFZ_ERR_ARG);
+        scw->halted = 1;
+      }
+      return;
+    }
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
     const int i0 = bk.x * TX + 1, j0 = bk.y * TY + 1;
     const int kb = bk.z * kz + 1, ke = min(kb + kz - 1, g.nz);
@@ -115,11 +133,13 @@ struct MomentumTile {
         issued = kk;
         if (tid == 0) {
           uint64_t* bar = s_bar + slot(kk);
-          tma::bar_expect_tx(bar, 7u * PXY * 8u);
-          double* dst[7] = {s_u + o, s_v + o, s_w + o, s_c + o, reinterpret_cast<double*>(s_fx + o),
-                            reinterpret_cast<double*>(s_fy + o), reinterpret_cast<double*>(s_fz + o)};
+          constexpr int NF = 7 + NX4;
+          tma::bar_expect_tx(bar, (uint32_t)NF * PXY * 8u);
+          double* dst[11] = {s_u + o, s_v + o, s_w + o, s_c + o, reinterpret_cast<double*>(s_fx + o),
+                             reinterpret_cast<double*>(s_fy + o), reinterpret_cast<double*>(s_fz + o),
+                             s_ps + o, s_ps + NSLOT * SP + o, s_ps + 2 * NSLOT * SP + o, s_ps + 3 * NSLOT * SP + o};
 #pragma unroll
-          for (int f = 0; f < 7; ++f) tma::load_3d(dst[f], &maps.m[f], i0 - 1, j0 - 1, kk, bar);
+          for (int f = 0; f < NF; ++f) tma::load_3d(dst[f], &maps.m[f], i0 - 1, j0 - 1, kk, bar);
         }
         return;
       }
@@ -199,11 +219,25 @@ struct MomentumTile {
         // the level's loads from global memory, issued before the stencil
         // arithmetic that hides their latency
         const int c = g.h(i, j, k), t = g.t(i, j, k);
-        const double pso_x = __ldg(psio + c + 1), pso_y = __ldg(psio + c + sx), pso_z = __ldg(psio + c + sxy);
-        const double p_x = __ldg(p + c + 1), p_y = __ldg(p + c + sx), p_z = __ldg(p + c + sxy);
-        const double po_x = __ldg(po + c + 1), po_y = __ldg(po + c + sx), po_z = __ldg(po + c + sxy);
-        const double k_x = (double)__ldg(kappa + c + 1), k_y = (double)__ldg(kappa + c + sx),
-                     k_z = (double)__ldg(kappa + c + sxy);
+        double pso_x, pso_y, pso_z, p_x, p_y, p_z, po_x, po_y, po_z, k_x, k_y, k_z;
+        if constexpr (NX4 > 0) {
+          // from the staged planes k and k+1 (own points too: the carried
+          // values below are those of the element-copy path)
+          const double* sps = s_ps;
+          const double* sp_ = s_ps + NSLOT * SP;
+          const double* spo = s_ps + 2 * NSLOT * SP;
+          const double* sk = s_ps + 3 * NSLOT * SP;
+          pso_c = sps[o0]; pso_x = sps[o0 + 1]; pso_y = sps[o0 + PX]; pso_z = sps[o1];
+          p_c = sp_[o0]; p_x = sp_[o0 + 1]; p_y = sp_[o0 + PX]; p_z = sp_[o1];
+          po_c = spo[o0]; po_x = spo[o0 + 1]; po_y = spo[o0 + PX]; po_z = spo[o1];
+          k_c = sk[o0]; k_x = sk[o0 + 1]; k_y = sk[o0 + PX]; k_z = sk[o1];
+        } else {
+          pso_x = __ldg(psio + c + 1); pso_y = __ldg(psio + c + sx); pso_z = __ldg(psio + c + sxy);
+          p_x = __ldg(p + c + 1); p_y = __ldg(p + c + sx); p_z = __ldg(p + c + sxy);
+          po_x = __ldg(po + c + 1); po_y = __ldg(po + c + sx); po_z = __ldg(po + c + sxy);
+          k_x = (double)__ldg(kappa + c + 1); k_y = (double)__ldg(kappa + c + sx);
+          k_z = (double)__ldg(kappa + c + sxy);
+        }
         const double hu0 = first ? 0. : (double)duo[t], hv0 = first ? 0. : (double)dvo[t],
                      hw0 = first ? 0. : (double)dwo[t];
         double sxn = 0., syn = 0., szn = 0., sxo = 0., syo = 0., szo = 0.;
@@ -398,16 +432,16 @@ struct MomentumTile {
     (void)sxy;
   }
 };
-template <typename TI, int TYV, int OPT>
+template <typename TI, int TYV, int OPT, int STG>
 __global__ void __launch_bounds__(tile::Shape<TYV>::NT, 512 / tile::Shape<TYV>::NT) k_momentum_tile(Geo g, Phys ph,
     const DevScalars* __restrict__ sc, int kz, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ w, const double* __restrict__ psi, const double* __restrict__ psio,
     const TI* __restrict__ fx, const TI* __restrict__ fy, const TI* __restrict__ fz, const double* __restrict__ p,
     const double* __restrict__ po, const TI* __restrict__ kappa, const double* __restrict__ s, const SurfSplit sp,
     TI* __restrict__ duo, TI* __restrict__ dvo, TI* __restrict__ dwo, double* __restrict__ uo,
-    double* __restrict__ vo, double* __restrict__ wo, const __grid_constant__ HaloMaps maps, int use_tma, int wrap) {
-  MomentumTile<TI, TYV, OPT>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, sp, duo,
-      dvo, dwo, uo, vo, wo, maps, use_tma, wrap);
+    double* __restrict__ vo, double* __restrict__ wo, const __grid_constant__ HaloMaps maps, int wrap) {
+  MomentumTile<TI, TYV, OPT, STG>::run(blk_here(), g, ph, sc, kz, u, v, w, psi, psio, fx, fy, fz, p, po, kappa, s, sp,
+      duo, dvo, dwo, uo, vo, wo, maps, wrap);
 }
 
 
@@ -462,14 +496,19 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
   std::memset(&maps, 0, sizeof(maps));
   int use_tma = 0;
   if (sizeof(TI) == 8 && L.tma) {
-    const void* f[7] = {u, v, w, psi, fx, fy, fz};
+    const void* f[11] = {u, v, w, psi, fx, fy, fz, psio, p, po, kappa};
     use_tma = 1;
-    for (int q = 0; q < 7; ++q)
+    for (int q = 0; q < 11; ++q)
       if (!make_halo_map(&maps.m[q], f[q], g, S::PX, S::TY + 2)) use_tma = 0;
   }
-  kgo<MomentumTile<TI, TYV, OPT>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT>, tile::grid_of<TYV>(g, kz),
-                                       dim3(S::TX, S::TY), mom_smem<TI, TYV>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
-                                       fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, use_tma, L.wrap);
+  if (use_tma)
+    kgo<MomentumTile<TI, TYV, OPT, 1>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT, 1>,
+        tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), mom_smem<TI, TYV, 1>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
+        fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, L.wrap);
+  else
+    kgo<MomentumTile<TI, TYV, OPT, 0>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT, 0>,
+        tile::grid_of<TYV>(g, kz), dim3(S::TX, S::TY), mom_smem<TI, TYV, 0>(), g, ph, sc, kz, u, v, w, psi, psio, fx,
+        fy, fz, p, po, kappa, s, sp, duo, dvo, dwo, uo, vo, wo, maps, L.wrap);
 }
 
 template <typename TI, int TYV>
@@ -521,8 +560,11 @@ template void launch_momentum_t<float>(const Launch&, const Geo&, const Phys&, c
 // the momentum tiles use more than the default 48 KB of dynamic shared memory
 template <typename TI, int TYV, int OPT>
 static void mom_attr() {
-  cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)mom_smem<TI, TYV>());
+  cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<TI, TYV, 0>());
+  if (sizeof(TI) == 8)
+    cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mom_smem<TI, TYV, 1>());
 }
 template <typename TI, int TYV>
 static void mom_attrs() {

@@ -22,7 +22,7 @@ namespace cansfz {
 // the tensor maps of one launch's staged fields (kernel parameter, or an
 // entry of a batched launch's argument table; 64-byte aligned either way)
 struct alignas(64) HaloMaps {
-  CUtensorMap m[7];
+  CUtensorMap m[11];
 };
 
 // host: encode the map of a halo-layout FP64 field with a box of bx x by x 1
