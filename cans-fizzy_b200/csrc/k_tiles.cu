@@ -45,6 +45,21 @@ namespace {
 template <typename T>
 __device__ __forceinline__ T sqr(T x) { return x * x; }
 
+// 1/(sqrt(s) + eps) for s >= 0, the normalisation factor of the face
+// normal in the ACDI regularisation flux (src/acdi.f90:150-190).  With r = 1/sqrt(s),
+// 1/(sqrt(s) + eps) = r/(1 + eps*r) = r*(1 - eps*r + (eps*r)^2 - ...); where
+// eps*r < 2^-26 the first two terms are exact to below 2^-52 relative, so
+// r - (eps*r)*r is within an ulp or two of the direct form; one rsqrt takes
+// the place of a square root and a division.  Elsewhere (|grad| below ~1e-8,
+// zero included) the direct form.
+template <typename T>
+__device__ __forceinline__ T inv_norm_eps(T s) {
+  const T r = rsqrt(s);
+  const T er = T(CANSFZ_EPS) * r;
+  if (er < T(1.4901161193847656e-8)) return r - er * r;
+  return T(1) / (sqrt(s) + T(CANSFZ_EPS));
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -201,7 +216,7 @@ __device__ __forceinline__ void acdi_face(const AcdiCoef<T>& cf, int dir, T dli,
   const T dpsi = cf.gs * (psiR - psiL) * dli;
   const T nxf = T(0.5) * (nxR + nxL), nyf = T(0.5) * (nyR + nyL), nzf = T(0.5) * (nzR + nzL);
   const T nn = dir == 0 ? nxf : (dir == 1 ? nyf : nzf);
-  const T rn = nn / (sqrt(sqr(nxf) + sqr(nyf) + sqr(nzf)) + T(CANSFZ_EPS));
+  const T rn = nn * inv_norm_eps(sqr(nxf) + sqr(nyf) + sqr(nzf));
   T sharp;
   if (SDF) {
     sharp = cf.qg * ((T(1.) - sqr(tanh(T(0.25) * (phiR + phiL) * cf.is))) * rn);

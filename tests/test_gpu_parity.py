@@ -324,7 +324,9 @@ def test_step_thinc():
 
 def test_step_rising_bubble_2d_nn_x():
     """The reference's tests/rising_bubble set-up (64x2x128, Neumann pressure in
-    x -> cosine transforms) for 10 steps, GPU vs oracle."""
+    x -> cosine transforms) for 10 steps, GPU vs oracle.  Started from rest,
+    like test_step_bubble_3d: the bar is 1e-11 or four times the oracle's own
+    change under a 1e-15 perturbation of psi, whichever is larger."""
     text = """
 &dns
 ng(1:3) = 64, 2, 128
@@ -355,4 +357,6 @@ psi_thickness_factor = 0.51
     u, v, w, pr = init.initflow(p, "zer")
     g, o, rg, ro = _run_pair(p, u, v, w, pr, psi, 10)
     assert rg == 0 and ro == 0
-    _check_step(g, o)
+    sens = _oracle_sensitivity(p, u, v, w, pr, psi, 10)
+    errs = _check_step(g, o, tol=max(1e-11, 4.0 * sens))
+    print(f"2-D bubble errors after 10 steps: {errs}; oracle self-sensitivity {sens:.2e}")
