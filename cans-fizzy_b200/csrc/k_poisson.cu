@@ -488,6 +488,217 @@ __global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, LinePlan pl, const Dev
 }
 
 // ---------------------------------------------------------------------------
+// x transforms of the periodic kind with one warp per line, for m = 32 R
+// complex points (R = 2 or 4: real lines of 128 or 256 points).  A lane
+// holds R points of the line in registers; the complex FFT is an R-point DFT
+// in each lane, a twiddle, and 32-point DFTs across the lanes by radix-2
+// decimation in frequency with shuffles, so a line needs no block-wide
+// barrier; the real-to-complex pre- and post-processing pair k with m - k
+// through a 2 KiB per-warp shared-memory line (FP64), synchronised by the
+// warp alone.  The same transform as the shared-memory Stockham kernels in
+// another summation order (differences at round-off).
+// ---------------------------------------------------------------------------
+constexpr int kWarpLines = 4;  // lines per warp
+template <typename T>
+__device__ __forceinline__ cx<T> shfl_xor_c(cx<T> v, int m) {
+  return mk<T>(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+template <typename T>
+__device__ __forceinline__ cx<T> shfl_c(cx<T> v, int src) {
+  return mk<T>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// complex FFT of length M = 32 R with sign SIGN (-1 forward, +1 backward) of
+// the line z held as v[q] = z_{lane + 32 q}.  With k = r + R s:
+//   Z_k = sum_l W_32^{l s} W_M^{l r} sum_q z_{l + 32 q} W_R^{q r}
+// (W_n = exp(SIGN 2 pi i / n)).  On return v[r] = Z_{r + R brev5(lane)}.
+template <typename T, int R, int SIGN>
+__device__ __forceinline__ void warp_fft(const LinePlan& pl, cx<T> (&v)[R], int lane) {
+  constexpr int M = 32 * R;
+  if (R == 2) {
+    const cx<T> a = v[0], b = v[1 % R];
+    v[0] = cadd<T>(a, b);
+    v[1 % R] = csub<T>(a, b);
+  } else if (R == 4) {
+    const cx<T> t0 = cadd<T>(v[0], v[2 % R]), t1 = csub<T>(v[0], v[2 % R]);
+    const cx<T> t2 = cadd<T>(v[1 % R], v[3 % R]), t3 = csub<T>(v[1 % R], v[3 % R]);
+    const cx<T> it3 = SIGN < 0 ? mk<T>(t3.y, -t3.x) : mk<T>(-t3.y, t3.x);  // W4 * t3
+    v[0] = cadd<T>(t0, t2);
+    v[1 % R] = cadd<T>(t1, it3);
+    v[2 % R] = csub<T>(t0, t2);
+    v[3 % R] = csub<T>(t1, it3);
+  }
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    if (lane > 0) {
+      cx<T> w = TW<T>(pl, lane * r);  // W_M^{lane r}, lane r < M
+      if (SIGN > 0) w = cconj<T>(w);
+      v[r] = cmul<T>(v[r], w);
+    }
+  }
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    // pairs (i, i + h) of each block of 2h lanes: the upper lane takes
+    // x_i + x_{i+h}, the lower one (x_i - x_{i+h}) W_{2h}^{i mod h}
+    const bool lo = (lane & h) != 0;
+    const int e = (lane & (h - 1)) * (M / (2 * h));  // W_{2h}^t = W_M^{t M / (2h)}
+    cx<T> w = mk<T>(1, 0);
+    if (lo && e > 0) {
+      w = TW<T>(pl, e);
+      if (SIGN > 0) w = cconj<T>(w);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const cx<T> p = shfl_xor_c<T>(v[r], h);
+      if (lo) {
+        const cx<T> d = csub<T>(p, v[r]);
+        v[r] = e > 0 ? cmul<T>(d, w) : d;
+      } else {
+        v[r] = cadd<T>(v[r], p);
+      }
+    }
+  }
+}
+
+// X_k of a forward real transform from Z_k and Z_{m-k} (as real_fwd_X)
+template <typename T>
+__device__ __forceinline__ cx<T> real_fwd_Xc(const LinePlan& pl, cx<T> zk, cx<T> zmk, int k) {
+  const cx<T> zc = cconj<T>(zmk);
+  const cx<T> w = TW2<T>(pl, k);
+  const cx<T> sum = mk<T>((T)0.5 * (zk.x + zc.x), (T)0.5 * (zk.y + zc.y));
+  const cx<T> dif = csub<T>(zk, zc);
+  const cx<T> wd = cmul<T>(w, dif);
+  return mk<T>(sum.x + (T)0.5 * wd.y, sum.y - (T)0.5 * wd.x);
+}
+
+template <typename T, bool FUSED, int R>
+struct FftXFwdW {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const double* __restrict__ src, const double* __restrict__ u,
+      const double* __restrict__ v, const double* __restrict__ w, const Phys& ph, T* __restrict__ work) {
+    if (HALTED(sc)) return;
+    constexpr int M = 32 * R, N = 2 * M;
+    __shared__ cx<T> sz[8][M];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, brl = (int)(__brev((unsigned)lane) >> 27);
+    const int nlines = g.ny * g.nz;
+    const double dti = FUSED ? sc->dti : 0.;
+    const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi;
+    for (int t = 0; t < kWarpLines; ++t) {
+      const int gl = (bk.x * 8 + warp) * kWarpLines + t;
+      if (gl >= nlines) break;  // the same for the whole warp
+      const int jj = gl % g.ny + 1, kk = gl / g.ny + 1;
+      const int cb = g.h(1, jj, kk);
+      const double dzk = FUSED ? dti * g.dzfi[kk] : 0.;
+      auto get = [&](int c) -> double {
+        if (FUSED)
+          return ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * dzk + (__ldg(v + c) - __ldg(v + c - g.sx)) * dtidyi +
+                            (__ldg(u + c) - __ldg(u + c - 1)) * dtidxi);
+        return __ldg(src + c);
+      };
+      cx<T> z[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int c = cb + 2 * (lane + 32 * q);
+        z[q] = mk<T>((T)get(c), (T)get(c + 1));
+      }
+      warp_fft<T, R, -1>(pl, z, lane);
+#pragma unroll
+      for (int r = 0; r < R; ++r) sz[warp][r + R * brl] = z[r];
+      __syncwarp();
+      cx<T>* out = reinterpret_cast<cx<T>*>(work + (size_t)gl * N);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int k = lane + 32 * q;
+        const cx<T> X = real_fwd_Xc<T>(pl, sz[warp][k], sz[warp][(M - k) % M], k);
+        if (k == 0) {
+          const cx<T> Xm = real_fwd_Xc<T>(pl, sz[warp][0], sz[warp][0], M);
+          out[0] = mk<T>(X.x, Xm.x);  // packed: r_0, r_m
+        } else {
+          out[k] = X;
+        }
+      }
+      __syncwarp();
+    }
+  }
+};
+template <typename T, bool FUSED, int R>
+__global__ void __launch_bounds__(256) k_fft_x_fwd_w(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
+    const double* __restrict__ src, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ w, Phys ph, T* __restrict__ work) {
+  FftXFwdW<T, FUSED, R>::run(blk_here(), g, pl, sc, src, u, v, w, ph, work);
+}
+
+template <typename T, bool ADD, int R>
+struct FftXBwdW {
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
+      int wrap) {
+    if (HALTED(sc)) return;
+    constexpr int M = 32 * R, N = 2 * M;
+    __shared__ cx<T> sz[8][M];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, brl = (int)(__brev((unsigned)lane) >> 27);
+    const int nlines = g.ny * g.nz;
+    for (int t = 0; t < kWarpLines; ++t) {
+      const int gl = (bk.x * 8 + warp) * kWarpLines + t;
+      if (gl >= nlines) break;  // the same for the whole warp
+      // the packed spectrum (r_0, r_m, r_1, i_1, ...): X_k = slot k, 1 <= k < m
+      const cx<T>* row = reinterpret_cast<const cx<T>*>(work + (size_t)gl * N);
+      cx<T> P[R], G[R], Z[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) P[q] = row[lane + 32 * q];
+      // X_{m-k} for k = lane + 32 q: slot 32 (R-1-q) + (32 - lane) of lane 32 - lane,
+      // for lane 0 slot 32 (R - q) of its own
+      const int srcl = (32 - lane) & 31;
+#pragma unroll
+      for (int q = 0; q < R; ++q) G[q] = shfl_c<T>(P[q], srcl);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int k = lane + 32 * q;
+        cx<T> xk = P[q], xmk = G[R - 1 - q];
+        if (lane == 0) {
+          if (q == 0) {
+            xk = mk<T>(P[0].x, (T)0);
+            xmk = mk<T>(P[0].y, (T)0);
+          } else {
+            xmk = G[(R - q) % R];
+          }
+        }
+        Z[q] = real_bwd_Z<T>(pl, xk, xmk, k);
+      }
+      warp_fft<T, R, +1>(pl, Z, lane);
+#pragma unroll
+      for (int r = 0; r < R; ++r) sz[warp][r + R * brl] = Z[r];
+      __syncwarp();
+      const int jj = gl % g.ny + 1, kk = gl / g.ny + 1;
+      const int cb = g.h(1, jj, kk);
+      const int oy = ADD ? 0 : wrap_oy(g, wrap, jj), oz = ADD ? 0 : wrap_oz(g, wrap, kk);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int j = lane + 32 * q;
+        const cx<T> zj = sz[warp][j];
+        const int c = cb + 2 * j;  // x_{2j} at i = 2j + 1, x_{2j+1} at i = 2j + 2
+        if (ADD) {
+          dst[c] = dst[c] + (double)zj.x * normfft;
+          dst[c + 1] = dst[c + 1] + (double)zj.y * normfft;
+        } else {
+          const double o0 = (double)zj.x * normfft, o1 = (double)zj.y * normfft;
+          dst[c] = o0;
+          dst[c + 1] = o1;
+          store_images(c, wrap_ox(g, wrap, 2 * j + 1), oy, oz, [&](int h) { dst[h] = o0; });
+          store_images(c + 1, wrap_ox(g, wrap, 2 * j + 2), oy, oz, [&](int h) { dst[h] = o1; });
+        }
+      }
+      __syncwarp();
+    }
+  }
+};
+template <typename T, bool ADD, int R>
+__global__ void __launch_bounds__(256) k_fft_x_bwd_w(Geo g, LinePlan pl, const DevScalars* __restrict__ sc,
+    const T* __restrict__ work, double normfft, double* __restrict__ dst, int wrap) {
+  FftXBwdW<T, ADD, R>::run(blk_here(), g, pl, sc, work, normfft, dst, wrap);
+}
+
+// ---------------------------------------------------------------------------
 // y transforms, in place on the spectral buffer.  Lines = L consecutive x
 // positions of one z plane; the tile is read and written row by row.
 // ---------------------------------------------------------------------------
@@ -1158,6 +1369,19 @@ static void x_forward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl,
   const int nlines = g.ny * g.nz;
   const dim3 grid((nlines + L - 1) / L);
   Phys pz{};
+  if constexpr (MC == 64 || MC == 128) {
+    if (pl.px.kind == 0) {
+      constexpr int R = MC / 32;
+      const dim3 gw((nlines + 8 * kWarpLines - 1) / (8 * kWarpLines));
+      if (fused)
+        kgo<FftXFwdW<T, true, R>, 256, 1>(Lc, k_fft_x_fwd_w<T, true, R>, gw, 256, 0, g, pl.px, sc, nullptr, u, v, w,
+                                          *ph, wbuf<T>(pl));
+      else
+        kgo<FftXFwdW<T, false, R>, 256, 1>(Lc, k_fft_x_fwd_w<T, false, R>, gw, 256, 0, g, pl.px, sc, src, nullptr,
+                                           nullptr, nullptr, pz, wbuf<T>(pl));
+      return;
+    }
+  }
   if (fused)
     kgo<FftXFwd<T, true, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_fwd<T, true, MC, xL<T, MC>()>, grid, 256, smem, g,
                                                    pl.px, sc, nullptr, u, v, w, *ph, wbuf<T>(pl), L);
@@ -1278,6 +1502,14 @@ static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl
   const int L = MC ? xL<T, MC>() : lines_per_cta(m, x_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
+  if constexpr (MC == 64 || MC == 128) {
+    if (pl.px.kind == 0) {
+      constexpr int R = MC / 32;
+      kgo<FftXBwdW<T, ADD, R>, 256, 1>(Lc, k_fft_x_bwd_w<T, ADD, R>, (nlines + 8 * kWarpLines - 1) / (8 * kWarpLines),
+                                       256, 0, g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, ADD ? 0 : Lc.wrap);
+      return;
+    }
+  }
   kgo<FftXBwd<T, ADD, MC, xL<T, MC>()>, 256, 1>(Lc, k_fft_x_bwd<T, ADD, MC, xL<T, MC>()>, (nlines + L - 1) / L, 256,
                                                 smem, g, pl.px, sc, wbuf<T>(pl), pl.normfft, dst, L,
                                                 ADD ? 0 : Lc.wrap);
