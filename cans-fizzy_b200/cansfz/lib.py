@@ -35,7 +35,8 @@ class Plan(ct.Structure):
     """cansfz_plan: the launch shapes the autotuner chooses."""
     _fields_ = [("phase_slots", ct.c_int32), ("momentum_slots", ct.c_int32), ("zsolve", ct.c_int32),
                 ("fp32_transforms", ct.c_int32), ("ms_per_step", D), ("tile_tma", ct.c_int32),
-                ("ghost_images", ct.c_int32), ("reserved", ct.c_int32 * 4)]
+                ("ghost_images", ct.c_int32), ("line_transforms", ct.c_int32),
+                ("reserved", ct.c_int32 * 3)]
 
 
 SIGNATURES = {

@@ -1964,6 +1964,7 @@ int cansfz_get_plan(cansfz_ctx* c, cansfz_plan* plan) {
   plan->fp32_transforms = c->P.fp32_transforms;
   plan->tile_tma = c->L.tma;
   plan->ghost_images = c->images;
+  plan->line_transforms = c->pl.ymode;
   return CANSFZ_OK;
 }
 
@@ -1972,7 +1973,7 @@ int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
   if (plan->phase_slots < 1 || plan->phase_slots > 1024 || plan->momentum_slots < 1 ||
       plan->momentum_slots > 1024 || plan->zsolve < 0 || plan->zsolve > 1 || plan->fp32_transforms < 0 ||
       plan->fp32_transforms > 1 || plan->tile_tma < 0 || plan->tile_tma > 1 || plan->ghost_images < 0 ||
-      plan->ghost_images > 1)
+      plan->ghost_images > 1 || plan->line_transforms < 0 || plan->line_transforms > 1)
     return CANSFZ_ERR_ARG;
   CK(cudaStreamSynchronize(c->st));
   c->L.tma = plan->tile_tma;
@@ -1980,6 +1981,7 @@ int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
   c->L.phase_slots = plan->phase_slots;
   c->L.mom_slots = plan->momentum_slots;
   c->pl.zmode = plan->zsolve;
+  c->pl.ymode = plan->line_transforms;
   if (plan->fp32_transforms != c->P.fp32_transforms) {
     if (plan->fp32_transforms == 1) {
       for (int d = 0; d < 2; ++d) {
@@ -2056,7 +2058,10 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         cansfz_plan q = best;
         double ms = 0.;
         const char* rest = ln.c_str() + key.size();
-        if (std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%lf", &q.phase_slots,
+        if (std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d img=%d yt=%d ms=%lf", &q.phase_slots,
+                        &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &q.tile_tma, &q.ghost_images,
+                        &q.line_transforms, &ms) == 8 ||
+            std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%lf", &q.phase_slots,
                         &q.momentum_slots, &q.zsolve, &q.fp32_transforms, &q.tile_tma, &q.ghost_images, &ms) == 7 ||
             std::sscanf(rest, " | phase=%d mom=%d z=%d xf=%d tma=%d ms=%lf", &q.phase_slots, &q.momentum_slots,
                         &q.zsolve, &q.fp32_transforms, &q.tile_tma, &ms) == 6) {
@@ -2070,9 +2075,9 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
         if (int rc = cansfz_set_plan(c, &best)) return rc;
         if (chosen) *chosen = best;
         if (report && cap > 0)
-          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.4f", best.phase_slots,
-                        best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ghost_images,
-                        best.ms_per_step);
+          std::snprintf(report, cap, "cached: phase=%d mom=%d z=%d xf=%d tma=%d img=%d yt=%d ms=%.4f",
+                        best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
+                        best.ghost_images, best.line_transforms, best.ms_per_step);
         return CANSFZ_OK;
       }
     }
@@ -2116,6 +2121,7 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   if (c->P.form == CANSFZ_FORM_FP64) try_knob(&cansfz_plan::tile_tma, {1, 0});
   if (c->wrap) try_knob(&cansfz_plan::ghost_images, {1, 0});
   if (z_part_ok(c->g, c->pl) && !c->pl.zpiv) try_knob(&cansfz_plan::zsolve, {0, 1});
+  if (poisson_y2_applies(c->pl)) try_knob(&cansfz_plan::line_transforms, {0, 1});
   if (c->mixed && c->sweeps >= 0 && (xform_gemm_length(c->n[0]) || xform_gemm_length(c->n[1])))
     try_knob(&cansfz_plan::fp32_transforms, {0, 1});
   cansfz_destroy(k);
@@ -2124,16 +2130,16 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   if (chosen) *chosen = best;
   if (cache_file) {
     if (FILE* f = std::fopen(cache_file, "a")) {
-      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.6f\n", key.c_str(), best.phase_slots,
-                   best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma, best.ghost_images,
-                   best.ms_per_step);
+      std::fprintf(f, "%s | phase=%d mom=%d z=%d xf=%d tma=%d img=%d yt=%d ms=%.6f\n", key.c_str(),
+                   best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
+                   best.ghost_images, best.line_transforms, best.ms_per_step);
       std::fclose(f);
     }
   }
   if (report && cap > 0)
-    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d tma=%d img=%d ms=%.4f", evals,
-                  best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
-                  best.ghost_images, best.ms_per_step);
+    std::snprintf(report, cap, "tuned (%d candidates): phase=%d mom=%d z=%d xf=%d tma=%d img=%d yt=%d ms=%.4f",
+                  evals, best.phase_slots, best.momentum_slots, best.zsolve, best.fp32_transforms, best.tile_tma,
+                  best.ghost_images, best.line_transforms, best.ms_per_step);
   return CANSFZ_OK;
 }
 

@@ -761,6 +761,192 @@ __global__ void __launch_bounds__(256) k_fft_y(Geo g, LinePlan pl, const DevScal
 }
 
 // ---------------------------------------------------------------------------
+// y transforms of the periodic kind in two register passes (complex lengths
+// m = A*B of 32, 64 and 128).  With j = j2 + B j1 and k = k1 + A k2,
+//   Z_{k1 + A k2} = sum_j2 W_B^{j2 k2} W_m^{j2 k1} sum_j1 z_{j2 + B j1} W_A^{j1 k1}
+// (W_n = exp(-2 pi i / n) forward, its conjugate backward): an A-point DFT
+// per (line, j2), a twiddle, then a B-point DFT per (line, k1), each in one
+// thread's registers.  The two passes meet once in shared memory, so a
+// transform takes one block barrier; the lines' samples go from HBM into
+// registers (and back) directly, the threads of a warp covering 16 or 32
+// consecutive x positions of a row, so every access is a whole 128-byte
+// row segment.  The real-sequence step pairs Z_k with Z_{m-k}: one thread
+// of the second forward pass (of the first backward pass) owns the columns
+// k1 and A - k1 (or 0 and A/2), which hold every such pair, so the pairing
+// stays in registers.
+// ---------------------------------------------------------------------------
+// v * exp(S 2 pi i E / 16), 0 <= E < 8 (E a constant after unrolling)
+template <typename T, int S>
+__device__ __forceinline__ cx<T> rot16(cx<T> v, int E) {
+  // cos and sin of 2 pi E / 16
+  constexpr double C1 = 0.92387953251128675613, S1 = 0.38268343236508977173, H = 0.70710678118654752440;
+  if (E == 0) return v;
+  if (E == 4) return S < 0 ? mk<T>(v.y, -v.x) : mk<T>(-v.y, v.x);  // times S i
+  const double c = E == 1 ? C1 : E == 2 ? H : E == 3 ? S1 : E == 5 ? -S1 : E == 6 ? -H : -C1;
+  const double s = (E == 1 || E == 7) ? S1 : (E == 2 || E == 6) ? H : C1;
+  const T wc = (T)c, ws = (T)(S * s);
+  return mk<T>(v.x * wc - v.y * ws, v.x * ws + v.y * wc);
+}
+
+// N-point DFT (N = 2, 4, 8, 16; sign S) of v[0], v[ST], ..., v[(N-1) ST]
+// into o[0..N-1], radix-2 decimation in time, unrolled into registers
+template <typename T, int N, int S, int ST>
+struct RegDft {
+  static __device__ __forceinline__ void run(const cx<T>* v, cx<T>* o) {
+    if constexpr (N == 2) {
+      o[0] = cadd<T>(v[0], v[ST]);
+      o[1] = csub<T>(v[0], v[ST]);
+    } else {
+      cx<T> e[N / 2], d[N / 2];
+      RegDft<T, N / 2, S, 2 * ST>::run(v, e);
+      RegDft<T, N / 2, S, 2 * ST>::run(v + ST, d);
+#pragma unroll
+      for (int k = 0; k < N / 2; ++k) {
+        const cx<T> t = rot16<T, S>(d[k], k * (16 / N));
+        o[k] = cadd<T>(e[k], t);
+        o[k + N / 2] = csub<T>(e[k], t);
+      }
+    }
+  }
+};
+
+template <int M> struct Y2Shape;  // complex length -> (A, B, lines per CTA)
+template <> struct Y2Shape<32> { static constexpr int A = 8, B = 4, L = 32; };
+template <> struct Y2Shape<64> { static constexpr int A = 8, B = 8, L = 16; };
+template <> struct Y2Shape<128> { static constexpr int A = 16, B = 8, L = 16; };
+__host__ __device__ constexpr bool y2_length(int m) { return m == 32 || m == 64 || m == 128; }
+
+template <typename T, int DIR, int MC>
+struct FftY2 {
+  static constexpr int A = Y2Shape<MC>::A, B = Y2Shape<MC>::B, L = Y2Shape<MC>::L, NT = B * L;
+  static_assert(A % 2 == 0 && A / 2 <= B, "the pair pass fits in the B-pass threads");
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, T* __restrict__ work) {
+    if (HALTED(sc)) return;
+    constexpr int M = MC;
+    __shared__ cx<T> sb[M * L];  // [k1][j2][line]
+    const int nx = g.nx;
+    const int l = threadIdx.x % L, q = threadIdx.x / L;
+    const int i = bk.x * L + l;
+    const bool in = i < nx;
+    // row r of this thread's line: col[r * nx]
+    T* col = work + (size_t)bk.y * nx * (2 * M) + (in ? i : 0);
+    auto row = [&](int r) -> T& { return col[(size_t)r * nx]; };
+    // the pair pass: columns k1a = p and k1b = A - p (p > 0), or 0 and A/2
+    const int p = q, k1a = p, k1b = p == 0 ? A / 2 : A - p;
+    if (DIR > 0) {
+      {  // A-point DFTs over j1, line l, j2 = q
+        const int j2 = q;
+        cx<T> z[A], y[A];
+#pragma unroll
+        for (int j1 = 0; j1 < A; ++j1) {
+          const int r = 2 * (j2 + B * j1);
+          z[j1] = in ? mk<T>(row(r), row(r + 1)) : mk<T>(0, 0);
+        }
+        RegDft<T, A, -1, 1>::run(z, y);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+          cx<T> v = y[k1];
+          if (k1 > 0 && j2 > 0) v = cmul<T>(v, TW<T>(pl, j2 * k1));
+          sb[(k1 * B + j2) * L + l] = v;
+        }
+      }
+      __syncthreads();
+      if (p < A / 2) {  // B-point DFTs over j2 for the columns k1a, k1b
+        cx<T> a[B], b[B], za[B], zb[B];
+#pragma unroll
+        for (int j2 = 0; j2 < B; ++j2) {
+          a[j2] = sb[(k1a * B + j2) * L + l];
+          b[j2] = sb[(k1b * B + j2) * L + l];
+        }
+        RegDft<T, B, -1, 1>::run(a, za);  // Z_{k1a + A k2} = za[k2]
+        RegDft<T, B, -1, 1>::run(b, zb);
+        if (in) {
+#pragma unroll
+          for (int k2 = 0; k2 < B; ++k2) {
+            // Z_{m-k}: m - (k1a + A k2) = k1b + A (B-1-k2) (p > 0) or A (B-k2) (p = 0)
+            const int ka = k1a + A * k2, kb = k1b + A * k2;
+            const cx<T> za_m = p > 0 ? zb[B - 1 - k2] : za[(B - k2) % B];
+            const cx<T> zb_m = p > 0 ? za[B - 1 - k2] : zb[B - 1 - k2];
+            const cx<T> Xa = real_fwd_Xc<T>(pl, za[k2], za_m, ka);
+            const cx<T> Xb = real_fwd_Xc<T>(pl, zb[k2], zb_m, kb);
+            if (ka == 0) {  // packed: r_0, r_m
+              row(0) = Xa.x;
+              row(1) = real_fwd_Xc<T>(pl, za[0], za[0], M).x;
+            } else {
+              row(2 * ka) = Xa.x;
+              row(2 * ka + 1) = Xa.y;
+            }
+            row(2 * kb) = Xb.x;
+            row(2 * kb + 1) = Xb.y;
+          }
+        }
+      }
+    } else {
+      if (p < A / 2) {  // Z_k from the packed spectrum, B-point DFTs over k2
+        cx<T> xa[B], xb[B];
+        T xm = (T)0;  // X_m (real), packed beside X_0
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) {
+          const int ka = k1a + A * k2, kb = k1b + A * k2;
+          if (ka == 0) {
+            xa[k2] = in ? mk<T>(row(0), (T)0) : mk<T>(0, 0);
+            xm = in ? row(1) : (T)0;
+          } else {
+            xa[k2] = in ? mk<T>(row(2 * ka), row(2 * ka + 1)) : mk<T>(0, 0);
+          }
+          xb[k2] = in ? mk<T>(row(2 * kb), row(2 * kb + 1)) : mk<T>(0, 0);
+        }
+        cx<T> za[B], zb[B];
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) {
+          const int ka = k1a + A * k2, kb = k1b + A * k2;
+          const cx<T> xa_m = p > 0 ? xb[B - 1 - k2] : (k2 == 0 ? mk<T>(xm, (T)0) : xa[B - k2]);
+          const cx<T> xb_m = p > 0 ? xa[B - 1 - k2] : xb[B - 1 - k2];
+          za[k2] = real_bwd_Z<T>(pl, xa[k2], xa_m, ka);
+          zb[k2] = real_bwd_Z<T>(pl, xb[k2], xb_m, kb);
+        }
+        cx<T> ua[B], ub[B];
+        RegDft<T, B, +1, 1>::run(za, ua);
+        RegDft<T, B, +1, 1>::run(zb, ub);
+#pragma unroll
+        for (int j2 = 0; j2 < B; ++j2) {
+          cx<T> va = ua[j2], vb = ub[j2];
+          if (j2 > 0) {
+            if (k1a > 0) va = cmul<T>(va, cconj<T>(TW<T>(pl, j2 * k1a)));
+            vb = cmul<T>(vb, cconj<T>(TW<T>(pl, j2 * k1b)));
+          }
+          sb[(k1a * B + j2) * L + l] = va;
+          sb[(k1b * B + j2) * L + l] = vb;
+        }
+      }
+      __syncthreads();
+      {  // A-point DFTs over k1, line l, j2 = q: z_{j2 + B j1}
+        const int j2 = q;
+        cx<T> u[A], z[A];
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) u[k1] = sb[(k1 * B + j2) * L + l];
+        RegDft<T, A, +1, 1>::run(u, z);
+        if (in) {
+#pragma unroll
+          for (int j1 = 0; j1 < A; ++j1) {
+            const int r = 2 * (j2 + B * j1);
+            row(r) = z[j1].x;
+            row(r + 1) = z[j1].y;
+          }
+        }
+      }
+    }
+  }
+};
+template <typename T, int DIR, int MC>
+__global__ void __launch_bounds__(FftY2<T, DIR, MC>::NT, 3) k_fft_y2(Geo g, LinePlan pl,
+                                                                   const DevScalars* __restrict__ sc,
+                                                                   T* __restrict__ work) {
+  FftY2<T, DIR, MC>::run(blk_here(), g, pl, sc, work);
+}
+
+// ---------------------------------------------------------------------------
 // z: batched Thomas (dgtsv_homebrewed with the eps pivot shift, src/solver.f90:
 // 151-177 / src/solver_gpu.f90:179-203).  One column per thread; the forward
 // sweep writes p' in place and keeps d only at chunk ends (shared memory);
@@ -1405,6 +1591,17 @@ static void x_forward(const Launch& Lc, const Geo& g, const PoissonPlan& pl, con
 template <typename T, int MC>
 static void y_pass_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
   const int m = pl.py.m < 1 ? 1 : pl.py.m;
+  if constexpr (y2_length(MC)) {
+    if (pl.py.kind == 0 && pl.ymode == 0) {
+      using Y = FftY2<T, 1, MC>;
+      const dim3 g2((g.nx + Y::L - 1) / Y::L, g.nz);
+      if (dir > 0)
+        kgo<FftY2<T, 1, MC>, Y::NT, 3>(Lc, k_fft_y2<T, 1, MC>, g2, Y::NT, 0, g, pl.py, sc, wbuf<T>(pl));
+      else
+        kgo<FftY2<T, -1, MC>, Y::NT, 3>(Lc, k_fft_y2<T, -1, MC>, g2, Y::NT, 0, g, pl.py, sc, wbuf<T>(pl));
+      return;
+    }
+  }
   const int L = MC ? yL<T, MC>() : lines_per_cta(m, y_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const dim3 grid((g.nx + L - 1) / L, g.nz);
@@ -1449,6 +1646,8 @@ static void z_part_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, co
   kgo<ZSolvePart<T, CH>, 256, sizeof(T) == 4 ? 4 : 2>(Lc, k_zsolve_part<T, CH>, ncol / ZP_NC, 32 * ZP_P, zpart_smem<T>(g.nz), ncol,
                                  g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl), pl.zsing);
 }
+
+bool poisson_y2_applies(const PoissonPlan& pl) { return pl.py.kind == 0 && y2_length(pl.py.m); }
 
 // the partitioned solve serves non-periodic z with nz = 8 * CH and whole
 // tiles of columns; few-column grids keep the factored solve

@@ -348,14 +348,18 @@ typedef struct cansfz_plan {
                                ghost images, so the ghost fills after them
                                skip those copies (default); 0 the fills copy
                                them.  The ghost values are the same bits     */
-  int32_t reserved[4];
+  int32_t line_transforms;  /* y transforms of the periodic kind with 64, 128
+                               or 256 points: 0 two register passes per line
+                               with one block barrier (default), 1 the
+                               shared-memory Stockham FFT                    */
+  int32_t reserved[3];
 } cansfz_plan;
 int cansfz_get_plan(cansfz_ctx* ctx, cansfz_plan* plan);
 /* Takes effect at the next step (the step graphs are captured again).    */
 int cansfz_set_plan(cansfz_ctx* ctx, const cansfz_plan* plan);
 /* Time candidate plans on a copy of the case (same parameters, the case's
  * current fields; the case itself does not advance) by a coordinate search
- * over the six knobs, and apply the fastest.  cache_file (NULL: none): a
+ * over the seven knobs, and apply the fastest.  cache_file (NULL: none): a
  * text file with one line per key (grid, form, refinement sweeps, options,
  * GPU name); a key found there is applied without timing, a new one is
  * appended.  report (NULL or cap bytes): a one-line account of the choice. */

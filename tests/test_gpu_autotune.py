@@ -3,8 +3,9 @@ cansfz_autotune), through the C ABI.
 
 * The tile kernels' z split is a launch shape only: steps with other splits
   are bit-equal.  The z-solve variant changes the elimination order
-  (round-off), the FP32 solve's transforms change the FP32 result before
-  refinement; both stay within the FP64 whole-step bar.
+  (round-off), the y-transform variant the FFT factorisation (round-off),
+  the FP32 solve's transforms change the FP32 result before refinement; all
+  stay within the FP64 whole-step bar.
 * The autotuner times on a copy: the case itself neither advances nor
   changes.  Its choice is written to the cache file and read back, without
   timing, by the next case with the same key.
@@ -77,6 +78,23 @@ def test_zsolve_variants_agree():
     assert q.zsolve == 0
     q.zsolve = 1
     b.set_plan(q)
+    assert a.step(5) == 0 and b.step(5) == 0
+    for nm, x, y in zip(("u", "v", "w", "p", "psi"), _state(a), _state(b)):
+        if nm == "p":
+            x, y = x[1:-1, 1:-1, 1:-1] - x[1:-1, 1:-1, 1:-1].mean(), y[1:-1, 1:-1, 1:-1] - y[1:-1, 1:-1, 1:-1].mean()
+        assert np.abs(x - y).max() <= 1e-11 * np.abs(y).max(), nm
+
+
+@pytest.mark.parametrize("n", [(256, 128, 64), (64, 64, 32), (48, 256, 32)])
+def test_line_transform_variants_agree(n):
+    # periodic y of 128, 64 and 256 points: the two-pass register y
+    # transforms (line_transforms = 0) against the Stockham kernels (1)
+    a, b = _case(n), _case(n)
+    q = b.plan()
+    assert q.line_transforms == 0
+    q.line_transforms = 1
+    b.set_plan(q)
+    assert b.plan().line_transforms == 1
     assert a.step(5) == 0 and b.step(5) == 0
     for nm, x, y in zip(("u", "v", "w", "p", "psi"), _state(a), _state(b)):
         if nm == "p":

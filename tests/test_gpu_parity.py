@@ -184,7 +184,11 @@ def test_projection_procedures(small):
                                         ("DDNNDD", (128, 256, 64)), ("PPPPDD", (256, 128, 128)),
                                         ("NNNNNN", (256, 128, 64)),
                                         # lines of 192 points (radix 4, 4, 2, 3); a z chunk of 24 levels
-                                        ("PPPPNN", (192, 192, 64)), ("PPPPNN", (256, 128, 192))])
+                                        ("PPPPNN", (192, 192, 64)), ("PPPPNN", (256, 128, 192)),
+                                        # periodic y of 64 and 256 points (the two-pass register y
+                                        # kernels), x lengths that leave a partial tile of lines
+                                        ("PPPPNN", (40, 64, 16)), ("NNPPNN", (24, 256, 16)),
+                                        ("PPPPDD", (48, 256, 24))])
 def test_poisson_bcs(cbcpre, ng):
     p = _nml(*ng, cbcpre, l=(1.0, 0.75, 1.2))
     g, o = C.Case(p), O.Case(p)
