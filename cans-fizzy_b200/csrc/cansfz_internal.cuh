@@ -196,10 +196,10 @@ struct PoissonPlan {
   // z solve of grids with many columns: 0 the partitioned tile solve where
   // it applies, 1 one column per thread (cansfz_plan.zsolve)
   int zmode;
-  // y transforms of the periodic kind: 0 the two-pass register kernels where
-  // the length allows, 1 the shared-memory Stockham kernels
-  // (cansfz_plan.line_transforms)
-  int ymode;
+  // x and y transforms of the periodic kind: 0 the two-pass register
+  // kernels where the length allows, 1 the one-warp-per-line (x) and
+  // shared-memory Stockham kernels (cansfz_plan.line_transforms)
+  int lmode;
 };
 
 // ---------------------------------------------------------------------------
@@ -369,7 +369,7 @@ double xform_coef(int kind, int dir, int n, int j, int k);
 std::vector<uint16_t> xform_bmat(int kind, int dir, int n);
 bool xform_gemm_length(int n);
 bool z_part_ok(const Geo& g, const PoissonPlan& pl);
-// the y transforms have a two-pass register kernel (periodic kind, 64-256 points)
+// the x or y transforms have a two-pass register kernel (periodic kind, 64-256 points)
 bool poisson_y2_applies(const PoissonPlan& pl);
 int xform_gemm_set_attributes();
 void launch_xform_gemm(const Launch& L, const Geo& g, int mode, bool add, const uint16_t* bmat, int n,

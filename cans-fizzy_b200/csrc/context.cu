@@ -1964,7 +1964,7 @@ int cansfz_get_plan(cansfz_ctx* c, cansfz_plan* plan) {
   plan->fp32_transforms = c->P.fp32_transforms;
   plan->tile_tma = c->L.tma;
   plan->ghost_images = c->images;
-  plan->line_transforms = c->pl.ymode;
+  plan->line_transforms = c->pl.lmode;
   return CANSFZ_OK;
 }
 
@@ -1981,7 +1981,7 @@ int cansfz_set_plan(cansfz_ctx* c, const cansfz_plan* plan) {
   c->L.phase_slots = plan->phase_slots;
   c->L.mom_slots = plan->momentum_slots;
   c->pl.zmode = plan->zsolve;
-  c->pl.ymode = plan->line_transforms;
+  c->pl.lmode = plan->line_transforms;
   if (plan->fp32_transforms != c->P.fp32_transforms) {
     if (plan->fp32_transforms == 1) {
       for (int d = 0; d < 2; ++d) {

@@ -939,6 +939,180 @@ struct FftY2 {
     }
   }
 };
+// x transforms of the periodic kind in the same two register passes.  An x
+// line is a contiguous row, so the threads of a line take consecutive j2
+// (first forward pass) or consecutive column pairs (k1a, k1b) (pair pass),
+// and a warp's accesses are whole row segments.  The two passes meet in
+// shared memory laid out [line][k1][j2] with a k1 pitch of B + 1 complex
+// values, which keeps the eight 16-byte accesses of a quarter warp on
+// distinct banks in both passes.  Forward: the input is the interior of a
+// halo-layout FP64 field, or (FUSED) fillps's right-hand side formed on the
+// fly; the packed spectrum goes to the line's row of the spectral buffer.
+// Backward: from that row into the halo-layout field, scaled by normfft,
+// with its periodic images (or added to it, ADD).
+template <typename T, bool FUSED, int MC>
+struct FftX2Fwd {
+  static constexpr int A = Y2Shape<MC>::A, B = Y2Shape<MC>::B, L = Y2Shape<MC>::L, NT = B * L, P = B + 1;
+  static constexpr int LP = A * P + (B == 4 ? 4 : 0);  // line pitch: two lines per quarter warp when B = 4
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const double* __restrict__ src, const double* __restrict__ u,
+      const double* __restrict__ v, const double* __restrict__ w, const Phys& ph, T* __restrict__ work) {
+    if (HALTED(sc)) return;
+    constexpr int M = MC, N = 2 * MC;
+    __shared__ cx<T> sb[L * LP];  // [line][k1][j2]
+    const int q = threadIdx.x % B, l = threadIdx.x / B;
+    const int gl = bk.x * L + l;
+    const bool in = gl < g.ny * g.nz;
+    const int jj = in ? gl % g.ny + 1 : 1, kk = in ? gl / g.ny + 1 : 1;
+    const int cb = g.h(1, jj, kk);
+    const double dti = FUSED ? sc->dti : 0.;
+    const double dtidxi = dti * g.dxi, dtidyi = dti * g.dyi, dzk = FUSED ? dti * g.dzfi[kk] : 0.;
+    auto get = [&](int c) -> double {
+      if (FUSED)
+        return ph.rho0 * ((__ldg(w + c) - __ldg(w + c - g.sxy)) * dzk + (__ldg(v + c) - __ldg(v + c - g.sx)) * dtidyi +
+                          (__ldg(u + c) - __ldg(u + c - 1)) * dtidxi);
+      return __ldg(src + c);
+    };
+    cx<T>* sl = sb + l * LP;
+    {  // A-point DFTs over j1, j2 = q
+      const int j2 = q;
+      cx<T> z[A], y[A];
+#pragma unroll
+      for (int j1 = 0; j1 < A; ++j1) {
+        const int c = cb + 2 * (j2 + B * j1);
+        z[j1] = in ? mk<T>((T)get(c), (T)get(c + 1)) : mk<T>(0, 0);
+      }
+      RegDft<T, A, -1, 1>::run(z, y);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) {
+        cx<T> t = y[k1];
+        if (k1 > 0 && j2 > 0) t = cmul<T>(t, TW<T>(pl, j2 * k1));
+        sl[k1 * P + j2] = t;
+      }
+    }
+    __syncthreads();
+    const int p = q;
+    if (p < A / 2 && in) {  // B-point DFTs over j2 for the columns k1a, k1b
+      const int k1a = p, k1b = p == 0 ? A / 2 : A - p;
+      cx<T> a[B], b[B], za[B], zb[B];
+#pragma unroll
+      for (int j2 = 0; j2 < B; ++j2) {
+        a[j2] = sl[k1a * P + j2];
+        b[j2] = sl[k1b * P + j2];
+      }
+      RegDft<T, B, -1, 1>::run(a, za);
+      RegDft<T, B, -1, 1>::run(b, zb);
+      cx<T>* out = reinterpret_cast<cx<T>*>(work + (size_t)gl * N);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) {
+        const int ka = k1a + A * k2, kb = k1b + A * k2;
+        const cx<T> za_m = p > 0 ? zb[B - 1 - k2] : za[(B - k2) % B];
+        const cx<T> zb_m = p > 0 ? za[B - 1 - k2] : zb[B - 1 - k2];
+        const cx<T> Xa = real_fwd_Xc<T>(pl, za[k2], za_m, ka);
+        if (ka == 0) out[0] = mk<T>(Xa.x, real_fwd_Xc<T>(pl, za[0], za[0], M).x);  // packed: r_0, r_m
+        else out[ka] = Xa;
+        out[kb] = real_fwd_Xc<T>(pl, zb[k2], zb_m, kb);
+      }
+    }
+  }
+};
+template <typename T, bool FUSED, int MC>
+__global__ void __launch_bounds__(FftX2Fwd<T, FUSED, MC>::NT, 3) k_fft_x2_fwd(Geo g, LinePlan pl,
+    const DevScalars* __restrict__ sc, const double* __restrict__ src, const double* __restrict__ u,
+    const double* __restrict__ v, const double* __restrict__ w, Phys ph, T* __restrict__ work) {
+  FftX2Fwd<T, FUSED, MC>::run(blk_here(), g, pl, sc, src, u, v, w, ph, work);
+}
+
+template <typename T, bool ADD, int MC>
+struct FftX2Bwd {
+  static constexpr int A = Y2Shape<MC>::A, B = Y2Shape<MC>::B, L = Y2Shape<MC>::L, NT = B * L, P = B + 1;
+  static constexpr int LP = A * P + (B == 4 ? 4 : 0);
+  static __device__ __forceinline__ void run(const Blk& bk, const Geo& g, const LinePlan& pl,
+      const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
+      int wrap) {
+    if (HALTED(sc)) return;
+    constexpr int N = 2 * MC;
+    __shared__ cx<T> sb[L * LP];  // [line][k1][j2]
+    const int q = threadIdx.x % B, l = threadIdx.x / B;
+    const int gl = bk.x * L + l;
+    const bool in = gl < g.ny * g.nz;
+    cx<T>* sl = sb + l * LP;
+    const int p = q;
+    if (p < A / 2 && in) {  // Z_k from the packed spectrum, B-point DFTs over k2
+      const int k1a = p, k1b = p == 0 ? A / 2 : A - p;
+      const cx<T>* row = reinterpret_cast<const cx<T>*>(work + (size_t)gl * N);
+      cx<T> xa[B], xb[B];
+      T xm = (T)0;
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) {
+        const int ka = k1a + A * k2, kb = k1b + A * k2;
+        const cx<T> ra = row[ka];
+        if (ka == 0) {
+          xa[k2] = mk<T>(ra.x, (T)0);
+          xm = ra.y;
+        } else {
+          xa[k2] = ra;
+        }
+        xb[k2] = row[kb];
+      }
+      cx<T> za[B], zb[B];
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) {
+        const int ka = k1a + A * k2, kb = k1b + A * k2;
+        const cx<T> xa_m = p > 0 ? xb[B - 1 - k2] : (k2 == 0 ? mk<T>(xm, (T)0) : xa[B - k2]);
+        const cx<T> xb_m = p > 0 ? xa[B - 1 - k2] : xb[B - 1 - k2];
+        za[k2] = real_bwd_Z<T>(pl, xa[k2], xa_m, ka);
+        zb[k2] = real_bwd_Z<T>(pl, xb[k2], xb_m, kb);
+      }
+      cx<T> ua[B], ub[B];
+      RegDft<T, B, +1, 1>::run(za, ua);
+      RegDft<T, B, +1, 1>::run(zb, ub);
+#pragma unroll
+      for (int j2 = 0; j2 < B; ++j2) {
+        cx<T> va = ua[j2], vb = ub[j2];
+        if (j2 > 0) {
+          if (k1a > 0) va = cmul<T>(va, cconj<T>(TW<T>(pl, j2 * k1a)));
+          vb = cmul<T>(vb, cconj<T>(TW<T>(pl, j2 * k1b)));
+        }
+        sl[k1a * P + j2] = va;
+        sl[k1b * P + j2] = vb;
+      }
+    }
+    __syncthreads();
+    if (in) {  // A-point DFTs over k1, j2 = q: z_{j2 + B j1}
+      const int j2 = q;
+      cx<T> uu[A], z[A];
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) uu[k1] = sl[k1 * P + j2];
+      RegDft<T, A, +1, 1>::run(uu, z);
+      const int jj = gl % g.ny + 1, kk = gl / g.ny + 1;
+      const int cb = g.h(1, jj, kk);
+      const int oy = ADD ? 0 : wrap_oy(g, wrap, jj), oz = ADD ? 0 : wrap_oz(g, wrap, kk);
+#pragma unroll
+      for (int j1 = 0; j1 < A; ++j1) {
+        const int j = j2 + B * j1;
+        const int c = cb + 2 * j;  // x_{2j} at i = 2j + 1, x_{2j+1} at i = 2j + 2
+        if (ADD) {
+          dst[c] = dst[c] + (double)z[j1].x * normfft;
+          dst[c + 1] = dst[c + 1] + (double)z[j1].y * normfft;
+        } else {
+          const double o0 = (double)z[j1].x * normfft, o1 = (double)z[j1].y * normfft;
+          dst[c] = o0;
+          dst[c + 1] = o1;
+          store_images(c, wrap_ox(g, wrap, 2 * j + 1), oy, oz, [&](int h) { dst[h] = o0; });
+          store_images(c + 1, wrap_ox(g, wrap, 2 * j + 2), oy, oz, [&](int h) { dst[h] = o1; });
+        }
+      }
+    }
+  }
+};
+template <typename T, bool ADD, int MC>
+__global__ void __launch_bounds__(FftX2Bwd<T, ADD, MC>::NT, 3) k_fft_x2_bwd(Geo g, LinePlan pl,
+    const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
+    int wrap) {
+  FftX2Bwd<T, ADD, MC>::run(blk_here(), g, pl, sc, work, normfft, dst, wrap);
+}
+
 template <typename T, int DIR, int MC>
 __global__ void __launch_bounds__(FftY2<T, DIR, MC>::NT, 3) k_fft_y2(Geo g, LinePlan pl,
                                                                    const DevScalars* __restrict__ sc,
@@ -1555,6 +1729,22 @@ static void x_forward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl,
   const int nlines = g.ny * g.nz;
   const dim3 grid((nlines + L - 1) / L);
   Phys pz{};
+  // the two-pass x forward; with fillps fused in (11 loads per sample pair),
+  // lines of 128 and 256 points keep the one-warp-per-line kernel, whose
+  // lanes hold 4 or 8 samples instead of 32 (0.158 against 0.184 ms at 256^3)
+  if constexpr (y2_length(MC)) {
+    if (pl.px.kind == 0 && pl.lmode == 0 && !(fused && (MC == 64 || MC == 128))) {
+      using X = FftX2Fwd<T, true, MC>;
+      const dim3 g2((nlines + X::L - 1) / X::L);
+      if (fused)
+        kgo<FftX2Fwd<T, true, MC>, X::NT, 3>(Lc, k_fft_x2_fwd<T, true, MC>, g2, X::NT, 0, g, pl.px, sc, nullptr, u, v,
+                                            w, *ph, wbuf<T>(pl));
+      else
+        kgo<FftX2Fwd<T, false, MC>, X::NT, 3>(Lc, k_fft_x2_fwd<T, false, MC>, g2, X::NT, 0, g, pl.px, sc, src,
+                                             nullptr, nullptr, nullptr, pz, wbuf<T>(pl));
+      return;
+    }
+  }
   if constexpr (MC == 64 || MC == 128) {
     if (pl.px.kind == 0) {
       constexpr int R = MC / 32;
@@ -1592,7 +1782,7 @@ template <typename T, int MC>
 static void y_pass_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, const DevScalars* sc, int dir) {
   const int m = pl.py.m < 1 ? 1 : pl.py.m;
   if constexpr (y2_length(MC)) {
-    if (pl.py.kind == 0 && pl.ymode == 0) {
+    if (pl.py.kind == 0 && pl.lmode == 0) {
       using Y = FftY2<T, 1, MC>;
       const dim3 g2((g.nx + Y::L - 1) / Y::L, g.nz);
       if (dir > 0)
@@ -1647,7 +1837,9 @@ static void z_part_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl, co
                                  g.nz, pl.lam, pl.a, pl.b, pl.c, sc, wbuf<T>(pl), pl.zsing);
 }
 
-bool poisson_y2_applies(const PoissonPlan& pl) { return pl.py.kind == 0 && y2_length(pl.py.m); }
+bool poisson_y2_applies(const PoissonPlan& pl) {
+  return (pl.py.kind == 0 && y2_length(pl.py.m)) || (pl.px.kind == 0 && y2_length(pl.px.m));
+}
 
 // the partitioned solve serves non-periodic z with nz = 8 * CH and whole
 // tiles of columns; few-column grids keep the factored solve
@@ -1701,6 +1893,14 @@ static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl
   const int L = MC ? xL<T, MC>() : lines_per_cta(m, x_maxL(m), sizeof(T));
   const size_t smem = 4 * (size_t)m * (L | 1) * sizeof(T);
   const int nlines = g.ny * g.nz;
+  if constexpr (y2_length(MC)) {
+    if (pl.px.kind == 0 && pl.lmode == 0) {
+      using X = FftX2Bwd<T, ADD, MC>;
+      kgo<FftX2Bwd<T, ADD, MC>, X::NT, 3>(Lc, k_fft_x2_bwd<T, ADD, MC>, (nlines + X::L - 1) / X::L, X::NT, 0, g,
+                                         pl.px, sc, wbuf<T>(pl), pl.normfft, dst, ADD ? 0 : Lc.wrap);
+      return;
+    }
+  }
   if constexpr (MC == 64 || MC == 128) {
     if (pl.px.kind == 0) {
       constexpr int R = MC / 32;

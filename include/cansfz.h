@@ -348,10 +348,11 @@ typedef struct cansfz_plan {
                                ghost images, so the ghost fills after them
                                skip those copies (default); 0 the fills copy
                                them.  The ghost values are the same bits     */
-  int32_t line_transforms;  /* y transforms of the periodic kind with 64, 128
-                               or 256 points: 0 two register passes per line
-                               with one block barrier (default), 1 the
-                               shared-memory Stockham FFT                    */
+  int32_t line_transforms;  /* x and y transforms of the periodic kind with
+                               64, 128 or 256 points: 0 two register passes
+                               per line with one block barrier (default), 1
+                               one warp per line (x lines of 128 or 256) or
+                               the shared-memory Stockham FFT                */
   int32_t reserved[3];
 } cansfz_plan;
 int cansfz_get_plan(cansfz_ctx* ctx, cansfz_plan* plan);

@@ -188,7 +188,10 @@ def test_projection_procedures(small):
                                         # periodic y of 64 and 256 points (the two-pass register y
                                         # kernels), x lengths that leave a partial tile of lines
                                         ("PPPPNN", (40, 64, 16)), ("NNPPNN", (24, 256, 16)),
-                                        ("PPPPDD", (48, 256, 24))])
+                                        ("PPPPDD", (48, 256, 24)),
+                                        # periodic x of 64 and 128 points (the two-pass register x
+                                        # kernels), line counts that leave a partial tile
+                                        ("PPPPNN", (64, 20, 14)), ("PPNNNN", (128, 40, 13))])
 def test_poisson_bcs(cbcpre, ng):
     p = _nml(*ng, cbcpre, l=(1.0, 0.75, 1.2))
     g, o = C.Case(p), O.Case(p)
