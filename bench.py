@@ -158,6 +158,7 @@ def plan_dict(q, report):
             "fp32_transforms": "tcgen05 GEMM" if q.fp32_transforms == 0 else "FFT",
             "tile_staging": "TMA" if q.tile_tma else "cp.async",
             "ghost_images": "written by the producing kernels" if q.ghost_images else "fill stages",
+            "line_transforms": "two register passes" if q.line_transforms == 0 else "warp per line / Stockham",
             "tuned_ms_per_step": q.ms_per_step, "report": report}
 
 
@@ -166,8 +167,8 @@ def measured_peaks():
     if os.path.exists(path):
         with open(path) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (MEASURED_PEAKS.json absent: an earlier copy measurement on this pool)"
 
 
 class Clocks:
@@ -547,7 +548,7 @@ def gpu_arm(args):
         "config": run_config(args, p, workload, world),
         "run": {"final_time": d.time, "final_dt": d.dt, "divmax": d.divmax},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "frac": achieved / peak, "peak_source": peak_kind,
                      "bytes_per_launch": bytes_launch, "traffic": traffic,
                      "step_frac": (B_ALG_STEP * cells / (ms_step * 1e-3) / 1e9) / peak},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
