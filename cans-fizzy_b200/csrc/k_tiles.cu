@@ -14,7 +14,9 @@
 // vertices.  The vertex gradient is evaluated in the form the reference uses
 // for the (+x,+y,+z) vertex of its lower cell, so a vertex that the
 // reference evaluates from another cell may differ in the last bit (sums of
-// the same four terms in another order).  The vertex plane of level k+1 and
+// the same four terms in another order).  A cell's normal sums its eight
+// vertices as the two half sums its curvature takes the difference of (the
+// reference sums them in order 1..8: the normal may differ in the last bit).  The vertex plane of level k+1 and
 // the cells of level k are evaluated in the same pass (three vertex planes,
 // four cell planes in the ring), so each level needs one barrier.  A vertex
 // plane has (TX+1)(TY+1) vertices, TX+TY+1 more than the tile's cells; a
@@ -164,15 +166,18 @@ struct YoungsTile {
           my[q] = src[VXY + vm + off[q]];
           mz[q] = src[2 * VXY + vm + off[q]];
         }
-        const T norm_x = T(.125) * (mx[0] + mx[1] + mx[2] + mx[3] + mx[4] + mx[5] + mx[6] + mx[7]);
-        const T norm_y = T(.125) * (my[0] + my[1] + my[2] + my[3] + my[4] + my[5] + my[6] + my[7]);
-        const T norm_z = T(.125) * (mz[0] + mz[1] + mz[2] + mz[3] + mz[4] + mz[5] + mz[6] + mz[7]);
+        // the half sums over the +/- vertices of each direction serve both
+        // the curvature (their difference) and the cell normal (their sum)
+        const T xp = mx[0] + mx[1] + mx[2] + mx[3], xm = mx[4] + mx[5] + mx[6] + mx[7];
+        const T yp = my[0] + my[2] + my[4] + my[6], ym = my[1] + my[3] + my[5] + my[7];
+        const T zp = mz[0] + mz[1] + mz[4] + mz[5], zm = mz[2] + mz[3] + mz[6] + mz[7];
+        const T norm_x = T(.125) * (xp + xm);
+        const T norm_y = T(.125) * (yp + ym);
+        const T norm_z = T(.125) * (zp + zm);
         const T inv = recip_rn(sqrt(sqr(norm_x) + sqr(norm_y) + sqr(norm_z)) + T(CANSFZ_EPS));
         const int c = g.h(i, j, k);
         const T ox = norm_x * inv, oy = norm_y * inv, oz = norm_z * inv;
-        const T kap = -(T(0.25) * ((mx[0] + mx[1] + mx[2] + mx[3]) - (mx[4] + mx[5] + mx[6] + mx[7])) * d1 +
-                        T(0.25) * ((my[0] + my[2] + my[4] + my[6]) - (my[1] + my[3] + my[5] + my[7])) * d2 +
-                        T(0.25) * ((mz[0] + mz[1] + mz[4] + mz[5]) - (mz[2] + mz[3] + mz[6] + mz[7])) * (T)g.dzfi[k]);
+        const T kap = -(T(0.25) * (xp - xm) * d1 + T(0.25) * (yp - ym) * d2 + T(0.25) * (zp - zm) * (T)g.dzfi[k]);
         normx[c] = ox;
         normy[c] = oy;
         normz[c] = oz;
