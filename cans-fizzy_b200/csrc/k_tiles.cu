@@ -193,7 +193,7 @@ struct YoungsTile {
   }
 };
 template <typename TI, int TYV>
-__global__ void __launch_bounds__(tile::Shape<TYV>::NT + tile::Shape<TYV>::TX, 3) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
+__global__ void __launch_bounds__(tile::Shape<TYV>::NT + tile::Shape<TYV>::TX, 4) k_youngs_tile(Geo g, const DevScalars* __restrict__ sc, int kz,
                                                           const TI* __restrict__ phi, TI* __restrict__ normx,
                                                           TI* __restrict__ normy, TI* __restrict__ normz,
                                                           TI* __restrict__ kappa, int wrap) {
@@ -420,7 +420,7 @@ static void youngs_go(const Launch& L, const Geo& g, const DevScalars* sc, const
                       TI* kappa) {
   using S = tile::Shape<TYV>;
   const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.phase_slots > 0 ? L.phase_slots : 24);
-  kgo<YoungsTile<TI, TYV>, S::NT + S::TX, 3>(L, k_youngs_tile<TI, TYV>, tile::grid_of<TYV>(g, kz),
+  kgo<YoungsTile<TI, TYV>, S::NT + S::TX, 4>(L, k_youngs_tile<TI, TYV>, tile::grid_of<TYV>(g, kz),
                                               dim3(S::TX, S::TY + 1), 0, g, sc, kz, phi, nx, ny, nz, kappa, L.wrap);
 }
 
