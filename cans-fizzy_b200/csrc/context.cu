@@ -900,7 +900,7 @@ int cansfz_create(const cansfz_params* prm, void* stream, cansfz_ctx** out) {
   // reductions: partial sums of one launch over the interior blocks
   const int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
   const size_t nblk = (size_t)((nx + bx - 1) / bx) * ny * nz;
-  // ... and four per block of the fused end-of-step reduction (8 blocks per SM at most)
+  // ... and four per block of the fused end-of-step reduction (4 blocks per SM)
   const size_t nred = 4 * (size_t)(c->L.nsm > 0 ? c->L.nsm : 148) * 8;
   if ((rc = dalloc(c, &c->partial, std::max(2 * nblk, nred) + 64))) return fail(rc);
   if ((rc = dalloc(c, &c->sc, 1))) return fail(rc);

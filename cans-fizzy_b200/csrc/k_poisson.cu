@@ -1107,7 +1107,7 @@ struct FftX2Bwd {
   }
 };
 template <typename T, bool ADD, int MC>
-__global__ void __launch_bounds__(FftX2Bwd<T, ADD, MC>::NT, 3) k_fft_x2_bwd(Geo g, LinePlan pl,
+__global__ void __launch_bounds__(FftX2Bwd<T, ADD, MC>::NT, 4) k_fft_x2_bwd(Geo g, LinePlan pl,
     const DevScalars* __restrict__ sc, const T* __restrict__ work, double normfft, double* __restrict__ dst,
     int wrap) {
   FftX2Bwd<T, ADD, MC>::run(blk_here(), g, pl, sc, work, normfft, dst, wrap);
@@ -1896,7 +1896,7 @@ static void x_backward_len(const Launch& Lc, const Geo& g, const PoissonPlan& pl
   if constexpr (y2_length(MC)) {
     if (pl.px.kind == 0 && pl.lmode == 0) {
       using X = FftX2Bwd<T, ADD, MC>;
-      kgo<FftX2Bwd<T, ADD, MC>, X::NT, 3>(Lc, k_fft_x2_bwd<T, ADD, MC>, (nlines + X::L - 1) / X::L, X::NT, 0, g,
+      kgo<FftX2Bwd<T, ADD, MC>, X::NT, 4>(Lc, k_fft_x2_bwd<T, ADD, MC>, (nlines + X::L - 1) / X::L, X::NT, 0, g,
                                          pl.px, sc, wbuf<T>(pl), pl.normfft, dst, ADD ? 0 : Lc.wrap);
       return;
     }

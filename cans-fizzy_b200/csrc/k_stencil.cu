@@ -1266,7 +1266,10 @@ __global__ void k_step_reduce_final(Phys ph, DevScalars* __restrict__ sc, int nb
 void launch_step_reductions(const Launch& L, const Geo& g, const Phys& ph, DevScalars* sc, double* partial,
                             const double* u, const double* v, const double* w) {
   const int nrows = g.ny * g.nz;
-  int nb = (L.nsm > 0 ? L.nsm : 148) * 8;
+  // one wave: four blocks of 256 threads per SM are resident at the
+  // kernel's 60 registers (eight, as two waves, left a tail: 0.107 against
+  // 0.096 ms at 256^3)
+  int nb = (L.nsm > 0 ? L.nsm : 148) * 4;
   if (nb > nrows) nb = nrows;
   kgo<StepReduce, 256, 1>(L, k_step_reduce, nb, kReduceThreads, 0, g, sc, ph.acdi, partial, u, v, w);
   kgo<StepReduceFinal, 1024, 1>(L, k_step_reduce_final, 1, 1024, 0, ph, sc, nb, partial);
