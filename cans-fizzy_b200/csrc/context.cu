@@ -2118,7 +2118,7 @@ int cansfz_autotune(cansfz_ctx* c, const char* cache_file, cansfz_plan* chosen, 
   };
   try_knob(&cansfz_plan::phase_slots, {12, 24, 48});
   try_knob(&cansfz_plan::momentum_slots, {24, 48, 96});
-  if (c->P.form == CANSFZ_FORM_FP64) try_knob(&cansfz_plan::tile_tma, {1, 0});
+  try_knob(&cansfz_plan::tile_tma, {1, 0});
   if (c->wrap) try_knob(&cansfz_plan::ghost_images, {1, 0});
   if (z_part_ok(c->g, c->pl) && !c->pl.zpiv) try_knob(&cansfz_plan::zsolve, {0, 1});
   if (poisson_y2_applies(c->pl)) try_knob(&cansfz_plan::line_transforms, {0, 1});

@@ -42,26 +42,32 @@ namespace cansfz {
 // from the extrapolated one, and the new force goes to the history slot.
 // ---------------------------------------------------------------------------
 namespace {
-// the plane slot pitch: for the FP64 drop-in the ring slots start on 128-byte
-// boundaries, where the TMA plane copies land
-template <typename TI, int TYV>
+// the plane slot pitch: with TMA staging (and for the FP64 drop-in) the
+// ring slots start on 128-byte boundaries, where the TMA plane copies land
+template <typename TI, int TYV, int STG>
 constexpr int mom_pitch() {
   using SH = tile::Shape<TYV>;
-  return sizeof(TI) == 8 ? (SH::PXY + 15) / 16 * 16 : SH::PXY;
+  return (sizeof(TI) == 8 || STG) ? (SH::PXY + 15) / 16 * 16 : SH::PXY;
 }
-// STG: the FP64 drop-in's planes are staged by TMA, and then psio, p, po
-// and kappa as well, so that their +x, +y, +z neighbours come from shared
-// memory; otherwise seven fields by element copies and those four through
-// the read-only cache
+// STG: the planes are staged by TMA, and then psio, p, po and kappa as well,
+// so that their +x, +y, +z neighbours come from shared memory; otherwise
+// seven fields by element copies and those four through the read-only cache.
+// With TI = float (the mixed form) only the FP64 fields can be TMA copies: a
+// tensor map needs row strides that are multiples of 16 bytes, and an FP32
+// halo row of nx + 2 values is not one in general; the three FP32 fluxes
+// and kappa are then element copies into the ring beside them.
 template <typename TI, int STG>
-constexpr int mom_extra() { return (STG && sizeof(TI) == 8) ? 4 : 0; }
+constexpr int mom_extra() { return STG ? 4 : 0; }
 template <typename TI, int TYV, int STG>
 constexpr size_t mom_smem() {
   using namespace tile;
   using SH = Shape<TYV>;
-  constexpr int SP = mom_pitch<TI, TYV>(), NSLOT = SH::NSLOT;
-  return (size_t)NSLOT * SP * ((4 + mom_extra<TI, STG>()) * sizeof(double) + 3 * sizeof(TI)) +
-         NSLOT * sizeof(uint64_t);
+  constexpr int SP = mom_pitch<TI, TYV, STG>(), NSLOT = SH::NSLOT;
+  // FP64 drop-in: u v w c | fx fy fz | psio p po kappa; mixed form with
+  // STG: u v w c | psio p po (FP64) | fx fy fz kappa (FP32); else u v w c | fx fy fz
+  constexpr size_t nd = 4 + (sizeof(TI) == 8 ? mom_extra<TI, STG>() : (STG ? 3 : 0));
+  constexpr size_t nt = 3 + ((sizeof(TI) != 8 && STG) ? 1 : 0);
+  return (size_t)NSLOT * SP * (nd * sizeof(double) + nt * sizeof(TI)) + NSLOT * sizeof(uint64_t);
 }
 }  // namespace
 
@@ -83,11 +89,12 @@ struct MomentumTile {
     using namespace tile;
     using SH = Shape<TYV>;
     constexpr int TX = SH::TX, TY = SH::TY, NT = SH::NT, PX = SH::PX, PXY = SH::PXY, NSLOT = SH::NSLOT;
-    constexpr int SP = mom_pitch<TI, TYV>();
-    // TMA plane copies for the FP64 drop-in's seven staged fields; the
-    // element copies otherwise (and for the FP32 fluxes of the mixed form)
-    // (a tensor map must sit on a 64-byte boundary; a misplaced one falls back)
-    constexpr bool tmaon = STG != 0 && sizeof(TI) == 8;
+    constexpr int SP = mom_pitch<TI, TYV, STG>();
+    // TMA plane copies for the staged FP64 fields; element copies for the
+    // rest (all fields without STG; the FP32 fluxes and kappa of the mixed
+    // form with it).  A tensor map must sit on a 64-byte boundary.
+    constexpr bool tmaon = STG != 0;
+    constexpr bool mixstg = STG != 0 && sizeof(TI) != 8;  // FP32 planes beside the TMA ones
     (void)TY;
     typedef double T;  // the RHS in FP64 for both storage types
     extern __shared__ __align__(128) unsigned char smem[];
@@ -95,12 +102,15 @@ struct MomentumTile {
     double* s_v = s_u + NSLOT * SP;
     double* s_w = s_v + NSLOT * SP;
     double* s_c = s_w + NSLOT * SP;
-    TI* s_fx = reinterpret_cast<TI*>(s_c + NSLOT * SP);
+    constexpr int NX4 = mom_extra<TI, STG>();  // staged psio, p, po, kappa
+    // mixed form with STG: psio, p, po (FP64) follow c, then fx fy fz kappa
+    TI* s_fx = mixstg ? reinterpret_cast<TI*>(s_c + 4 * NSLOT * SP) : reinterpret_cast<TI*>(s_c + NSLOT * SP);
     TI* s_fy = s_fx + NSLOT * SP;
     TI* s_fz = s_fy + NSLOT * SP;
-    constexpr int NX4 = mom_extra<TI, STG>();  // staged psio, p, po, kappa (FP64 drop-in)
-    double* s_ps = reinterpret_cast<double*>(s_fz + NSLOT * SP);  // [NX4][NSLOT][SP]
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_ps + NX4 * NSLOT * SP);  // [NSLOT]
+    TI* s_kf = s_fz + NSLOT * SP;  // kappa, mixed form with STG only
+    double* s_ps = mixstg ? s_c + NSLOT * SP : reinterpret_cast<double*>(s_fz + NSLOT * SP);  // [NX4][NSLOT][SP]
+    uint64_t* s_bar = mixstg ? reinterpret_cast<uint64_t*>(s_kf + NSLOT * SP)
+                             : reinterpret_cast<uint64_t*>(s_ps + NX4 * NSLOT * SP);  // [NSLOT]
     if (HALTED(sc)) return;
     if (tmaon && (reinterpret_cast<uintptr_t>(&maps) & 63) != 0) {
       // a tensor map must sit on a 64-byte boundary (the host aligns them)
@@ -134,13 +144,35 @@ struct MomentumTile {
         issued = kk;
         if (tid == 0) {
           uint64_t* bar = s_bar + slot(kk);
-          constexpr int NF = 7 + NX4;
-          tma::bar_expect_tx(bar, (uint32_t)NF * PXY * 8u);
-          double* dst[11] = {s_u + o, s_v + o, s_w + o, s_c + o, reinterpret_cast<double*>(s_fx + o),
-                             reinterpret_cast<double*>(s_fy + o), reinterpret_cast<double*>(s_fz + o),
-                             s_ps + o, s_ps + NSLOT * SP + o, s_ps + 2 * NSLOT * SP + o, s_ps + 3 * NSLOT * SP + o};
+          if constexpr (!mixstg) {
+            constexpr int NF = 7 + NX4;
+            tma::bar_expect_tx(bar, (uint32_t)NF * PXY * 8u);
+            double* dst[11] = {s_u + o, s_v + o, s_w + o, s_c + o, reinterpret_cast<double*>(s_fx + o),
+                               reinterpret_cast<double*>(s_fy + o), reinterpret_cast<double*>(s_fz + o),
+                               s_ps + o, s_ps + NSLOT * SP + o, s_ps + 2 * NSLOT * SP + o, s_ps + 3 * NSLOT * SP + o};
 #pragma unroll
-          for (int f = 0; f < NF; ++f) tma::load_3d(dst[f], &maps.m[f], i0 - 1, j0 - 1, kk, bar);
+            for (int f = 0; f < NF; ++f) tma::load_3d(dst[f], &maps.m[f], i0 - 1, j0 - 1, kk, bar);
+          } else {
+            // the seven FP64 fields: maps 0-3 (u v w psi) and 7-9 (psio p po)
+            tma::bar_expect_tx(bar, 7u * PXY * 8u);
+            double* dst[7] = {s_u + o, s_v + o, s_w + o, s_c + o, s_ps + o, s_ps + NSLOT * SP + o,
+                              s_ps + 2 * NSLOT * SP + o};
+            const int mi[7] = {0, 1, 2, 3, 7, 8, 9};
+#pragma unroll
+            for (int f = 0; f < 7; ++f) tma::load_3d(dst[f], &maps.m[mi[f]], i0 - 1, j0 - 1, kk, bar);
+          }
+        }
+        if constexpr (mixstg) {
+          for (int q = tid; q < PXY; q += NT) {
+            int h;
+            const bool ok = plane_cell<PX>(g, i0, j0, kk, q, &h);
+            const int hh = ok ? h : 0;
+            cp_async(s_fx + o + q, fx + hh, ok);
+            cp_async(s_fy + o + q, fy + hh, ok);
+            cp_async(s_fz + o + q, fz + hh, ok);
+            cp_async(s_kf + o + q, kappa + hh, ok);
+          }
+          cp_commit();
         }
         return;
       }
@@ -199,11 +231,15 @@ struct MomentumTile {
     bool fail = false;
     for (int k = kb; k <= ke; ++k) {
       if (k + 2 <= ke + 1) issue(k + 2);
-      else if (!tmaon) cp_commit();
+      else if (!tmaon || mixstg) cp_commit();
       if (tmaon) {
         // planes k and k+1 are in (each thread waits for the copies itself)
         if (!tma::bar_wait(s_bar + slot(k), phase(k)) || !tma::bar_wait(s_bar + slot(k + 1), phase(k + 1)))
           fail = true;
+        if constexpr (mixstg) {
+          cp_wait<1>();
+          __syncthreads();  // every thread's element copies of planes k and k+1 are in
+        }
       } else {
         cp_wait<1>();
         __syncthreads();  // planes k and k+1 are in; every thread is done with level k-1
@@ -231,7 +267,11 @@ struct MomentumTile {
           pso_c = sps[o0]; pso_x = sps[o0 + 1]; pso_y = sps[o0 + PX]; pso_z = sps[o1];
           p_c = sp_[o0]; p_x = sp_[o0 + 1]; p_y = sp_[o0 + PX]; p_z = sp_[o1];
           po_c = spo[o0]; po_x = spo[o0 + 1]; po_y = spo[o0 + PX]; po_z = spo[o1];
-          k_c = sk[o0]; k_x = sk[o0 + 1]; k_y = sk[o0 + PX]; k_z = sk[o1];
+          if constexpr (mixstg) {
+            k_c = (double)s_kf[o0]; k_x = (double)s_kf[o0 + 1]; k_y = (double)s_kf[o0 + PX]; k_z = (double)s_kf[o1];
+          } else {
+            k_c = sk[o0]; k_x = sk[o0 + 1]; k_y = sk[o0 + PX]; k_z = sk[o1];
+          }
         } else {
           if (k + 1 < ke && (tx & 15) == 0) {
             // the +z neighbours two levels up into L2: they are fresh DRAM
@@ -512,15 +552,19 @@ static void momentum_go(const Launch& L, const Geo& g, const Phys& ph, const Dev
                         double* wo) {
   using S = tile::Shape<TYV>;
   const int kz = tile::kz_of<TYV>(g, L.batched, L.nsm, L.mom_slots > 0 ? L.mom_slots : kMomSlots);
-  // the staged fields' tensor maps (FP64 drop-in only)
+  // the staged fields' tensor maps: all eleven in the FP64 drop-in; the
+  // seven FP64 ones (u v w psi, psio p po: entries 0-3 and 7-9) in the mixed
+  // form, whose FP32 planes are element copies
   HaloMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   int use_tma = 0;
-  if (sizeof(TI) == 8 && L.tma) {
+  if (L.tma) {
     const void* f[11] = {u, v, w, psi, fx, fy, fz, psio, p, po, kappa};
     use_tma = 1;
-    for (int q = 0; q < 11; ++q)
+    for (int q = 0; q < 11; ++q) {
+      if (sizeof(TI) != 8 && ((q >= 4 && q <= 6) || q == 10)) continue;
       if (!make_halo_map(&maps.m[q], f[q], g, S::PX, S::TY + 2)) use_tma = 0;
+    }
   }
   if (use_tma)
     kgo<MomentumTile<TI, TYV, OPT, 1>, S::NT, 512 / S::NT>(L, k_momentum_tile<TI, TYV, OPT, 1>,
@@ -583,9 +627,8 @@ template <typename TI, int TYV, int OPT>
 static void mom_attr() {
   cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)mom_smem<TI, TYV, 0>());
-  if (sizeof(TI) == 8)
-    cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)mom_smem<TI, TYV, 1>());
+  cudaFuncSetAttribute(k_momentum_tile<TI, TYV, OPT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mom_smem<TI, TYV, 1>());
 }
 template <typename TI, int TYV>
 static void mom_attrs() {

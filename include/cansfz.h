@@ -340,9 +340,10 @@ typedef struct cansfz_plan {
                                where the line lengths allow, 1 FFTs           */
   double  ms_per_step;      /* step time measured with the plan by
                                cansfz_autotune (0: not measured)              */
-  int32_t tile_tma;         /* FP64 drop-in momentum tile: 1 stages its planes
-                               with TMA tensor copies (default), 0 with
-                               element-wise cp.async                          */
+  int32_t tile_tma;         /* momentum tile: 1 stages its FP64 planes with
+                               TMA tensor copies (default; the mixed form's
+                               FP32 planes are element copies beside them), 0
+                               all planes with element-wise cp.async          */
   int32_t ghost_images;     /* periodic directions: 1 the kernels that produce
                                a field in the step also write its periodic
                                ghost images, so the ghost fills after them

@@ -85,6 +85,22 @@ def test_zsolve_variants_agree():
         assert np.abs(x - y).max() <= 1e-11 * np.abs(y).max(), nm
 
 
+@pytest.mark.parametrize("form", [0, 1])
+def test_tile_staging_is_bit_equal(form):
+    """The momentum tile's planes staged by TMA tensor copies (tile_tma = 1;
+    in the mixed form the FP64 planes, with the FP32 ones as element copies)
+    or all by element copies (0): the same values in shared memory, the same
+    arithmetic, the same bits."""
+    a, b = _case((64, 32, 48), form=form), _case((64, 32, 48), form=form)
+    q = b.plan()
+    assert q.tile_tma == 1
+    q.tile_tma = 0
+    b.set_plan(q)
+    assert a.step(6) == 0 and b.step(6) == 0
+    for nm, x, y in zip(("u", "v", "w", "p", "psi"), _state(a), _state(b)):
+        assert np.array_equal(x, y), nm
+
+
 @pytest.mark.parametrize("n", [(256, 128, 64), (64, 64, 32), (48, 256, 32)])
 def test_line_transform_variants_agree(n):
     # periodic y of 128, 64 and 256 points: the two-pass register y
