@@ -82,3 +82,26 @@ def test_ensemble_stops_on_abort():
     rc2, _ = ens.step(1)
     assert rc2 == rc  # the ensemble stays stopped
     ens.close()
+
+
+def test_batched_two_pass_line_transforms():
+    """Same-shape cases with periodic x and y lines of 64 and 128 points: their
+    batched launches run the two-pass register transforms (y both ways, x
+    backward, and x forward with fillps for the 64-point lines) and compute
+    bit for bit what each case computes alone."""
+    specs = [W._bubble_case(64, 64, 32, 1.0, 1.0, 0.5, 100.0, 10.0, 8.0, 0.3, False),
+             W._bubble_case(64, 64, 32, 1.0, 1.0, 0.5, 1000.0, 100.0, 20.0, 0.35, False),
+             W._bubble_case(128, 128, 16, 1.0, 1.0, 0.125, 10.0, 10.0, 2.0, 0.1, False),
+             W._bubble_case(128, 128, 16, 1.0, 1.0, 0.125, 100.0, 10.0, 5.0, 0.12, False)]
+    single = _build(specs)
+    for c in single:
+        assert c.step(6) == 0
+    batch = _build(specs)
+    ens = C.Ensemble(batch, batch=2)
+    rc, _ = ens.step(6)
+    assert rc == 0
+    assert ens.groups() == (2, 4)
+    for a, b in zip(single, batch):
+        for nm in ("u", "v", "w", "p", "psi"):
+            assert np.array_equal(a.get(nm), b.get(nm)), nm
+    ens.close()
